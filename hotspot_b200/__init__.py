@@ -1,0 +1,12 @@
+"""hotspot_b200 -- HotSpot's grid thermal model on NVIDIA B200 (sm_100a).
+
+The product is ``libhotspot_b200.so`` (C host code + CUDA kernels, C-ABI in
+``include/``).  This package holds its ctypes bindings (:mod:`._abi`), a
+Python mirror of the reference's model API (:mod:`.model`), seeded
+benchmark inputs in the reference's file formats (:mod:`.workloads`), and the
+batch and serving layers.
+"""
+from . import _abi  # noqa: F401
+from ._abi import FORM_FAST, FORM_PARITY, HotspotError, lib  # noqa: F401
+
+__all__ = ["lib", "FORM_PARITY", "FORM_FAST", "HotspotError"]

@@ -1,0 +1,135 @@
+// dev_model.cuh -- device-resident grid model shared by all kernels.
+//
+// HBM layout (one model):
+//   state vectors are the reference's dcuboid_tail layout (util.c:231-261):
+//   [nl][nr][nc] doubles followed by the n_extra package nodes, so a whole
+//   vector is one contiguous array of ncell + nx doubles and cell
+//   c = (n*nr + i)*nc + j.  Per-cell coefficient arrays (detailed 3-D and
+//   microchannel models) use the same cell indexing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+extern "C" {
+#include "hotspot_b200_types.h"
+#include "hsb_device.h"
+}
+
+namespace hsb {
+
+// kinds of layers with package terms (temperature_grid.c:2474-2589, 3193-3254)
+enum LayerKind { LK_PLAIN = 0, LK_SPREADER, LK_SINK, LK_SUB, LK_SOLDER, LK_PCB };
+
+// Per-layer coefficients of one multigrid level.  All resistances are the
+// exact doubles the reference divides by, precomputed on the host with the
+// reference's arithmetic (e.g. rNS = rx/2.0 + rx/2.0, temperature_grid.c:126).
+struct LayerCoef {
+  double rNS, rEW;        // lateral neighbour resistance, N/S and E/W
+  double rz;              // rz of this layer: R to the layer below; ambient R for the sink
+  double cap;             // capacitance of one cell
+  double edgeNS, edgeEW;  // R to the package node on the N/S and E/W edges
+  double ramb;            // R to ambient per cell (sink: rz; PCB: r_convec_sec share)
+  int kind;               // LayerKind
+  int pad;
+};
+
+struct StencilArgs {
+  int nl, nr, nc, nx;
+  long long plane, ncell;
+  int field;              // per-cell coefficient arrays in use
+  int secondary;
+  unsigned long long uchan_mask;   // bit n set: layer n has advection terms
+  double ambient;
+  const LayerCoef *L;     // nl entries (device)
+  const package_RC_t *pk; // device copy of the package R/C
+  const double *rN, *rS, *rW, *rE, *rA, *rB, *cap;
+  const double *aN, *aS, *aW, *aE, *aO, *qin;
+};
+
+struct LevelBuf {
+  int nr, nc;
+  double *p;              // power at this level (ncell + nx)
+  double *v;              // temperature at this level (ncell + nx)
+  LayerCoef *L;           // device per-layer table for this level
+  LayerCoef hostL[HSB_MAX_LAYERS];
+};
+
+}  // namespace hsb
+
+struct hsb_dev_model {
+  int nl, nr, nc, nx;
+  long long plane, ncell, vlen;   // vlen = ncell + nx
+  int spidx, hsidx, subidx, solderidx, pcbidx;
+  int field, map_mode, total_n_blocks;
+  double ambient, width, height, pcb_amb_num;
+  double h_rx[HSB_MAX_LAYERS], h_ry[HSB_MAX_LAYERS], h_rz[HSB_MAX_LAYERS], h_c[HSB_MAX_LAYERS];
+  package_RC_t h_pk;
+  int device;
+  cudaStream_t stream;
+
+  // state and work vectors (FP64, vlen each)
+  double *y;          // transient state (last_trans)
+  double *ys;         // steady state (last_steady)
+  double *pgrid;      // grid power
+  double *k1, *k2, *k3, *ytemp, *t1, *t2;
+  unsigned long long *errbits;   // device max-norm accumulator
+  double *h_err;                 // pinned host mirror
+  package_RC_t *pk;   // device package R/C
+  hsb::LayerCoef *L0; // finest-level layer table (device)
+  hsb::LayerCoef hostL0[HSB_MAX_LAYERS];
+
+  // per-cell coefficients (field mode)
+  double *rN, *rS, *rW, *rE, *rA, *rB, *cap;
+  // advection
+  double *aN, *aS, *aW, *aE, *aO, *qin;
+  unsigned long long uchan_mask;
+
+  // block <-> grid maps
+  int *b2g_ptr, *b2g_blk;
+  double *b2g_occ, *b2g_area;
+  double cell_area;
+  int *g2b;
+  double *blk_in, *blk_out;      // device block vectors (total_n_blocks + nx)
+  double *h_blk;                 // pinned staging (2 * (total_n_blocks + nx))
+
+  // multigrid levels for the exact nested-iteration replay
+  int n_levels;
+  hsb::LevelBuf *levels;
+  int *gs_status;                // device: [0]=converged flag, [1]=sweeps done
+  double *gs_delta;              // device: last sweep's max change
+  int *h_gs;                     // pinned host mirror of gs_status
+  double *h_gsd;
+
+  // fast-form workspace (allocated lazily by those solvers)
+  void *fast;
+  void (*fast_free)(void *);
+};
+
+namespace hsb {
+
+StencilArgs make_args(const hsb_dev_model *m, const LayerCoef *L, int nr, int nc);
+int set_error(int code, const std::string &msg);
+int cuda_check(cudaError_t e, const char *what);
+
+// b2g / g2b on the device (temperature_grid.c:1888-2015)
+int b2g(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type);
+int g2b(hsb_dev_model *m, const double *grid_dev, double *blk_dev);
+
+// exact-replay solvers
+int rk4_exact_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
+int gs_exact_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
+
+// fast-form solvers
+int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
+int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
+int bicgstab_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
+
+}  // namespace hsb
+
+#define HSB_CUDA(call)                                              \
+  do {                                                              \
+    cudaError_t _e = (call);                                        \
+    if (_e != cudaSuccess) return hsb::cuda_check(_e, #call);       \
+  } while (0)

@@ -1,0 +1,134 @@
+/*
+ * hsb_device.h -- the thin C-ABI between libhotspot_b200's C host code and
+ * its sm_100a CUDA kernels.  Plain pointers, sizes and status codes only.
+ *
+ * The host side (grid_model.c) owns everything the reference computes once
+ * per model -- layers, block<->grid maps, package R/C, per-cell detailed-3D
+ * resistances, microchannel flow rates -- and hands the results to the device
+ * model through these calls.  The device model keeps the grid state resident
+ * in HBM and runs the hot loops that the reference runs on the CPU:
+ *
+ *   hsb_dev_transient  replaces compute_temp_grid's RK4 loop
+ *                      (temperature_grid.c:3603-3704, RCutil.c:440-640,
+ *                       slope_fn_grid/slope_fn_pack :3130-3601, :2857-3093)
+ *   hsb_dev_steady     replaces steady_state_temp_grid's solver
+ *                      (temperature_grid.c:2426-2851; the SuperLU-only
+ *                       microchannel direct solve :5130-5194 becomes BiCGStab)
+ *   b2g / g2b          xlate_vector_b2g / xlate_temp_g2b (:1888-2015) run on
+ *                      the device inside the two calls above.
+ *
+ * Every function returns 0 on success or a negative HSB_E* code; the message
+ * of the last failure on the calling thread is hsb_dev_last_error().
+ */
+#ifndef HSB_DEVICE_H
+#define HSB_DEVICE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HSB_OK            0
+#define HSB_E_ARG        -1   /* invalid argument / state                */
+#define HSB_E_CUDA       -2   /* CUDA runtime error                      */
+#define HSB_E_NOMEM      -3   /* device allocation failed / over budget  */
+#define HSB_E_NOCONV     -4   /* iteration cap reached without converging */
+#define HSB_E_NODEV      -5   /* no CUDA device visible                  */
+
+#define HSB_MAX_LAYERS   64
+
+/* solver forms */
+#define HSB_FORM_PARITY  0    /* FP64, replays the reference's operation order */
+#define HSB_FORM_FAST    1    /* FP32 stencil work, FP64 state/refinement       */
+
+/* steady methods */
+#define HSB_STEADY_AUTO       0  /* GS replay for FORM_PARITY; MG-PCG (or BiCGStab with advection) for FORM_FAST */
+#define HSB_STEADY_GS_REPLAY  1  /* nested-iteration multigrid + exact-order Gauss-Seidel */
+#define HSB_STEADY_MG         2  /* V-cycle preconditioned CG, FP32 inner, FP64 refinement */
+#define HSB_STEADY_BICGSTAB   3  /* BiCGStab, FP32 inner, FP64 refinement (non-symmetric) */
+
+typedef struct hsb_grid_desc {
+  int nl, nr, nc;            /* layers, rows, cols (finest grid) */
+  int n_extra;               /* 12, or 28 with the secondary path */
+  int spidx, hsidx;          /* spreader / heat-sink layer indices */
+  int subidx, solderidx, pcbidx;  /* secondary-path layers, -1 if absent */
+  int field;                 /* 0: per-layer R/C (uniform); 1: per-cell arrays */
+  int map_mode;              /* HSB_GRID_* block mapping for temperatures */
+  int total_n_blocks;
+  double ambient;
+  double width, height;      /* die size (m): cell sizes of every multigrid level */
+  double pcb_amb_num;        /* r_convec_sec * s_pcb^2, secondary path only */
+  /* per layer (nl entries): the reference's layer_t rx, ry, rz, c */
+  const double *layer_rx, *layer_ry, *layer_rz, *layer_c;
+  const double *pack;        /* 52 doubles, package_RC_t field order */
+} hsb_grid_desc;
+
+typedef struct hsb_solver_opts {
+  int form;                  /* HSB_FORM_* */
+  int steady_method;         /* HSB_STEADY_* */
+  double steady_tol;         /* FP64 residual target (K) for MG / BiCGStab */
+  int max_iters;             /* cap on sweeps / cycles / Krylov iterations (0 = default) */
+} hsb_solver_opts;
+
+typedef struct hsb_stats {
+  long long rk4_steps;       /* accepted RK4 steps */
+  long long rk4_attempts;    /* RK4 attempts including rejected ones */
+  long long slope_evals;     /* stencil evaluations */
+  long long sweeps;          /* Gauss-Seidel sweeps, summed over levels */
+  long long cycles;          /* V-cycles / Krylov iterations */
+  long long refinements;     /* FP64 iterative-refinement passes */
+  double residual;           /* final max |r| (W) of the FP64 residual, or last GS delta */
+  double sim_time;           /* simulated seconds advanced */
+  double device_ms;          /* device time of the call (CUDA events) */
+} hsb_stats;
+
+struct hsb_dev_model;
+typedef struct hsb_dev_model hsb_dev_model;
+
+int  hsb_dev_create(hsb_dev_model **out, const hsb_grid_desc *d);
+void hsb_dev_destroy(hsb_dev_model *m);
+
+/* per-layer values may change (populate_R_model re-called, natural convection) */
+int hsb_dev_set_layers(hsb_dev_model *m, const double *rx, const double *ry,
+                       const double *rz, const double *c, const double *pack52,
+                       double ambient, double width, double height,
+                       double pcb_amb_num);
+
+/* per-cell detailed-3D coefficients; each array has nl*nr*nc entries.
+ * r?[c] is the resistance between cell c and its N/S/W/E/above/below
+ * neighbour exactly as find_res(neighbour, c) returns it (0 where absent). */
+int hsb_dev_set_cells(hsb_dev_model *m, const double *rN, const double *rS,
+                      const double *rW, const double *rE, const double *rA,
+                      const double *rB, const double *cap);
+
+/* microchannel advection per cell (nl*nr*nc each, zero outside channel
+ * layers): aN..aE = Cv*flow(neighbour->cell) for fluid pairs, aO = outlet
+ * self coefficient, qin = inlet source (W). */
+int hsb_dev_set_advection(hsb_dev_model *m, const double *aN, const double *aS,
+                          const double *aW, const double *aE, const double *aO,
+                          const double *qin);
+
+/* block->grid map: CSR over the nl*nr*nc cells, entries (block, occupancy,
+ * block area); g2b: 5 ints per block (layer, i1, i2, j1, j2). */
+int hsb_dev_set_maps(hsb_dev_model *m, const int *b2g_ptr, const int *b2g_blk,
+                     const double *b2g_occ, const double *b2g_area,
+                     double cell_area, const int *g2b);
+
+int hsb_dev_transient(hsb_dev_model *m, const double *block_power,
+                      const double *block_temp_in, double time_elapsed,
+                      double *block_temp_out, const hsb_solver_opts *o,
+                      hsb_stats *st);
+int hsb_dev_steady(hsb_dev_model *m, const double *block_power,
+                   double *block_temp_out, const hsb_solver_opts *o,
+                   hsb_stats *st);
+
+/* which: 0 = transient state (last_trans), 1 = steady state (last_steady);
+ * n = nl*nr*nc + n_extra doubles */
+int hsb_dev_get_state(hsb_dev_model *m, int which, double *out);
+int hsb_dev_set_state(hsb_dev_model *m, int which, const double *in);
+
+const char *hsb_dev_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
