@@ -325,8 +325,13 @@ gs_sweeps(StencilArgs A, double *__restrict__ vg, const double *__restrict__ p, 
     if (threadIdx.x == 0) {
       double gmax = red[0];
       for (int w = 1; w < (int)(blockDim.x >> 5); w++) gmax = fmax(gmax, red[w]);
+      // "return MAX(max, single_iteration_steady_pack(...))" (:2607): the
+      // reference's MAX macro evaluates the package update twice when the
+      // grid's change is not the larger one; the grid and so the edge sums
+      // are unchanged between the two evaluations
       const double pmax = gs_pack(A, v, es, nr, nc, spidx, hsidx, subidx, solderidx, pcbidx);
-      delta = gmax > pmax ? gmax : pmax;   // MAX(max, pack) (:2607)
+      delta = gmax > pmax ? gmax
+                          : gs_pack(A, v, es, nr, nc, spidx, hsidx, subidx, solderidx, pcbidx);
       red[0] = delta;
       if (fabs(delta - 0) < GS_DELTA) done = 1;
     }

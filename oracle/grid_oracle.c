@@ -588,8 +588,12 @@ static double gs_sweep_level(const orc_model *m, const level_t *L, double *v, co
         d = fabs(prev - v[c]);
         if (d > max) max = d;
       }
+  /* "return MAX(max, single_iteration_steady_pack(...))" (:2607) with the
+   * reference's MAX macro evaluates the package update a second time
+   * whenever the grid's change is not larger than the package's */
   pmax = gs_pack(m, L, v);
-  return max > pmax ? max : pmax;
+  if (max > pmax) return max;
+  return gs_pack(m, L, v);
 }
 
 double orc_gs_sweep(const orc_model *m, double *v, const double *p)
