@@ -126,7 +126,8 @@ class Stats(C.Structure):
     _fields_ = [("rk4_steps", C.c_longlong), ("rk4_attempts", C.c_longlong),
                 ("slope_evals", C.c_longlong), ("sweeps", C.c_longlong),
                 ("cycles", C.c_longlong), ("refinements", C.c_longlong),
-                ("residual", C.c_double), ("sim_time", C.c_double), ("device_ms", C.c_double)]
+                ("residual", C.c_double), ("sim_time", C.c_double), ("device_ms", C.c_double),
+                ("kernel_ms", C.c_double), ("launches", C.c_longlong)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -158,6 +158,7 @@ static void fill_layer_table(const hsb_dev_model *m, LayerCoef *L, int nr, int n
 }
 
 int upload_layers(hsb_dev_model *m) {
+  m->coef_version++;
   fill_layer_table(m, m->hostL0, m->nr, m->nc, 1.0, 1.0);
   HSB_CUDA(cudaMemcpyAsync(m->L0, m->hostL0, sizeof(LayerCoef) * m->nl, cudaMemcpyHostToDevice,
                            m->stream));
@@ -185,6 +186,8 @@ int upload_layers(hsb_dev_model *m) {
 static void free_model(hsb_dev_model *m) {
   if (!m) return;
   if (m->fast && m->fast_free) m->fast_free(m->fast);
+  if (m->mg && m->mg_free) m->mg_free(m->mg);
+  if (m->krylov && m->krylov_free) m->krylov_free(m->krylov);
   double **bufs[] = {&m->y, &m->ys, &m->pgrid, &m->k1, &m->k2, &m->k3, &m->ytemp, &m->t1, &m->t2,
                      &m->rN, &m->rS, &m->rW, &m->rE, &m->rA, &m->rB, &m->cap, &m->aN, &m->aS,
                      &m->aW, &m->aE, &m->aO, &m->qin, &m->b2g_occ, &m->b2g_area, &m->blk_in,
@@ -356,6 +359,7 @@ int hsb_dev_set_cells(hsb_dev_model *m, const double *rN, const double *rS, cons
       (rc = upload_array(m, &m->cap, cap, n)))
     return rc;
   m->field = 1;
+  m->coef_version++;
   HSB_CUDA(cudaStreamSynchronize(m->stream));
   return HSB_OK;
 }
@@ -381,6 +385,7 @@ int hsb_dev_set_advection(hsb_dev_model *m, const double *aN, const double *aS, 
       }
   }
   m->uchan_mask = mask;
+  m->coef_version++;
   HSB_CUDA(cudaStreamSynchronize(m->stream));
   return HSB_OK;
 }
@@ -429,10 +434,12 @@ int hsb_dev_transient(hsb_dev_model *m, const double *block_power, const double 
   HSB_CUDA(cudaMemcpyAsync(m->blk_in, block_power, sizeof(double) * nb, cudaMemcpyHostToDevice,
                            m->stream));
   if ((rc = b2g(m, m->blk_in, m->pgrid, HSB_V_POWER))) return rc;
+  st->launches += 1;
   if (block_temp_in) {
     HSB_CUDA(cudaMemcpyAsync(m->blk_in + nb, block_temp_in, sizeof(double) * nb,
                              cudaMemcpyHostToDevice, m->stream));
     if ((rc = b2g(m, m->blk_in + nb, m->y, HSB_V_TEMP))) return rc;
+    st->launches += 1;
   }
   const int form = o ? o->form : HSB_FORM_PARITY;
   rc = form == HSB_FORM_FAST ? rk4_fast_interval(m, time_elapsed, st)
@@ -440,6 +447,7 @@ int hsb_dev_transient(hsb_dev_model *m, const double *block_power, const double 
   if (rc) return rc;
   if (block_temp_out) {
     if ((rc = g2b(m, m->y, m->blk_out))) return rc;
+    st->launches += 1;
     HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb,
                              cudaMemcpyDeviceToHost, m->stream));
   }
@@ -470,10 +478,12 @@ int hsb_dev_steady(hsb_dev_model *m, const double *block_power, double *block_te
   HSB_CUDA(cudaMemcpyAsync(m->blk_in, block_power, sizeof(double) * nb, cudaMemcpyHostToDevice,
                            m->stream));
   if ((rc = b2g(m, m->blk_in, m->pgrid, HSB_V_POWER))) return rc;
+  st->launches += 1;
   int method = o->steady_method;
   if (method == HSB_STEADY_AUTO) {
     if (m->uchan_mask) method = HSB_STEADY_BICGSTAB;
-    else method = o->form == HSB_FORM_FAST ? HSB_STEADY_MG : HSB_STEADY_GS_REPLAY;
+    else if (o->form == HSB_FORM_FAST && m->nx == HSB_EXTRA) method = HSB_STEADY_MG;
+    else method = HSB_STEADY_GS_REPLAY;
   }
   if (method == HSB_STEADY_GS_REPLAY && m->uchan_mask)
     return set_error(HSB_E_ARG,
@@ -487,6 +497,7 @@ int hsb_dev_steady(hsb_dev_model *m, const double *block_power, double *block_te
   if (rc) return rc;
   if (block_temp_out) {
     if ((rc = g2b(m, m->ys, m->blk_out))) return rc;
+    st->launches += 1;
     HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb,
                              cudaMemcpyDeviceToHost, m->stream));
   }

@@ -102,9 +102,15 @@ struct hsb_dev_model {
   int *h_gs;                     // pinned host mirror of gs_status
   double *h_gsd;
 
-  // fast-form workspace (allocated lazily by those solvers)
+  // fast-form workspaces (allocated lazily by those solvers); coef_version
+  // counts coefficient uploads so derived FP32 tables are rebuilt when stale
+  int coef_version;
   void *fast;
   void (*fast_free)(void *);
+  void *mg;
+  void (*mg_free)(void *);
+  void *krylov;
+  void (*krylov_free)(void *);
 };
 
 namespace hsb {

@@ -1,0 +1,803 @@
+// mg_steady.cu -- converged steady state (HSB_STEADY_MG, the fast form).
+//
+// Solves the steady system of the grid model, G T = P (the fixed point the
+// reference's Gauss-Seidel approaches, i.e. the system that
+// build_transient_grid_matrix / build_transient_power_vector define,
+// temperature_grid.c:5196-6694), to FP64 accuracy:
+//
+//   outer loop (FP64):  r = P - G T;  solve G e = r approximately;  T += e
+//   inner solver (FP32): conjugate gradients preconditioned by one V-cycle
+//
+// V-cycle: cell-centred geometric multigrid that halves rows and columns
+// (layers are kept), like the reference's own coarsening; coarse operators
+// sum vertical/ambient/edge conductances over the 2x2 children and average
+// the two lateral faces crossing a coarse face, so a uniform model gets
+// exactly the reference's coarse R values (rz/4, rx and ry unchanged).
+// Smoother: red-black z-line Gauss-Seidel -- every (i,j) column is solved
+// exactly along z with a tridiagonal (Thomas) solve, which handles the thin,
+// highly conductive TIM layers -- followed by an exact dense solve of the
+// 12 package nodes given the grid.  Pre-smoothing runs red, black, package;
+// post-smoothing package, black, red, so the preconditioner is symmetric.
+// Restriction sums the 2x2 children, prolongation injects (its transpose).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "dev_model.cuh"
+
+namespace hsb {
+
+#define MGT 256
+#define NXP 12
+
+struct PackSys {               // the 12 package nodes' equations
+  float D[NXP];                // diagonal (edge cells + links + ambient) at level 0
+  float link[NXP][NXP];        // conductance between package nodes
+  float gamb[NXP];             // conductance to ambient
+  int elayer[NXP], eside[NXP]; // attached edge: layer, side (0 N,1 S,2 W,3 E), -1 none
+  float ge0[NXP];              // per-cell edge conductance at level 0
+};
+
+struct MgLevelDev {
+  int nr, nc, nl;
+  long long plane, ncell;
+  const float *gE, *gS, *gB;   // face conductances: (i,j)->(i,j+1), (i,j)->(i+1,j), n->n+1
+  const float *diag;
+  const float *gAmbL;          // per layer ambient conductance per cell
+  const float *gEdgeNS, *gEdgeEW;  // per layer edge conductance per cell
+  int spidx, hsidx;
+  float scale;                 // 2^level: edge conductances per coarse cell
+};
+
+struct MgLevel {
+  int nr, nc;
+  long long plane, ncell, n;
+  float *gE, *gS, *gB, *diag, *gAmbL, *gEdgeNS, *gEdgeEW;
+  float *x, *f, *r;
+};
+
+struct MgWork {
+  int nlev, coef_version;
+  std::vector<MgLevel> lv;
+  PackSys ps;
+  PackSys *d_ps;
+  // FP64 fine-level operator for the refinement residual
+  double *gE64, *gS64, *gB64, *gAmb64, *gEdgeNS64, *gEdgeEW64;  // per cell (faces) / per layer
+  double *r64, *b64;             // residual, right-hand side (vlen)
+  // PCG vectors (fine level, FP32, n = ncell + 12)
+  float *p, *q, *z, *e, *rr;
+  double *red;                   // reduction scratch
+  double *h_red;
+};
+
+// ---------------------------------------------------------------------------
+// operator application helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int edge_node(int layer, int side, int spidx, int hsidx) {
+  // side 0 N, 1 S, 2 W, 3 E
+  if (layer == hsidx) return side == 0 ? HSB_SINK_C_N : side == 1 ? HSB_SINK_C_S : side == 2 ? HSB_SINK_C_W : HSB_SINK_C_E;
+  if (layer == spidx) return side == 0 ? HSB_SP_N : side == 1 ? HSB_SP_S : side == 2 ? HSB_SP_W : HSB_SP_E;
+  return -1;
+}
+
+// y = A x on level L (cells only; package rows handled by pack_apply)
+__global__ void mg_apply_cells(MgLevelDev L, const float *__restrict__ x, float *__restrict__ y,
+                               const float *__restrict__ f, int mode) {
+  // mode 0: y = A x ; mode 1: y = f - A x
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.ncell) return;
+  const int n = (int)(c / L.plane);
+  const long long r = c - n * L.plane;
+  const int i = (int)(r / L.nc), j = (int)(r - (long long)i * L.nc);
+  float s = L.diag[c] * x[c];
+  if (j < L.nc - 1) s -= L.gE[c] * x[c + 1];
+  if (j > 0) s -= L.gE[c - 1] * x[c - 1];
+  if (i < L.nr - 1) s -= L.gS[c] * x[c + L.nc];
+  if (i > 0) s -= L.gS[c - L.nc] * x[c - L.nc];
+  if (n < L.nl - 1) s -= L.gB[c] * x[c + L.plane];
+  if (n > 0) s -= L.gB[c - L.plane] * x[c - L.plane];
+  const float *xp = x + L.ncell;
+  if (n == L.spidx || n == L.hsidx) {
+    if (i == 0) s -= L.gEdgeNS[n] * xp[edge_node(n, 0, L.spidx, L.hsidx)];
+    if (i == L.nr - 1) s -= L.gEdgeNS[n] * xp[edge_node(n, 1, L.spidx, L.hsidx)];
+    if (j == 0) s -= L.gEdgeEW[n] * xp[edge_node(n, 2, L.spidx, L.hsidx)];
+    if (j == L.nc - 1) s -= L.gEdgeEW[n] * xp[edge_node(n, 3, L.spidx, L.hsidx)];
+  }
+  y[c] = mode ? f[c] - s : s;
+}
+
+// package rows: one CTA; sums of the attached edges by warps
+__global__ void mg_apply_pack(MgLevelDev L, const PackSys *__restrict__ ps, const float *__restrict__ x,
+                              float *__restrict__ y, const float *__restrict__ f, int mode) {
+  __shared__ float esum[NXP];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int k = w; k < NXP; k += blockDim.x >> 5) {
+    float s = 0.f;
+    const int layer = ps->elayer[k], side = ps->eside[k];
+    if (layer >= 0) {
+      const int len = side < 2 ? L.nc : L.nr;
+      const long long base = (long long)layer * L.plane +
+                             (side == 0 ? 0 : side == 1 ? (long long)(L.nr - 1) * L.nc : side == 2 ? 0 : L.nc - 1);
+      const long long st = side < 2 ? 1 : L.nc;
+      for (int q = lane; q < len; q += 32) s += x[base + q * st];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    if (lane == 0) esum[k] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < NXP) {
+    const int k = threadIdx.x;
+    const float *xp = x + L.ncell;
+    const int cnt = ps->elayer[k] < 0 ? 0 : (ps->eside[k] < 2 ? L.nc : L.nr);
+    const float ge = ps->ge0[k] * L.scale;
+    float D = cnt * ge + ps->gamb[k];
+    for (int o = 0; o < NXP; o++) D += ps->link[k][o];
+    float s = D * xp[k] - ge * esum[k];
+    for (int o = 0; o < NXP; o++) s -= ps->link[k][o] * xp[o];
+    y[L.ncell + k] = mode ? f[L.ncell + k] - s : s;
+  }
+}
+
+// red-black z-line Gauss-Seidel half sweep on level L: solve A x = f
+__global__ void mg_zline(MgLevelDev L, float *__restrict__ x, const float *__restrict__ f, int color) {
+  long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= L.plane) return;
+  const int i = (int)(col / L.nc), j = (int)(col - (long long)i * L.nc);
+  if (((i + j) & 1) != color) return;
+  const int nl = L.nl;
+  float cp[HSB_MAX_LAYERS], dp[HSB_MAX_LAYERS];
+  const float *xp = x + L.ncell;
+  float prev_c = 0.f, prev_d = 0.f;
+  for (int n = 0; n < nl; n++) {
+    const long long c = (long long)n * L.plane + col;
+    float rhs = f[c];
+    if (j < L.nc - 1) rhs += L.gE[c] * x[c + 1];
+    if (j > 0) rhs += L.gE[c - 1] * x[c - 1];
+    if (i < L.nr - 1) rhs += L.gS[c] * x[c + L.nc];
+    if (i > 0) rhs += L.gS[c - L.nc] * x[c - L.nc];
+    if (n == L.spidx || n == L.hsidx) {
+      if (i == 0) rhs += L.gEdgeNS[n] * xp[edge_node(n, 0, L.spidx, L.hsidx)];
+      if (i == L.nr - 1) rhs += L.gEdgeNS[n] * xp[edge_node(n, 1, L.spidx, L.hsidx)];
+      if (j == 0) rhs += L.gEdgeEW[n] * xp[edge_node(n, 2, L.spidx, L.hsidx)];
+      if (j == L.nc - 1) rhs += L.gEdgeEW[n] * xp[edge_node(n, 3, L.spidx, L.hsidx)];
+    }
+    const float a = n > 0 ? -L.gB[c - L.plane] : 0.f;   // sub-diagonal
+    const float cc = n < nl - 1 ? -L.gB[c] : 0.f;        // super-diagonal
+    const float b = L.diag[c];
+    // Thomas forward elimination
+    const float den = b - a * prev_c;
+    const float cn = cc / den;
+    const float dn = (rhs - a * prev_d) / den;
+    cp[n] = cn;
+    dp[n] = dn;
+    prev_c = cn;
+    prev_d = dn;
+  }
+  float v = dp[nl - 1];
+  x[(long long)(nl - 1) * L.plane + col] = v;
+  for (int n = nl - 2; n >= 0; n--) {
+    v = dp[n] - cp[n] * v;
+    x[(long long)n * L.plane + col] = v;
+  }
+}
+
+// exact solve of the package nodes with the grid fixed (Gaussian elimination)
+__global__ void mg_pack_solve(MgLevelDev L, const PackSys *__restrict__ ps, float *__restrict__ x,
+                              const float *__restrict__ f) {
+  __shared__ float esum[NXP];
+  __shared__ float M[NXP][NXP + 1];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int k = w; k < NXP; k += blockDim.x >> 5) {
+    float s = 0.f;
+    const int layer = ps->elayer[k], side = ps->eside[k];
+    if (layer >= 0) {
+      const int len = side < 2 ? L.nc : L.nr;
+      const long long base = (long long)layer * L.plane +
+                             (side == 0 ? 0 : side == 1 ? (long long)(L.nr - 1) * L.nc : side == 2 ? 0 : L.nc - 1);
+      const long long st = side < 2 ? 1 : L.nc;
+      for (int q = lane; q < len; q += 32) s += x[base + q * st];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    if (lane == 0) esum[k] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < NXP) {
+    const int k = threadIdx.x;
+    const int cnt = ps->elayer[k] < 0 ? 0 : (ps->eside[k] < 2 ? L.nc : L.nr);
+    const float ge = ps->ge0[k] * L.scale;
+    float D = cnt * ge + ps->gamb[k];
+    for (int o = 0; o < NXP; o++) {
+      D += ps->link[k][o];
+      M[k][o] = -ps->link[k][o];
+    }
+    M[k][k] = D;
+    M[k][NXP] = f[L.ncell + k] + ge * esum[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int p = 0; p < NXP; p++) {           // diagonally dominant: no pivoting
+      const float inv = 1.f / M[p][p];
+      for (int r = p + 1; r < NXP; r++) {
+        const float fct = M[r][p] * inv;
+        if (fct != 0.f)
+          for (int c = p; c <= NXP; c++) M[r][c] -= fct * M[p][c];
+      }
+    }
+    for (int p = NXP - 1; p >= 0; p--) {
+      float s = M[p][NXP];
+      for (int c = p + 1; c < NXP; c++) s -= M[p][c] * x[L.ncell + c];
+      x[L.ncell + p] = s / M[p][p];
+    }
+  }
+}
+
+// coarse f = sum of the 2x2 fine residuals; package residuals carried over
+__global__ void mg_restrict_f(const float *__restrict__ rf, float *__restrict__ fc, int nl, int cnr,
+                              int cnc, int nx) {
+  const long long cpl = (long long)cnr * cnc, ncell = cpl * nl;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int fnc = 2 * cnc;
+  const long long fpl = 4 * cpl;
+  if (t < ncell) {
+    const int n = (int)(t / cpl);
+    const long long r = t - n * cpl;
+    const int i = (int)(r / cnc), j = (int)(r - (long long)i * cnc);
+    const float *s = rf + n * fpl;
+    fc[t] = s[(2 * i) * fnc + 2 * j] + s[(2 * i + 1) * fnc + 2 * j] + s[(2 * i) * fnc + 2 * j + 1] +
+            s[(2 * i + 1) * fnc + 2 * j + 1];
+  } else if (t < ncell + nx) {
+    fc[t] = rf[fpl * nl + (t - ncell)];
+  }
+}
+
+// fine x += injected coarse correction
+__global__ void mg_prolong_add(const float *__restrict__ xc, float *__restrict__ xf, int nl, int cnr,
+                               int cnc, int nx) {
+  const int fnr = 2 * cnr, fnc = 2 * cnc;
+  const long long fpl = (long long)fnr * fnc, cpl = (long long)cnr * cnc;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < fpl * nl) {
+    const int n = (int)(t / fpl);
+    const long long r = t - n * fpl;
+    const int fi = (int)(r / fnc), fj = (int)(r - (long long)fi * fnc);
+    xf[t] += xc[n * cpl + (fi / 2) * cnc + fj / 2];
+  } else if (t < fpl * nl + nx) {
+    xf[t] += xc[cpl * nl + (t - fpl * nl)];
+  }
+}
+
+__global__ void mg_zero(float *x, long long n) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) x[t] = 0.f;
+}
+
+// coarse-level face conductances from the fine level
+__global__ void mg_coarsen(const float *__restrict__ gEf, const float *__restrict__ gSf,
+                           const float *__restrict__ gBf, float *__restrict__ gEc, float *__restrict__ gSc,
+                           float *__restrict__ gBc, int nl, int cnr, int cnc) {
+  const long long cpl = (long long)cnr * cnc;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cpl * nl) return;
+  const int n = (int)(t / cpl);
+  const long long r = t - n * cpl;
+  const int i = (int)(r / cnc), j = (int)(r - (long long)i * cnc);
+  const int fnc = 2 * cnc;
+  const long long fo = (long long)n * 4 * cpl;
+  const long long f00 = fo + (2 * i) * fnc + 2 * j, f10 = f00 + fnc;
+  gEc[t] = j < cnc - 1 ? 0.5f * (gEf[f00 + 1] + gEf[f10 + 1]) : 0.f;
+  gSc[t] = i < cnr - 1 ? 0.5f * (gSf[f10] + gSf[f10 + 1]) : 0.f;
+  gBc[t] = gBf[f00] + gBf[f00 + 1] + gBf[f10] + gBf[f10 + 1];
+}
+
+// diagonal of level L from its faces, ambient and edge conductances
+__global__ void mg_diag(MgLevelDev L, float *__restrict__ diag) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.ncell) return;
+  const int n = (int)(c / L.plane);
+  const long long r = c - n * L.plane;
+  const int i = (int)(r / L.nc), j = (int)(r - (long long)i * L.nc);
+  float d = L.gAmbL[n];
+  if (j < L.nc - 1) d += L.gE[c];
+  if (j > 0) d += L.gE[c - 1];
+  if (i < L.nr - 1) d += L.gS[c];
+  if (i > 0) d += L.gS[c - L.nc];
+  if (n < L.nl - 1) d += L.gB[c];
+  if (n > 0) d += L.gB[c - L.plane];
+  if (n == L.spidx || n == L.hsidx) {
+    if (i == 0) d += L.gEdgeNS[n];
+    if (i == L.nr - 1) d += L.gEdgeNS[n];
+    if (j == 0) d += L.gEdgeEW[n];
+    if (j == L.nc - 1) d += L.gEdgeEW[n];
+  }
+  diag[c] = d;
+}
+
+// FP64 residual of the finest level: r = b - G T, returns max |r| via atomics
+__global__ void fine_residual64(const hsb::StencilArgs S, const double *__restrict__ gE,
+                                const double *__restrict__ gS, const double *__restrict__ gB,
+                                const double *__restrict__ gAmb, const double *__restrict__ gENS,
+                                const double *__restrict__ gEEW, const double *__restrict__ T,
+                                const double *__restrict__ b, double *__restrict__ r, float *__restrict__ r32,
+                                unsigned long long *maxbits) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double res = 0.0;
+  if (c < S.ncell) {
+    const int n = (int)(c / S.plane);
+    const long long q = c - n * S.plane;
+    const int i = (int)(q / S.nc), j = (int)(q - (long long)i * S.nc);
+    const double Tc = T[c];
+    double s = gAmb[n] * Tc;
+    if (j < S.nc - 1) s += gE[c] * (Tc - T[c + 1]);
+    if (j > 0) s += gE[c - 1] * (Tc - T[c - 1]);
+    if (i < S.nr - 1) s += gS[c] * (Tc - T[c + S.nc]);
+    if (i > 0) s += gS[c - S.nc] * (Tc - T[c - S.nc]);
+    if (n < S.nl - 1) s += gB[c] * (Tc - T[c + S.plane]);
+    if (n > 0) s += gB[c - S.plane] * (Tc - T[c - S.plane]);
+    const double *x = T + S.ncell;
+    const hsb::LayerCoef &Ln = S.L[n];
+    if (Ln.kind == hsb::LK_SPREADER || Ln.kind == hsb::LK_SINK) {
+      const int sp = Ln.kind == hsb::LK_SPREADER;
+      if (i == 0) s += gENS[n] * (Tc - x[sp ? HSB_SP_N : HSB_SINK_C_N]);
+      if (i == S.nr - 1) s += gENS[n] * (Tc - x[sp ? HSB_SP_S : HSB_SINK_C_S]);
+      if (j == 0) s += gEEW[n] * (Tc - x[sp ? HSB_SP_W : HSB_SINK_C_W]);
+      if (j == S.nc - 1) s += gEEW[n] * (Tc - x[sp ? HSB_SP_E : HSB_SINK_C_E]);
+    }
+    res = b[c] - s;
+    r[c] = res;
+    r32[c] = (float)res;
+  }
+  for (int o = 16; o > 0; o >>= 1) res = fmax(fabs(res), fabs(__shfl_down_sync(0xffffffffu, res, o)));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(fabs(res)));
+}
+
+// package rows of the FP64 residual (one CTA)
+__global__ void pack_residual64(const hsb::StencilArgs S, const PackSys *__restrict__ ps,
+                                const double *__restrict__ ge64, const double *__restrict__ link64,
+                                const double *__restrict__ gamb64, const double *__restrict__ T,
+                                const double *__restrict__ b, double *__restrict__ r,
+                                float *__restrict__ r32, unsigned long long *maxbits) {
+  __shared__ double esum[NXP];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int k = w; k < NXP; k += blockDim.x >> 5) {
+    double s = 0.0;
+    const int layer = ps->elayer[k], side = ps->eside[k];
+    if (layer >= 0) {
+      const int len = side < 2 ? S.nc : S.nr;
+      const long long base = (long long)layer * S.plane +
+                             (side == 0 ? 0 : side == 1 ? (long long)(S.nr - 1) * S.nc : side == 2 ? 0 : S.nc - 1);
+      const long long st = side < 2 ? 1 : S.nc;
+      for (int q = lane; q < len; q += 32) s += T[S.ncell + k] - T[base + q * st];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    if (lane == 0) esum[k] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < NXP) {
+    const int k = threadIdx.x;
+    const double *x = T + S.ncell;
+    double s = ge64[k] * esum[k] + gamb64[k] * x[k];
+    for (int o = 0; o < NXP; o++) s += link64[k * NXP + o] * (x[k] - x[o]);
+    const double res = b[S.ncell + k] - s;
+    r[S.ncell + k] = res;
+    r32[S.ncell + k] = (float)res;
+    atomicMax(maxbits, (unsigned long long)__double_as_longlong(fabs(res)));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PCG vector kernels (FP32 data, FP64 reductions in a fixed order)
+// ---------------------------------------------------------------------------
+__global__ void dot_partial(const float *__restrict__ a, const float *__restrict__ b, long long n,
+                            double *__restrict__ part) {
+  __shared__ double sm[MGT / 32];
+  double s = 0.0;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    s += (double)a[k] * (double)b[k];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < MGT / 32; w++) t += sm[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void dot_final(const double *__restrict__ part, int np, double *__restrict__ out) {
+  __shared__ double sm[32];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < np; k += blockDim.x) s += part[k];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sm[w];
+    *out = t;
+  }
+}
+
+// x += alpha p; r -= alpha q   with alpha = rz / pq
+__global__ void pcg_update_xr(float *__restrict__ x, float *__restrict__ r, const float *__restrict__ p,
+                              const float *__restrict__ q, const double *__restrict__ sc, long long n) {
+  const double alpha = sc[0] / sc[1];
+  const float a = (float)alpha;
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) {
+    x[k] += a * p[k];
+    r[k] -= a * q[k];
+  }
+}
+
+// p = z + beta p with beta = rz_new / rz_old
+__global__ void pcg_update_p(float *__restrict__ p, const float *__restrict__ z, const double *__restrict__ sc,
+                             long long n, int first) {
+  const float beta = first ? 0.f : (float)(sc[2] / sc[0]);
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) p[k] = z[k] + beta * p[k];
+}
+
+__global__ void shift_scalars(double *sc) {
+  // sc[0] = rz (old) <- sc[2] (new)
+  sc[0] = sc[2];
+}
+
+__global__ void add_correction(double *__restrict__ T, const float *__restrict__ e, long long n) {
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) T[k] += (double)e[k];
+}
+
+__global__ void copy_f(const float *__restrict__ a, float *__restrict__ b, long long n) {
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) b[k] = a[k];
+}
+
+// right-hand side in FP64: P + ambient conductances * ambient
+__global__ void build_rhs64(const hsb::StencilArgs S, const double *__restrict__ pgrid,
+                            const double *__restrict__ gAmb, const double *__restrict__ gamb64,
+                            double *__restrict__ b) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < S.ncell) {
+    const int n = (int)(c / S.plane);
+    b[c] = pgrid[c] + gAmb[n] * S.ambient;
+  } else if (c < S.ncell + S.nx) {
+    b[c] = gamb64[c - S.ncell] * S.ambient;
+  }
+}
+
+// heuristic start in FP64 (set_heuristic_temp semantics, any precision)
+__global__ void heuristic_start(const hsb::StencilArgs S, const double *__restrict__ p, double *__restrict__ v) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < S.plane) {
+    double sum = 0.0;
+    for (int n = 0; n < S.nl; n++) sum += p[n * S.plane + t];
+    v[(S.nl - 1) * S.plane + t] = S.ambient + sum * S.L[S.nl - 1].rz;
+    sum -= p[(S.nl - 1) * S.plane + t];
+    for (int n = S.nl - 2; n >= 0; n--) {
+      v[n * S.plane + t] = v[(n + 1) * S.plane + t] + S.L[n].rz * sum;
+      sum -= p[n * S.plane + t];
+    }
+  }
+  if (t < S.nx) v[S.ncell + t] = S.ambient;
+}
+
+// fine FP64 face conductances for a uniform model (1/R of the layer)
+__global__ void uniform_faces64(const hsb::StencilArgs S, double *gE, double *gS, double *gB) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= S.ncell) return;
+  const int n = (int)(c / S.plane);
+  const long long q = c - n * S.plane;
+  const int i = (int)(q / S.nc), j = (int)(q - (long long)i * S.nc);
+  gE[c] = j < S.nc - 1 ? 1.0 / S.L[n].rEW : 0.0;
+  gS[c] = i < S.nr - 1 ? 1.0 / S.L[n].rNS : 0.0;
+  gB[c] = n < S.nl - 1 ? 1.0 / S.L[n].rz : 0.0;
+}
+
+// fine FP64 face conductances from per-cell resistances (detailed 3-D)
+__global__ void field_faces64(const hsb::StencilArgs S, double *gE, double *gS, double *gB) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= S.ncell) return;
+  const int n = (int)(c / S.plane);
+  const long long q = c - n * S.plane;
+  const int i = (int)(q / S.nc), j = (int)(q - (long long)i * S.nc);
+  gE[c] = j < S.nc - 1 ? 1.0 / S.rE[c] : 0.0;
+  gS[c] = i < S.nr - 1 ? 1.0 / S.rS[c] : 0.0;
+  gB[c] = n < S.nl - 1 ? 1.0 / S.rB[c] : 0.0;
+}
+
+__global__ void d2f(const double *__restrict__ a, float *__restrict__ b, long long n) {
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) b[k] = (float)a[k];
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static inline unsigned nb(long long n) { return (unsigned)((n + MGT - 1) / MGT); }
+
+static MgLevelDev dev_level(const hsb_dev_model *m, const MgLevel &L, int lvl) {
+  MgLevelDev d;
+  d.nr = L.nr; d.nc = L.nc; d.nl = m->nl;
+  d.plane = L.plane; d.ncell = L.ncell;
+  d.gE = L.gE; d.gS = L.gS; d.gB = L.gB; d.diag = L.diag;
+  d.gAmbL = L.gAmbL; d.gEdgeNS = L.gEdgeNS; d.gEdgeEW = L.gEdgeEW;
+  d.spidx = m->spidx; d.hsidx = m->hsidx;
+  d.scale = (float)(1 << lvl);
+  return d;
+}
+
+static void free_mg(void *p);
+
+static int mg_setup(hsb_dev_model *m, MgWork **out) {
+  MgWork *w = new MgWork();
+  w->coef_version = -1;
+  const int nl = m->nl, nx = m->nx;
+  // levels: halve while both sides are even and >= 4 (keep >= 2x2 columns)
+  int nr = m->nr, nc = m->nc;
+  while (true) {
+    MgLevel L{};
+    L.nr = nr; L.nc = nc;
+    L.plane = (long long)nr * nc;
+    L.ncell = L.plane * nl;
+    L.n = L.ncell + nx;
+    w->lv.push_back(L);
+    if (nr < 4 || nc < 4 || (nr & 1) || (nc & 1) || L.ncell <= 4096) break;
+    nr /= 2; nc /= 2;
+  }
+  w->nlev = (int)w->lv.size();
+  for (int l = 0; l < w->nlev; l++) {
+    MgLevel &L = w->lv[l];
+    HSB_CUDA(cudaMalloc(&L.gE, sizeof(float) * L.ncell));
+    HSB_CUDA(cudaMalloc(&L.gS, sizeof(float) * L.ncell));
+    HSB_CUDA(cudaMalloc(&L.gB, sizeof(float) * L.ncell));
+    HSB_CUDA(cudaMalloc(&L.diag, sizeof(float) * L.ncell));
+    HSB_CUDA(cudaMalloc(&L.gAmbL, sizeof(float) * HSB_MAX_LAYERS));
+    HSB_CUDA(cudaMalloc(&L.gEdgeNS, sizeof(float) * HSB_MAX_LAYERS));
+    HSB_CUDA(cudaMalloc(&L.gEdgeEW, sizeof(float) * HSB_MAX_LAYERS));
+    HSB_CUDA(cudaMalloc(&L.x, sizeof(float) * L.n));
+    HSB_CUDA(cudaMalloc(&L.f, sizeof(float) * L.n));
+    HSB_CUDA(cudaMalloc(&L.r, sizeof(float) * L.n));
+  }
+  const long long n0 = w->lv[0].n, ncell = m->ncell;
+  HSB_CUDA(cudaMalloc(&w->gE64, sizeof(double) * ncell));
+  HSB_CUDA(cudaMalloc(&w->gS64, sizeof(double) * ncell));
+  HSB_CUDA(cudaMalloc(&w->gB64, sizeof(double) * ncell));
+  HSB_CUDA(cudaMalloc(&w->gAmb64, sizeof(double) * (HSB_MAX_LAYERS + 3 * NXP + NXP * NXP)));
+  HSB_CUDA(cudaMalloc(&w->gEdgeNS64, sizeof(double) * HSB_MAX_LAYERS));
+  HSB_CUDA(cudaMalloc(&w->gEdgeEW64, sizeof(double) * HSB_MAX_LAYERS));
+  HSB_CUDA(cudaMalloc(&w->r64, sizeof(double) * n0));
+  HSB_CUDA(cudaMalloc(&w->b64, sizeof(double) * n0));
+  HSB_CUDA(cudaMalloc(&w->p, sizeof(float) * n0));
+  HSB_CUDA(cudaMalloc(&w->q, sizeof(float) * n0));
+  HSB_CUDA(cudaMalloc(&w->z, sizeof(float) * n0));
+  HSB_CUDA(cudaMalloc(&w->e, sizeof(float) * n0));
+  HSB_CUDA(cudaMalloc(&w->rr, sizeof(float) * n0));
+  HSB_CUDA(cudaMalloc(&w->red, sizeof(double) * 4096));
+  HSB_CUDA(cudaMalloc(&w->d_ps, sizeof(PackSys)));
+  HSB_CUDA(cudaMallocHost(&w->h_red, sizeof(double) * 8));
+  *out = w;
+  return HSB_OK;
+}
+
+static void free_mg(void *p) {
+  MgWork *w = (MgWork *)p;
+  if (!w) return;
+  for (auto &L : w->lv) {
+    float *b[] = {L.gE, L.gS, L.gB, L.diag, L.gAmbL, L.gEdgeNS, L.gEdgeEW, L.x, L.f, L.r};
+    for (float *q : b)
+      if (q) cudaFree(q);
+  }
+  void *b2[] = {w->gE64, w->gS64, w->gB64, w->gAmb64, w->gEdgeNS64, w->gEdgeEW64, w->r64, w->b64,
+                w->p, w->q, w->z, w->e, w->rr, w->red, w->d_ps};
+  for (void *q : b2)
+    if (q) cudaFree(q);
+  if (w->h_red) cudaFreeHost(w->h_red);
+  delete w;
+}
+
+// build level operators from the device model's current conductances
+static int mg_build(hsb_dev_model *m, MgWork *w) {
+  const StencilArgs S = make_args(m, m->L0, m->nr, m->nc);
+  const int nl = m->nl;
+  const package_RC_t &pk = m->h_pk;
+  // FP64 fine faces
+  if (m->field) field_faces64<<<nb(m->ncell), MGT, 0, m->stream>>>(S, w->gE64, w->gS64, w->gB64);
+  else uniform_faces64<<<nb(m->ncell), MGT, 0, m->stream>>>(S, w->gE64, w->gS64, w->gB64);
+  // per-layer ambient and edge conductances (FP64 and per level FP32)
+  double gamb[HSB_MAX_LAYERS] = {0}, gens[HSB_MAX_LAYERS] = {0}, geew[HSB_MAX_LAYERS] = {0};
+  for (int n = 0; n < nl; n++) {
+    const LayerCoef &c = m->hostL0[n];
+    if (c.kind == LK_SINK) gamb[n] = 1.0 / c.ramb;
+    if (c.kind == LK_SINK || c.kind == LK_SPREADER) {
+      gens[n] = 1.0 / c.edgeNS;
+      geew[n] = 1.0 / c.edgeEW;
+    }
+  }
+  // package system
+  PackSys ps;
+  memset(&ps, 0, sizeof(ps));
+  double link64[NXP * NXP] = {0}, gamb_p[NXP] = {0}, ge_p[NXP] = {0};
+  for (int k = 0; k < NXP; k++) ps.elayer[k] = -1;
+  auto link = [&](int a, int b, double r) {
+    link64[a * NXP + b] += 1.0 / r;
+    link64[b * NXP + a] += 1.0 / r;
+  };
+  const int nodesC[4] = {HSB_SINK_C_N, HSB_SINK_C_S, HSB_SINK_C_W, HSB_SINK_C_E};
+  const int nodesO[4] = {HSB_SINK_N, HSB_SINK_S, HSB_SINK_W, HSB_SINK_E};
+  const int nodesS[4] = {HSB_SP_N, HSB_SP_S, HSB_SP_W, HSB_SP_E};
+  for (int s = 0; s < 4; s++) {
+    const bool y = s < 2;
+    gamb_p[nodesO[s]] = 1.0 / (pk.r_hs_per + pk.r_amb_per);
+    link(nodesO[s], nodesC[s], (y ? pk.r_hs2_y : pk.r_hs2_x) + pk.r_hs);
+    gamb_p[nodesC[s]] = 1.0 / (y ? pk.r_hs_c_per_y + pk.r_amb_c_per_y : pk.r_hs_c_per_x + pk.r_amb_c_per_x);
+    link(nodesC[s], nodesS[s], y ? pk.r_sp_per_y : pk.r_sp_per_x);
+    ps.elayer[nodesC[s]] = m->hsidx;
+    ps.eside[nodesC[s]] = s;
+    ge_p[nodesC[s]] = y ? gens[m->hsidx] : geew[m->hsidx];
+    ps.elayer[nodesS[s]] = m->spidx;
+    ps.eside[nodesS[s]] = s;
+    ge_p[nodesS[s]] = y ? gens[m->spidx] : geew[m->spidx];
+  }
+  for (int k = 0; k < NXP; k++) {
+    ps.gamb[k] = (float)gamb_p[k];
+    ps.ge0[k] = (float)ge_p[k];
+    for (int o = 0; o < NXP; o++) ps.link[k][o] = (float)link64[k * NXP + o];
+  }
+  w->ps = ps;
+  HSB_CUDA(cudaMemcpyAsync(w->d_ps, &ps, sizeof(ps), cudaMemcpyHostToDevice, m->stream));
+  double pack64[HSB_MAX_LAYERS + 3 * NXP + NXP * NXP];
+  memcpy(pack64, gamb, sizeof(double) * HSB_MAX_LAYERS);
+  memcpy(pack64 + HSB_MAX_LAYERS, ge_p, sizeof(double) * NXP);
+  memcpy(pack64 + HSB_MAX_LAYERS + NXP, gamb_p, sizeof(double) * NXP);
+  memcpy(pack64 + HSB_MAX_LAYERS + 3 * NXP, link64, sizeof(double) * NXP * NXP);
+  HSB_CUDA(cudaMemcpyAsync(w->gAmb64, pack64, sizeof(pack64), cudaMemcpyHostToDevice, m->stream));
+  HSB_CUDA(cudaMemcpyAsync(w->gEdgeNS64, gens, sizeof(double) * HSB_MAX_LAYERS, cudaMemcpyHostToDevice, m->stream));
+  HSB_CUDA(cudaMemcpyAsync(w->gEdgeEW64, geew, sizeof(double) * HSB_MAX_LAYERS, cudaMemcpyHostToDevice, m->stream));
+  // FP32 levels
+  for (int l = 0; l < w->nlev; l++) {
+    MgLevel &L = w->lv[l];
+    float ga[HSB_MAX_LAYERS], gn[HSB_MAX_LAYERS], ge[HSB_MAX_LAYERS];
+    const double mul4 = (double)(1ll << (2 * l)), mul2 = (double)(1ll << l);
+    for (int n = 0; n < nl; n++) {
+      ga[n] = (float)(gamb[n] * mul4);   // ambient per cell grows with the cell area
+      gn[n] = (float)(gens[n] * mul2);   // an edge cell spans 2^l fine edge cells
+      ge[n] = (float)(geew[n] * mul2);
+    }
+    HSB_CUDA(cudaMemcpyAsync(L.gAmbL, ga, sizeof(float) * nl, cudaMemcpyHostToDevice, m->stream));
+    HSB_CUDA(cudaMemcpyAsync(L.gEdgeNS, gn, sizeof(float) * nl, cudaMemcpyHostToDevice, m->stream));
+    HSB_CUDA(cudaMemcpyAsync(L.gEdgeEW, ge, sizeof(float) * nl, cudaMemcpyHostToDevice, m->stream));
+    if (l == 0) {
+      d2f<<<nb(L.ncell), MGT, 0, m->stream>>>(w->gE64, L.gE, L.ncell);
+      d2f<<<nb(L.ncell), MGT, 0, m->stream>>>(w->gS64, L.gS, L.ncell);
+      d2f<<<nb(L.ncell), MGT, 0, m->stream>>>(w->gB64, L.gB, L.ncell);
+    } else {
+      const MgLevel &F = w->lv[l - 1];
+      mg_coarsen<<<nb(L.ncell), MGT, 0, m->stream>>>(F.gE, F.gS, F.gB, L.gE, L.gS, L.gB, nl, L.nr, L.nc);
+    }
+    mg_diag<<<nb(L.ncell), MGT, 0, m->stream>>>(dev_level(m, L, l), L.diag);
+  }
+  HSB_CUDA(cudaGetLastError());
+  return HSB_OK;
+}
+
+static void smooth(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f, int pre, int sweeps) {
+  const MgLevel &L = w->lv[l];
+  const MgLevelDev d = dev_level(m, L, l);
+  for (int s = 0; s < sweeps; s++) {
+    if (pre) {
+      mg_zline<<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, 0);
+      mg_zline<<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, 1);
+      mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
+    } else {
+      mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
+      mg_zline<<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, 1);
+      mg_zline<<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, 0);
+    }
+  }
+}
+
+// z = V-cycle(r) on level l (x <- approximate solution of A x = f, from x = 0)
+static void vcycle(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f) {
+  const MgLevel &L = w->lv[l];
+  mg_zero<<<nb(L.n), MGT, 0, m->stream>>>(x, L.n);
+  if (l == w->nlev - 1) {
+    smooth(m, w, l, x, f, 1, 16);
+    smooth(m, w, l, x, f, 0, 16);
+    return;
+  }
+  const MgLevelDev d = dev_level(m, L, l);
+  smooth(m, w, l, x, f, 1, 2);
+  mg_apply_cells<<<nb(L.ncell), MGT, 0, m->stream>>>(d, x, L.r, f, 1);
+  mg_apply_pack<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, L.r, f, 1);
+  MgLevel &C = w->lv[l + 1];
+  mg_restrict_f<<<nb(C.n), MGT, 0, m->stream>>>(L.r, C.f, m->nl, C.nr, C.nc, m->nx);
+  vcycle(m, w, l + 1, C.x, C.f);
+  mg_prolong_add<<<nb(L.n), MGT, 0, m->stream>>>(C.x, x, m->nl, C.nr, C.nc, m->nx);
+  smooth(m, w, l, x, f, 0, 2);
+}
+
+static int dot(hsb_dev_model *m, MgWork *w, const float *a, const float *b, long long n, double *out) {
+  const int np = 296;
+  dot_partial<<<np, MGT, 0, m->stream>>>(a, b, n, w->red + 16);
+  dot_final<<<1, 256, 0, m->stream>>>(w->red + 16, np, out);
+  return HSB_OK;
+}
+
+int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
+  if (m->nx != HSB_EXTRA) return set_error(HSB_E_ARG, "the multigrid steady solver models the primary heat path only");
+  if (m->uchan_mask) return set_error(HSB_E_ARG, "advection makes the system non-symmetric: use BiCGStab");
+  MgWork *w = (MgWork *)m->mg;
+  int rc;
+  if (!w) {
+    if ((rc = mg_setup(m, &w))) return rc;
+    m->mg = w;
+    m->mg_free = free_mg;
+  }
+  if (w->coef_version != m->coef_version) {
+    if ((rc = mg_build(m, w))) return rc;
+    w->coef_version = m->coef_version;
+  }
+  const StencilArgs S = make_args(m, m->L0, m->nr, m->nc);
+  const long long n0 = m->vlen;
+  const double tol = (o && o->steady_tol > 0) ? o->steady_tol : 1e-7;
+  const int max_ref = (o && o->max_iters > 0) ? o->max_iters : 60;
+  double *T = m->ys;
+  double *gambL = w->gAmb64, *ge_p = w->gAmb64 + HSB_MAX_LAYERS, *gamb_p = ge_p + NXP;
+  double *link64 = w->gAmb64 + HSB_MAX_LAYERS + 3 * NXP;
+  build_rhs64<<<nb(n0), MGT, 0, m->stream>>>(S, m->pgrid, gambL, gamb_p, w->b64);
+  heuristic_start<<<nb(m->plane), MGT, 0, m->stream>>>(S, m->pgrid, T);
+  HSB_CUDA(cudaGetLastError());
+  const MgLevel &L0 = w->lv[0];
+  const MgLevelDev d0 = dev_level(m, L0, 0);
+  double *sc = w->red;   // [0] rz, [1] pq, [2] rz_new, [3] |e|^2, [4] max|r| bits
+  unsigned long long *maxbits = (unsigned long long *)(w->red + 4);
+  int refine = 0;
+  double rmax = 0.0, emax = 1e300;
+  for (refine = 0; refine < max_ref; refine++) {
+    // FP64 residual r = b - G T
+    HSB_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), m->stream));
+    fine_residual64<<<nb(m->ncell), MGT, 0, m->stream>>>(S, w->gE64, w->gS64, w->gB64, gambL, w->gEdgeNS64,
+                                                         w->gEdgeEW64, T, w->b64, w->r64, w->rr, maxbits);
+    pack_residual64<<<1, 384, 0, m->stream>>>(S, w->d_ps, ge_p, link64, gamb_p, T, w->b64, w->r64, w->rr, maxbits);
+    // inner FP32 PCG on G e = r, a fixed number of iterations
+    mg_zero<<<nb(n0), MGT, 0, m->stream>>>(w->e, n0);
+    const int inner = 6;
+    for (int it = 0; it < inner; it++) {
+      vcycle(m, w, 0, w->z, w->rr);
+      dot(m, w, w->rr, w->z, n0, sc + 2);
+      pcg_update_p<<<nb(n0), MGT, 0, m->stream>>>(w->p, w->z, sc, n0, it == 0);
+      shift_scalars<<<1, 1, 0, m->stream>>>(sc);
+      mg_apply_cells<<<nb(L0.ncell), MGT, 0, m->stream>>>(d0, w->p, w->q, nullptr, 0);
+      mg_apply_pack<<<1, 384, 0, m->stream>>>(d0, w->d_ps, w->p, w->q, nullptr, 0);
+      dot(m, w, w->p, w->q, n0, sc + 1);
+      pcg_update_xr<<<nb(n0), MGT, 0, m->stream>>>(w->e, w->rr, w->p, w->q, sc, n0);
+    }
+    add_correction<<<nb(n0), MGT, 0, m->stream>>>(T, w->e, n0);
+    // the l2 norm of this correction (>= its max norm, in K) decides convergence
+    dot(m, w, w->e, w->e, n0, sc + 3);
+    HSB_CUDA(cudaGetLastError());
+    HSB_CUDA(cudaMemcpyAsync(w->h_red, sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, m->stream));
+    HSB_CUDA(cudaStreamSynchronize(m->stream));
+    emax = sqrt(w->h_red[3]);
+    st->refinements += 1;
+    st->cycles += inner;
+    if (emax < tol) break;
+  }
+  // final FP64 residual for the record
+  HSB_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), m->stream));
+  fine_residual64<<<nb(m->ncell), MGT, 0, m->stream>>>(S, w->gE64, w->gS64, w->gB64, gambL, w->gEdgeNS64,
+                                                       w->gEdgeEW64, T, w->b64, w->r64, w->rr, maxbits);
+  pack_residual64<<<1, 384, 0, m->stream>>>(S, w->d_ps, ge_p, link64, gamb_p, T, w->b64, w->r64, w->rr, maxbits);
+  HSB_CUDA(cudaMemcpyAsync(w->h_red, sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, m->stream));
+  HSB_CUDA(cudaStreamSynchronize(m->stream));
+  {
+    unsigned long long bits;
+    memcpy(&bits, w->h_red + 4, sizeof(bits));
+    memcpy(&rmax, &bits, sizeof(rmax));
+  }
+  st->residual = rmax;
+  if (emax >= tol) return set_error(HSB_E_NOCONV, "multigrid steady solve did not converge");
+  return HSB_OK;
+}
+
+}  // namespace hsb

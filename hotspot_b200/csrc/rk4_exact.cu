@@ -150,6 +150,7 @@ static int rk4_step(hsb_dev_model *m, const StencilArgs &A, double *h, double *n
   double max, new_h = *h;
   stage(m, A, m->y, nullptr, 0.0, m->k1, E, EPI_STORE);   // k1 = f(y)
   st->slope_evals += 1;
+  st->launches += 1;
   do {
     *h = new_h;
     rk4_core(m, A, E, m->y, m->k1, *h, m->ytemp, nullptr);
@@ -163,6 +164,7 @@ static int rk4_step(hsb_dev_model *m, const StencilArgs &A, double *h, double *n
     HSB_CUDA(cudaStreamSynchronize(m->stream));
     max = m->h_err[0];
     st->slope_evals += 10;
+    st->launches += 10;
     st->rk4_attempts += 1;
     if (max <= RK4_PRECISION) {
       new_h = RK4_SAFETY * (*h) * pow(fabs(RK4_PRECISION / max), 0.2);

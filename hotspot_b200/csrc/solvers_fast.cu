@@ -4,12 +4,6 @@
 
 namespace hsb {
 
-int rk4_fast_interval(hsb_dev_model *, double, hsb_stats *) {
-  return set_error(HSB_E_ARG, "the fast transient form is not available in this build");
-}
-int mg_steady(hsb_dev_model *, const hsb_solver_opts *, hsb_stats *) {
-  return set_error(HSB_E_ARG, "the multigrid steady solver is not available in this build");
-}
 int bicgstab_steady(hsb_dev_model *, const hsb_solver_opts *, hsb_stats *) {
   return set_error(HSB_E_ARG, "the BiCGStab steady solver is not available in this build");
 }

@@ -79,6 +79,8 @@ typedef struct hsb_stats {
   double residual;           /* final max |r| (W) of the FP64 residual, or last GS delta */
   double sim_time;           /* simulated seconds advanced */
   double device_ms;          /* device time of the call (CUDA events) */
+  double kernel_ms;          /* device time of the solver kernels alone (CUDA events) */
+  long long launches;        /* kernels this library launched during the call */
 } hsb_stats;
 
 struct hsb_dev_model;

@@ -1,0 +1,85 @@
+"""The fast forms (HSB_FORM_FAST) against the FP64 oracle.
+
+Transient: FP32 stencil stages with FP64 state, error norm and step control
+on the device; compared with the oracle's exact FP64 replay of the
+reference (same adaptive algorithm), bar max |dT| <= 0.01 K.
+Steady: FP32 multigrid-preconditioned CG inside FP64 iterative refinement;
+compared with the converged FP64 solution of the same system by sparse
+direct LU, bar max |dT| <= 0.01 K (the solver converges far below it).
+"""
+import numpy as np
+import pytest
+
+from hotspot_b200 import FORM_FAST
+from hotspot_b200 import model as hm
+from hotspot_b200 import workloads as W
+from oracle.restatement import OracleModel
+
+pytestmark = pytest.mark.gpu
+TOL = 0.01
+
+
+def _transient(sc, steps):
+    m = hm.from_scenario(sc)
+    m.set_solver(FORM_FAST)
+    o = OracleModel(sc)
+    t, to = m.vector(o.init_temp), o.vector(o.init_temp)
+    worst = 0.0
+    for k in range(steps):
+        p = m.power_vector(sc.block_power[k])
+        m.compute_temp(p.copy(), t if k == 0 else None, sc.dt)
+        o.compute_temp(p.copy(), to if k == 0 else None, sc.dt)
+        worst = max(worst, float(np.max(np.abs(t - to))))
+    grid_err = float(np.max(np.abs(m.grid("trans") - o.grid("trans"))))
+    m.close()
+    return worst, grid_err
+
+
+@pytest.mark.parametrize("grid", [32, 64])
+def test_fast_transient_chip2d(workdir, grid):
+    sc = W.scenario_chip2d(workdir, seed=11, grid=grid, steps=40)
+    worst, grid_err = _transient(sc, sc.steps)
+    assert worst <= TOL and grid_err <= TOL
+
+
+def test_fast_transient_stack(workdir):
+    sc = W.scenario_stack3d(workdir, seed=12, grid=64, steps=20, n_blocks=16)
+    worst, grid_err = _transient(sc, sc.steps)
+    assert worst <= TOL and grid_err <= TOL
+
+
+def test_fast_transient_detailed(workdir):
+    sc = W.scenario_stack3d(workdir, seed=13, grid=32, steps=10, n_blocks=10)
+    sc.detailed_3D = True
+    worst, grid_err = _transient(sc, sc.steps)
+    assert worst <= TOL and grid_err <= TOL
+
+
+def test_fast_transient_microchannel(workdir):
+    sc = W.scenario_microchannel(workdir, seed=2, grid=32, die=2e-3, channel_w=125e-6,
+                                 channel_h=125e-6, pitch=250e-6, blocks=8)
+    sc.block_power = np.repeat(sc.block_power, 3, axis=0)
+    sc.dt = 1e-5
+    worst, grid_err = _transient(sc, 3)
+    assert worst <= TOL and grid_err <= TOL
+
+
+@pytest.mark.parametrize("builder,grid", [("chip2d", 64), ("stack3d", 64), ("detailed", 32)])
+def test_mg_steady_converged(workdir, builder, grid):
+    if builder == "chip2d":
+        sc = W.scenario_chip2d(workdir, seed=21, grid=grid, steps=2)
+    else:
+        sc = W.scenario_stack3d(workdir, seed=22, grid=grid, steps=2, n_blocks=14)
+        sc.detailed_3D = builder == "detailed"
+    m = hm.from_scenario(sc)
+    m.set_solver(FORM_FAST)
+    o = OracleModel(sc)
+    avg = m.power_vector(sc.block_power.mean(0))
+    s = m.vector()
+    m.steady(avg.copy(), s)
+    T, Tb = o.steady_direct(avg)
+    assert np.max(np.abs(s - Tb)) <= TOL
+    assert np.max(np.abs(m.grid("steady") - T)) <= TOL
+    st = m.stats()
+    assert st["refinements"] >= 1
+    m.close()
