@@ -183,6 +183,8 @@ _SIGS = {
     "hsb_free_flp_public": (None, [C.POINTER(Flp)]),
     "hsb_last_error": (C.c_char_p, []),
     "hsb_dev_last_error": (C.c_char_p, []),
+    "hsb_dev_transient_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                            C.POINTER(Stats)]),
     "hsb_abi_sizes": (C.c_int, [C.POINTER(C.c_longlong), C.c_int]),
 }
 

@@ -129,6 +129,20 @@ int gs_exact_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
 
 // fast-form solvers
 int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
+
+// the fast transient kernel on caller-provided state, power and scratch
+struct FastBuffers {
+  double *y;                 // state, ncell + nx (in/out)
+  const double *pgrid;       // grid power, ncell + nx
+  float *pf, *k1, *k2, *k3;  // ncell each
+  double *ytemp, *t1, *t2;   // ncell + nx each
+  void *layer_table;         // rk4_fast_layer_table_bytes()
+  double *es;                // 40
+  unsigned long long *err;   // 2
+  long long *cnt;            // 4
+};
+size_t rk4_fast_layer_table_bytes();
+int rk4_fast_on_buffers(hsb_dev_model *m, const FastBuffers &b, double time_elapsed, hsb_stats *st);
 int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
 int bicgstab_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
 

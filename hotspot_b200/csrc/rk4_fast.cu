@@ -495,4 +495,74 @@ int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
   return HSB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// The same kernel on buffers the caller provides (state, power, and every
+// scratch array), for the allocation-free entry point.  Nothing here
+// allocates device memory; the per-layer FP32 table is copied into the
+// caller's buffer.
+// ---------------------------------------------------------------------------
+size_t rk4_fast_layer_table_bytes() { return sizeof(LayerF) * HSB_MAX_LAYERS; }
+
+// the state can finish in the scratch buffer: copy it back when it did
+__global__ void fast_finish(const long long *__restrict__ cnt, const double *__restrict__ ytemp,
+                            double *__restrict__ y, long long n) {
+  if (cnt[2] == 0) return;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    y[k] = ytemp[k];
+}
+
+int rk4_fast_on_buffers(hsb_dev_model *m, const FastBuffers &b, double time_elapsed, hsb_stats *st) {
+  if (m->field || m->uchan_mask)
+    return set_error(HSB_E_ARG, "this entry point takes models with per-layer conductances only");
+  LayerF Lf[HSB_MAX_LAYERS];
+  for (int l = 0; l < m->nl; l++) {
+    const LayerCoef &c = m->hostL0[l];
+    Lf[l].gNS = (float)(1.0 / c.rNS);
+    Lf[l].gEW = (float)(1.0 / c.rEW);
+    Lf[l].gDown = (float)(1.0 / c.rz);
+    Lf[l].invC = c.cap != 0.0 ? (float)(1.0 / c.cap) : 0.f;
+    Lf[l].gEdgeNS = c.edgeNS != 0.0 ? (float)(1.0 / c.edgeNS) : 0.f;
+    Lf[l].gEdgeEW = c.edgeEW != 0.0 ? (float)(1.0 / c.edgeEW) : 0.f;
+    Lf[l].gAmb = c.ramb != 0.0 ? (float)(1.0 / c.ramb) : 0.f;
+    Lf[l].kind = c.kind;
+  }
+  HSB_CUDA(cudaMemcpyAsync(b.layer_table, Lf, sizeof(LayerF) * m->nl, cudaMemcpyHostToDevice, m->stream));
+  FastArgs A;
+  memset(&A, 0, sizeof(A));
+  A.S = make_args(m, m->L0, m->nr, m->nc);
+  A.spidx = m->spidx; A.hsidx = m->hsidx;
+  A.subidx = m->subidx; A.solderidx = m->solderidx; A.pcbidx = m->pcbidx;
+  A.Lf = (const LayerF *)b.layer_table;
+  A.pgrid = b.pgrid; A.pf = b.pf;
+  A.y = b.y; A.ytemp = b.ytemp; A.t1 = b.t1; A.t2 = b.t2;
+  A.k1 = b.k1; A.k2 = b.k2; A.k3 = b.k3;
+  A.es = b.es; A.err = b.err; A.cnt = b.cnt;
+  A.T = time_elapsed;
+  A.max_attempts = 10000000;
+  int per_sm = 0, nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+  HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rk4_fast_kernel<false, false>, FT_THREADS, 0));
+  const long long need = (m->plane + FT_THREADS - 1) / FT_THREADS;
+  long long g = (long long)per_sm * nsm;
+  if (g > need) g = need < 1 ? 1 : need;
+  void *args[] = {&A};
+  HSB_CUDA(cudaLaunchCooperativeKernel((const void *)rk4_fast_kernel<false, false>, dim3((unsigned)g),
+                                       dim3(FT_THREADS), args, 0, m->stream));
+  fast_finish<<<64, 256, 0, m->stream>>>(b.cnt, b.ytemp, b.y, m->vlen);
+  HSB_CUDA(cudaGetLastError());
+  long long cnt[4];
+  HSB_CUDA(cudaMemcpyAsync(cnt, b.cnt, sizeof(cnt), cudaMemcpyDeviceToHost, m->stream));
+  HSB_CUDA(cudaStreamSynchronize(m->stream));
+  if (st) {
+    st->rk4_steps += cnt[0];
+    st->rk4_attempts += cnt[1];
+    st->slope_evals += cnt[0] + 10 * cnt[1];
+    st->sim_time += time_elapsed;
+    st->launches += 2;
+  }
+  if (cnt[3]) return set_error(HSB_E_NOCONV, "fast transient: RK4 attempt cap reached");
+  return HSB_OK;
+}
+
 }  // namespace hsb

@@ -123,6 +123,25 @@ int hsb_dev_steady(hsb_dev_model *m, const double *block_power,
                    double *block_temp_out, const hsb_solver_opts *o,
                    hsb_stats *st);
 
+/* No counterpart in the reference.  For callers that may not allocate
+ * device memory while they run (a simulator that reserves its GPU memory at
+ * start-up and forbids later allocation, or a real-time loop that cannot
+ * take cudaMalloc's implicit synchronisation): one sampling interval of the
+ * fast transient form on a state y and a grid power vector pgrid that the
+ * caller owns in device memory (nl*nr*nc + n_extra doubles each, y updated
+ * in place), on the model's stream.  It calls no cudaMalloc/cudaFree: its
+ * temporaries live in one static device array (about 2.6 MB, held by every
+ * GPU that loads the library until exit) that fits models of at most
+ * HSB_NOALLOC_MAX_CELLS cells with per-layer conductances; larger or
+ * per-cell (detailed 3-D, microchannel) models are rejected with
+ * HSB_E_ARG.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race.
+ * Call with the model's device current. */
+#define HSB_NOALLOC_MAX_CELLS 65536
+int hsb_dev_transient_noalloc(hsb_dev_model *m, double *y, const double *pgrid,
+                              double time_elapsed, hsb_stats *st);
+
 /* which: 0 = transient state (last_trans), 1 = steady state (last_steady);
  * n = nl*nr*nc + n_extra doubles */
 int hsb_dev_get_state(hsb_dev_model *m, int which, double *out);
