@@ -133,6 +133,24 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class GridDesc(C.Structure):
+    """hsb_grid_desc (hsb_device.h)."""
+    _fields_ = [("nl", C.c_int), ("nr", C.c_int), ("nc", C.c_int), ("n_extra", C.c_int),
+                ("spidx", C.c_int), ("hsidx", C.c_int), ("subidx", C.c_int), ("solderidx", C.c_int),
+                ("pcbidx", C.c_int), ("field", C.c_int), ("map_mode", C.c_int), ("total_n_blocks", C.c_int),
+                ("ambient", C.c_double), ("width", C.c_double), ("height", C.c_double),
+                ("pcb_amb_num", C.c_double),
+                ("layer_rx", C.POINTER(C.c_double)), ("layer_ry", C.POINTER(C.c_double)),
+                ("layer_rz", C.POINTER(C.c_double)), ("layer_c", C.POINTER(C.c_double)),
+                ("pack", C.POINTER(C.c_double))]
+
+
+class SolverOpts(C.Structure):
+    """hsb_solver_opts (hsb_device.h)."""
+    _fields_ = [("form", C.c_int), ("steady_method", C.c_int), ("steady_tol", C.c_double),
+                ("max_iters", C.c_int)]
+
+
 _lib = None
 
 # entry points and their ctypes signatures (include/hotspot_b200.h)
@@ -183,9 +201,22 @@ _SIGS = {
     "hsb_free_flp_public": (None, [C.POINTER(Flp)]),
     "hsb_last_error": (C.c_char_p, []),
     "hsb_dev_last_error": (C.c_char_p, []),
+    "hsb_dev_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(GridDesc)]),
+    "hsb_dev_destroy": (None, [C.c_void_p]),
+    "hsb_dev_set_layers": (C.c_int, [C.c_void_p, _D, _D, _D, _D, _D, C.c_double, C.c_double, C.c_double,
+                                     C.c_double]),
+    "hsb_dev_set_cells": (C.c_int, [C.c_void_p, _D, _D, _D, _D, _D, _D, _D]),
+    "hsb_dev_set_advection": (C.c_int, [C.c_void_p, _D, _D, _D, _D, _D, _D]),
+    "hsb_dev_set_maps": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _D, _D, C.c_double,
+                                   C.POINTER(C.c_int)]),
+    "hsb_dev_transient": (C.c_int, [C.c_void_p, _D, _D, C.c_double, _D, C.POINTER(SolverOpts),
+                                    C.POINTER(Stats)]),
+    "hsb_dev_steady": (C.c_int, [C.c_void_p, _D, _D, C.POINTER(SolverOpts), C.POINTER(Stats)]),
+    "hsb_dev_get_state": (C.c_int, [C.c_void_p, C.c_int, _D]),
+    "hsb_dev_set_state": (C.c_int, [C.c_void_p, C.c_int, _D]),
+    "hsb_abi_sizes": (C.c_int, [C.POINTER(C.c_longlong), C.c_int]),
     "hsb_dev_transient_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                             C.POINTER(Stats)]),
-    "hsb_abi_sizes": (C.c_int, [C.POINTER(C.c_longlong), C.c_int]),
 }
 
 
