@@ -137,11 +137,14 @@ struct FastBuffers {
   float *pf, *k1, *k2, *k3;  // ncell each
   double *ytemp, *t1, *t2;   // ncell + nx each
   void *layer_table;         // rk4_fast_layer_table_bytes()
-  double *es;                // 40
+  void *pack_table;          // rk4_fast_pack_table_bytes()
+  double *part;              // rk4_fast_part_bytes(m): per-tile edge partial sums
   unsigned long long *err;   // 2
   long long *cnt;            // 4
 };
 size_t rk4_fast_layer_table_bytes();
+size_t rk4_fast_pack_table_bytes();
+size_t rk4_fast_part_bytes(const hsb_dev_model *m);
 int rk4_fast_on_buffers(hsb_dev_model *m, const FastBuffers &b, double time_elapsed, hsb_stats *st);
 int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
 int bicgstab_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);

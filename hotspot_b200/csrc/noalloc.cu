@@ -9,9 +9,10 @@
 // owns in device memory, and takes all of its temporaries from one
 // file-scope static device array instead of calling cudaMalloc.
 //
-// The array is hsb_noalloc_scratch below, about 2.6 MB; every GPU that
+// The array is hsb_noalloc_scratch below, about 2.8 MB; every GPU that
 // loads this library holds it until the process exits.  It fits models of
-// up to HSB_NOALLOC_MAX_CELLS grid cells.  Every call shares it and it keeps
+// up to HSB_NOALLOC_MAX_CELLS grid cells of at most 4096 rows and 16384
+// columns.  Every call shares it and it keeps
 // the previous call's contents, so calls whose work overlaps on the GPU
 // (different streams, or different host threads on one device) race; the
 // error accumulators that must start at zero are cleared by each call.
@@ -32,9 +33,12 @@ constexpr size_t kOffYt = a256(kOffK3 + sizeof(float) * kMaxCells);
 constexpr size_t kOffT1 = a256(kOffYt + sizeof(double) * kMaxVec);
 constexpr size_t kOffT2 = a256(kOffT1 + sizeof(double) * kMaxVec);
 constexpr size_t kLayerBytes = 64 * 32;
+constexpr size_t kPackBytes = 8192;
+constexpr size_t kPartBytes = sizeof(double) * 2 * 20 * 512;   // 512 tile rows or columns
 constexpr size_t kOffLt = a256(kOffT2 + sizeof(double) * kMaxVec);
-constexpr size_t kOffEs = a256(kOffLt + kLayerBytes);
-constexpr size_t kOffErr = a256(kOffEs + sizeof(double) * 40);
+constexpr size_t kOffPk = a256(kOffLt + kLayerBytes);
+constexpr size_t kOffPt = a256(kOffPk + kPackBytes);
+constexpr size_t kOffErr = a256(kOffPt + kPartBytes);
 constexpr size_t kOffCnt = a256(kOffErr + sizeof(unsigned long long) * 2);
 constexpr size_t kTotal = a256(kOffCnt + sizeof(long long) * 4);
 
@@ -76,8 +80,11 @@ extern "C" int hsb_dev_transient_noalloc(hsb_dev_model *m, double *y, const doub
   if (m->field || m->uchan_mask)
     return set_error(HSB_E_ARG, "the allocation-free entry point takes models with per-layer "
                                 "conductances only (no detailed 3-D or microchannel layers)");
-  if (rk4_fast_layer_table_bytes() > kLayerBytes)
-    return set_error(HSB_E_ARG, "layer table does not fit the static scratch");
+  if (rk4_fast_layer_table_bytes() > kLayerBytes || rk4_fast_pack_table_bytes() > kPackBytes)
+    return set_error(HSB_E_ARG, "coefficient tables do not fit the static scratch");
+  if (rk4_fast_part_bytes(m) > kPartBytes)
+    return set_error(HSB_E_ARG, "grid too elongated for the allocation-free entry point's static "
+                                "scratch (at most 4096 rows and 16384 columns)");
   int dev = -1;
   HSB_CUDA(cudaGetDevice(&dev));
   if (dev != m->device) return set_error(HSB_E_ARG, "call with the model's device current");
@@ -95,7 +102,8 @@ extern "C" int hsb_dev_transient_noalloc(hsb_dev_model *m, double *y, const doub
   b.t1 = (double *)(s + kOffT1);
   b.t2 = (double *)(s + kOffT2);
   b.layer_table = (void *)(s + kOffLt);
-  b.es = (double *)(s + kOffEs);
+  b.pack_table = (void *)(s + kOffPk);
+  b.part = (double *)(s + kOffPt);
   b.err = (unsigned long long *)(s + kOffErr);
   b.cnt = (long long *)(s + kOffCnt);
   // what the kernel reads before writing starts from zero on every call

@@ -3,22 +3,31 @@
 // The same adaptive step-doubling RK4 as the reference (RCutil.c:544-640,
 // including the reuse of k1 = f(t1) on a retry) and the same interval loop
 // (temperature_grid.c:3676-3692), run as ONE cooperative persistent kernel
-// per sampling interval:
-//   * every RK4 stage is a grid-stride pass over (i, j) columns, each thread
-//     walking the layers so vertical neighbours stay in registers; stage
-//     inputs t = y + a*k are formed on the fly (no axpy passes);
-//   * stencil arithmetic in FP32: neighbour differences are taken in FP64
-//     (y is FP64) and rounded once to FP32, slopes k are stored in FP32;
-//   * state y, the RK4 combination y + h(k1+2k2+2k3+k4)/6 and the error
-//     norm |ytemp - t2| stay in FP64;
-//   * the package nodes' edge sums are reduced by dedicated warps in a fixed
-//     order (deterministic); every CTA then evaluates the package nodes
-//     redundantly in shared memory, so one grid barrier per stage suffices;
-//   * step-size control runs on the device: each CTA reads the global
+// per sampling interval, one grid barrier per RK4 stage:
+//   * a stage works on 32x8 (j x i) tiles through all layers: one thread of
+//     the CTA issues TMA tensor copies (cp.async.bulk.tensor, completion on
+//     an mbarrier) of the tile with its one-cell halo and of every per-cell
+//     operand of the stage, all layers at once, into shared memory; each
+//     thread then evaluates its (i, j) column from shared memory (vertical
+//     neighbours included), so a stage waits on one round trip to L2/HBM;
+//   * stencil arithmetic in FP32: the stage input t = y + a*k is formed in
+//     FP64 (y is FP64) once per cell and kept as the FP32 deviation t - T_amb,
+//     slopes k are FP32;
+//   * state y, the combination y + h(k1+2k2+2k3+k4)/6 and the error norm
+//     |ytemp - t2| stay in FP64;
+//   * the package nodes' edge sums come from per-tile partials reduced in a
+//     fixed order (deterministic); every CTA evaluates the package nodes from
+//     a precomputed sparse FP64 conductance table, one lane per node, at the
+//     start of the next stage while that stage's tile copies are in flight;
+//   * step-size control runs on the device: every CTA reads the global
 //     max-norm after the barrier and takes the identical decision.
 #include <cooperative_groups.h>
+#include <cuda.h>
 
 #include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
 
 #include "stencil_exact.cuh"
 
@@ -28,7 +37,19 @@ namespace hsb {
 
 #define FT_THREADS 256
 #define FT_WARPS (FT_THREADS / 32)
+#define TJ 32                 // tile columns (j)
+#define TI 8                  // tile rows (i)
+#define NI (TI * TJ)          // cells of a tile layer, one per thread
+#define HR (TI + 2)           // halo box rows
+#define DW 36                 // FP64 halo box row: columns j0-2 .. j0+33 (x start 16-byte aligned)
+#define KW 40                 // FP32 halo box row: columns j0-4 .. j0+35
+#define DP (HR * DW)          // FP64 halo box layer
+#define KP (HR * KW)          // FP32 halo box layer
 #define NXMAX (HSB_EXTRA + HSB_EXTRA_SEC)
+#define NEDGE 20
+#define FT_MAX_LAYERS 16
+#define PK_LINKS 4
+#define WAIT_LIMIT (1 << 22)  // mbarrier polls before a tile copy is declared lost
 
 struct LayerF {
   float gNS, gEW;       // lateral conductances
@@ -38,24 +59,49 @@ struct LayerF {
   int kind;
 };
 
+// package nodes as conductances (FP64): dv_k = (ge_k * es[eidx_k] +
+// gamb_k (amb - x_k) + sum_l g[k][l] (x_nb[k][l] - x_k)) * invC_k, the
+// couplings of slope_fn_pack (temperature_grid.c:2857-3093), including its
+// one-sided solder/substrate links; every node has at most two links
+struct PackF {
+  double invC[NXMAX], gamb[NXMAX], ge[NXMAX];
+  double g[NXMAX][PK_LINKS];
+  int eidx[NXMAX];
+  int nb[NXMAX][PK_LINKS];
+};
+
+// TMA descriptors of the arrays a stage reads: halo boxes (_h) for stage
+// inputs, interior boxes (_i) for per-cell operands.  P and Q are the two
+// state buffers that swap roles (y / ytemp) as steps are accepted.
+struct Maps {
+  CUtensorMap yP_h, yP_i, yQ_h, yQ_i, t1_h, k1_h, k1_i, k2_h, k2_i, k3_h, pf_i;
+};
+
 struct FastWork {
   long long ncell;
-  int grid, coef_version;
+  int grid, coef_version, segmax;
   float *k1, *k2, *k3, *pf;
   double *ytemp, *t1, *t2;
   float *gN, *gS, *gW, *gE, *gA, *gB, *invC;
   float *aN, *aS, *aW, *aE, *aO;
   LayerF *Lf;
-  double *es;                     // [2][20] edge sums
+  PackF *pk;
+  double *part;                   // [2][NEDGE][segmax] edge partial sums
   unsigned long long *err;        // [2] max-norm bits
   long long *cnt;                 // [0]=steps [1]=attempts [2]=final buffer [3]=status
   long long *h_cnt;               // pinned mirror
+  Maps maps;
+  const double *mapP, *mapQ;      // the state buffers the maps describe
 };
 
 struct FastArgs {
-  StencilArgs S;                  // FP64 layer table and package (for the package nodes)
+  Maps M;
+  const double *bufP, *bufQ;
+  StencilArgs S;
   int spidx, hsidx, subidx, solderidx, pcbidx;
+  int segmax;
   const LayerF *Lf;
+  const PackF *pk;
   const float *gN, *gS, *gW, *gE, *gA, *gB, *invC;
   const float *aN, *aS, *aW, *aE, *aO;
   const double *qin;
@@ -63,11 +109,19 @@ struct FastArgs {
   float *pf;
   double *y, *ytemp, *t1, *t2;
   float *k1, *k2, *k3;
-  double *es;
+  double *part;
   unsigned long long *err;
   long long *cnt;
   double T;
   long long max_attempts;
+};
+
+// Layers are processed in fixed-size chunks, so that a chunk's per-cell
+// coefficient loads (detailed 3-D and microchannel models) are all issued
+// before their first use.
+template <bool FIELD, bool ADV>
+struct Chunk {
+  static constexpr int n = (FIELD || ADV) ? 1 : 4;
 };
 
 enum { M_K = 0, M_COMBINE = 1, M_COMBINE_ERR = 2 };
@@ -80,242 +134,489 @@ struct StageIO {
   double a;             // t = y + a * kin
   float *kout;          // output slope (M_K)
   double *koutp;
-  // combine
-  const float *k1, *k2;
-  const double *k1p, *k2p;
+  const double *k1p, *k2p;  // combine
   double h;
   double *yout, *youtp;
-  const double *ycmp, *ycmpp;
+  const double *ycmpp;
+  const CUtensorMap *m_yb, *m_kin, *m_k1, *m_k2, *m_yc;
 };
 
-__device__ __forceinline__ float tdiff(double ynb, double yc, float a, float knb, float kc) {
-  // (y_nb + a k_nb) - (y_c + a k_c), the FP64 part first
-  return (float)(ynb - yc) + a * (knb - kc);
+// Running control state, identical in every thread: the package-node part
+// of a stage is evaluated at the start of the NEXT stage, while that stage's
+// tile copies are in flight, and `mode` .. `ycmpp` record what is pending.
+struct Ctl {
+  int mode;             // -1: nothing pending
+  int psp;              // edge-partial slot of the pending stage
+  double h;
+  double *koutp, *youtp;
+  const double *ypb, *k1p, *k2p, *kinp, *ycmpp;
+  int ep;               // error-accumulator slot
+  int sp;               // edge-partial slot of the next stage
+  unsigned phase;       // completed tile-copy phases
+};
+
+// per-CTA shared state of the kernel (static part)
+struct Shared {
+  double yp[NXMAX], kp1[NXMAX], kp2[NXMAX], kp3[NXMAX], ytp[NXMAX], t1p[NXMAX], t2p[NXMAX];
+  double xs[2][NXMAX];  // package-node stage inputs, by partial slot
+  double es[NEDGE], wred[FT_WARPS];
+  double gmax, pmax;
+  float xsf[NXMAX];     // xs - T_amb in FP32, for the cells' edge terms
+  unsigned long long bar;
+  int lost;
+  LayerF L[FT_MAX_LAYERS];
+};
+
+// dynamic shared memory, per layer: FP64 halo box of the base state (turned
+// into the stage input t in place), FP32 halo box of k, the interior cells'
+// power and, for the combination stages, k1, k2, comparison state and base
+// state; FP32 deviations t - T_amb; then the package table
+struct DynSmem {
+  double *th;           // [nl][HR][DW]
+  float *kh;            // [nl][HR][KW]
+  float *pw, *k1, *k2;  // [nl][NI]
+  double *yc, *yb;      // [nl][NI]
+  float *d;             // [nl][HR][DW]
+  PackF *pk;
+};
+
+__host__ __device__ inline size_t al128(size_t x) { return (x + 127) & ~(size_t)127; }
+
+// byte offsets of the DynSmem arrays; returns the bytes to request (with
+// slack for aligning the base to 128 bytes, as TMA destinations need)
+__host__ __device__ inline size_t dyn_layout(int nl, size_t off[9]) {
+  size_t o = 0;
+  off[0] = o; o = al128(o + 8 * (size_t)nl * DP);
+  off[1] = o; o = al128(o + 4 * (size_t)nl * KP);
+  off[2] = o; o = al128(o + 4 * (size_t)nl * NI);
+  off[3] = o; o = al128(o + 4 * (size_t)nl * NI);
+  off[4] = o; o = al128(o + 4 * (size_t)nl * NI);
+  off[5] = o; o = al128(o + 8 * (size_t)nl * NI);
+  off[6] = o; o = al128(o + 8 * (size_t)nl * NI);
+  off[7] = o; o = al128(o + 4 * (size_t)nl * DP);
+  off[8] = o; o = al128(o + sizeof(PackF));
+  return o + 128;
 }
 
-template <bool FIELD, bool ADV, int MODE>
-__device__ __forceinline__ double stage(const FastArgs &A, cg::grid_group &grid, const StageIO &io,
-                                        int &ep, int &sp, double *xs, double *es_s, double *dv,
-                                        double *wred) {
+// ---------------------------------------------------------------------------
+// TMA and mbarrier primitives
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// 3-D tiled load of box (x, y, z=0) into shared memory; x is 16-byte aligned
+// by construction (halo boxes start 2 doubles / 4 floats left of the tile)
+__device__ __forceinline__ void tma3(void *dst, const CUtensorMap *map, int x, int y, unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(0), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// wait for the current tile-copy phase, bounded; a lost copy is recorded
+// and the kernel runs on to its end (the host reports the error)
+__device__ __forceinline__ void tile_wait(Shared &sh, Ctl &c) {
+  int it = 0;
+  while (!mbar_try_wait(&sh.bar, c.phase & 1u)) {
+    if (++it >= WAIT_LIMIT) {
+      sh.lost = 1;
+      break;
+    }
+  }
+  c.phase++;
+}
+
+__device__ __forceinline__ const CUtensorMap *halo_map(const FastArgs &A, const double *p) {
+  return p == A.bufP ? &A.M.yP_h : p == A.bufQ ? &A.M.yQ_h : &A.M.t1_h;
+}
+__device__ __forceinline__ const CUtensorMap *int_map(const FastArgs &A, const double *p) {
+  return p == A.bufP ? &A.M.yP_i : &A.M.yQ_i;
+}
+
+template <int MODE>
+__device__ __forceinline__ void issue_tile(const FastArgs &A, const StageIO &io, const DynSmem &ds,
+                                           Shared &sh, int i0, int j0) {
+  if (threadIdx.x != 0) return;
+  const unsigned nl = (unsigned)A.S.nl;
+  unsigned bytes = nl * (DP * 8 + NI * 4);
+  if (io.kin) bytes += nl * KP * 4;
+  if (MODE != M_K) bytes += nl * NI * 8;
+  if (MODE == M_COMBINE_ERR) bytes += nl * NI * 8;
+  // order the generic-proxy writes seen through the grid barrier (global)
+  // and the reads of the previous tile (shared) before the async copies
+  asm volatile("fence.proxy.async.global;\n" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  mbar_expect_tx(&sh.bar, bytes);
+  tma3(ds.th, io.m_yb, j0 - 2, i0 - 1, &sh.bar);
+  if (io.kin) tma3(ds.kh, io.m_kin, j0 - 4, i0 - 1, &sh.bar);
+  tma3(ds.pw, &A.M.pf_i, j0, i0, &sh.bar);
+  if (MODE != M_K) {
+    tma3(ds.k1, io.m_k1, j0, i0, &sh.bar);
+    tma3(ds.k2, io.m_k2, j0, i0, &sh.bar);
+  }
+  if (MODE == M_COMBINE_ERR) tma3(ds.yc, io.m_yc, j0, i0, &sh.bar);
+}
+
+// Package nodes of the pending stage: edge partial sums reduced in a fixed
+// order, then one lane of warp 0 per node.  Each package vector entry is
+// read and written by the same lane throughout the kernel, so no barrier is
+// needed after it.  Returns the package part of the error norm folded with
+// the cells' part (combination-with-error stages), else 0.
+__device__ __forceinline__ double finish_pending(const FastArgs &A, Ctl &c, Shared &sh, const DynSmem &ds) {
+  if (c.mode < 0) return 0.0;
   const StencilArgs &S = A.S;
-  const int nl = S.nl, nr = S.nr, nc = S.nc, nx = S.nx;
-  const long long plane = S.plane, ncell = S.ncell;
-  const float af = (float)io.a;
-  const bool hasK = io.kin != nullptr;
-  double errl = 0.0;
-
-  // package-node temperatures of this stage's input
-  if (threadIdx.x < nx) xs[threadIdx.x] = hasK ? io.ypb[threadIdx.x] + io.a * io.kinp[threadIdx.x]
-                                               : io.ypb[threadIdx.x];
-  __syncthreads();
-
-  // edge sums sum_k (t_k - x_node), one warp per edge, fixed order
-  {
-    const int ne = S.secondary ? 20 : 8;
-    const int gw = blockIdx.x * FT_WARPS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (gw < ne) {
-      int layer, which, node;
-      edge_desc(gw, A.spidx, A.hsidx, A.subidx, A.solderidx, A.pcbidx, &layer, &which, &node);
-      const double x = xs[node];
-      const int len = which < 2 ? nc : nr;
-      const long long base = (long long)layer * plane +
-                             (which == 0 ? 0 : which == 1 ? (long long)(nr - 1) * nc : which == 2 ? 0 : nc - 1);
-      const long long stride = which < 2 ? 1 : nc;
-      double s = 0.0;
-      for (int q = lane; q < len; q += 32) {
-        const long long c = base + q * stride;
-        const double t = hasK ? io.yb[c] + io.a * (double)io.kin[c] : io.yb[c];
-        s += t - x;
-      }
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-      if (lane == 0) A.es[sp * 20 + gw] = s;
-    }
+  const int nx = S.nx, ne = S.secondary ? NEDGE : 8;
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const int ntj = (S.nc + TJ - 1) / TJ, nti = (S.nr + TI - 1) / TI;
+  if (c.mode == M_COMBINE_ERR && tid == FT_THREADS - 1)
+    sh.gmax = __longlong_as_double((long long)(*(volatile unsigned long long *)(A.err + c.ep)));
+  for (int e = ty; e < ne; e += FT_WARPS) {
+    const int nseg = (e & 3) < 2 ? ntj : nti;
+    const double *pp = A.part + ((long long)c.psp * NEDGE + e) * A.segmax;
+    double s = 0.0;
+    for (int q = tx; q < nseg; q += 32) s += pp[q];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (tx == 0) sh.es[e] = s;
   }
-
-  // grid cells, one (i, j) column per thread iteration
-  const long long ncol = plane;
-  for (long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x; col < ncol;
-       col += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(col / nc), j = (int)(col - (long long)i * nc);
-    double yUp = 0.0, yC = io.yb[col];
-    float kUp = 0.f, kC = hasK ? io.kin[col] : 0.f;
-    for (int n = 0; n < nl; n++) {
-      const long long c = (long long)n * plane + col;
-      double yDn = 0.0;
-      float kDn = 0.f;
-      if (n < nl - 1) {
-        yDn = io.yb[c + plane];
-        kDn = hasK ? io.kin[c + plane] : 0.f;
-      }
-      const LayerF &L = A.Lf[n];
-      float psum = 0.f;
-      if (i > 0) {
-        const float g = FIELD ? A.gN[c] : L.gNS;
-        psum += g * tdiff(io.yb[c - nc], yC, af, hasK ? io.kin[c - nc] : 0.f, kC);
-      }
-      if (i < nr - 1) {
-        const float g = FIELD ? A.gS[c] : L.gNS;
-        psum += g * tdiff(io.yb[c + nc], yC, af, hasK ? io.kin[c + nc] : 0.f, kC);
-      }
-      if (j < nc - 1) {
-        const float g = FIELD ? A.gE[c] : L.gEW;
-        psum += g * tdiff(io.yb[c + 1], yC, af, hasK ? io.kin[c + 1] : 0.f, kC);
-      }
-      if (j > 0) {
-        const float g = FIELD ? A.gW[c] : L.gEW;
-        psum += g * tdiff(io.yb[c - 1], yC, af, hasK ? io.kin[c - 1] : 0.f, kC);
-      }
-      if (n > 0) {
-        const float g = FIELD ? A.gA[c] : A.Lf[n - 1].gDown;
-        psum += g * tdiff(yUp, yC, af, kUp, kC);
-      }
-      if (n < nl - 1) {
-        const float g = FIELD ? A.gB[c] : L.gDown;
-        psum += g * tdiff(yDn, yC, af, kDn, kC);
-      }
-      if (L.kind != LK_PLAIN) {
-        int eN, eS, eE, eW;
-        switch (L.kind) {
-          case LK_SPREADER: eN = HSB_SP_N; eS = HSB_SP_S; eE = HSB_SP_E; eW = HSB_SP_W; break;
-          case LK_SINK:
-            psum += L.gAmb * ((float)(S.ambient - yC) - af * kC);
-            eN = HSB_SINK_C_N; eS = HSB_SINK_C_S; eE = HSB_SINK_C_E; eW = HSB_SINK_C_W; break;
-          case LK_PCB:
-            psum += L.gAmb * ((float)(S.ambient - yC) - af * kC);
-            eN = HSB_PCB_C_N; eS = HSB_PCB_C_S; eE = HSB_PCB_C_E; eW = HSB_PCB_C_W; break;
-          case LK_SUB: eN = HSB_SUB_N; eS = HSB_SUB_S; eE = HSB_SUB_E; eW = HSB_SUB_W; break;
-          default: eN = HSB_SOLDER_N; eS = HSB_SOLDER_S; eE = HSB_SOLDER_E; eW = HSB_SOLDER_W; break;
-        }
-        if (i == 0) psum += L.gEdgeNS * ((float)(xs[eN] - yC) - af * kC);
-        if (i == nr - 1) psum += L.gEdgeNS * ((float)(xs[eS] - yC) - af * kC);
-        if (j == nc - 1) psum += L.gEdgeEW * ((float)(xs[eE] - yC) - af * kC);
-        if (j == 0) psum += L.gEdgeEW * ((float)(xs[eW] - yC) - af * kC);
-      }
-      if (ADV && ((S.uchan_mask >> n) & 1ull)) {
-        // advection carries absolute temperatures: FP64
-        const double tc = yC + io.a * (double)kC;
-        double adv = 0.0;
-        if (i > 0) adv += (double)A.aN[c] * ((io.yb[c - nc] + io.a * (double)(hasK ? io.kin[c - nc] : 0.f) + tc) / 2.0);
-        if (i < nr - 1) adv += (double)A.aS[c] * ((io.yb[c + nc] + io.a * (double)(hasK ? io.kin[c + nc] : 0.f) + tc) / 2.0);
-        if (j > 0) adv += (double)A.aW[c] * ((io.yb[c - 1] + io.a * (double)(hasK ? io.kin[c - 1] : 0.f) + tc) / 2.0);
-        if (j < nc - 1) adv += (double)A.aE[c] * ((io.yb[c + 1] + io.a * (double)(hasK ? io.kin[c + 1] : 0.f) + tc) / 2.0);
-        adv += A.qin[c] + (double)A.aO[c] * tc;
-        psum += (float)adv;
-      }
-      const float k = (A.pf[c] + psum) * (FIELD ? A.invC[c] : L.invC);
-      if (MODE == M_K) {
-        io.kout[c] = k;
+  __syncthreads();
+  if (ty == 0) {
+    double perr = 0.0;
+    if (tx < nx) {
+      const double *xs = sh.xs[c.psp];
+      const PackF &P = *ds.pk;
+      const double xq = xs[tx];
+      double s = P.gamb[tx] * (S.ambient - xq);
+      if (P.eidx[tx] >= 0) s += P.ge[tx] * sh.es[P.eidx[tx]];
+#pragma unroll
+      for (int l = 0; l < PK_LINKS; l++)
+        if (P.nb[tx][l] >= 0) s += P.g[tx][l] * (xs[P.nb[tx][l]] - xq);
+      const double d = s * P.invC[tx];
+      if (c.mode == M_K) {
+        c.koutp[tx] = d;
       } else {
-        const double yo = io.yb[c] + io.h * ((double)io.k1[c] + 2.0 * (double)io.k2[c] +
-                                             2.0 * (double)kC + (double)k) / 6.0;
-        io.yout[c] = yo;
-        if (MODE == M_COMBINE_ERR) errl = fmax(errl, fabs(io.ycmp[c] - yo));
+        const double yo = c.ypb[tx] + c.h * (c.k1p[tx] + 2.0 * c.k2p[tx] + 2.0 * c.kinp[tx] + d) / 6.0;
+        c.youtp[tx] = yo;
+        if (c.mode == M_COMBINE_ERR) perr = fabs(c.ycmpp[tx] - yo);
       }
-      yUp = yC; kUp = kC;
-      yC = yDn; kC = kDn;
+    }
+    if (c.mode == M_COMBINE_ERR) {
+      for (int o = 16; o > 0; o >>= 1) perr = fmax(perr, __shfl_down_sync(0xffffffffu, perr, o));
+      if (tx == 0) sh.pmax = perr;
     }
   }
-  if (MODE == M_COMBINE_ERR) {
-    for (int o = 16; o > 0; o >>= 1) errl = fmax(errl, __shfl_down_sync(0xffffffffu, errl, o));
-    if ((threadIdx.x & 31) == 0) wred[threadIdx.x >> 5] = errl;
+  if (c.mode == M_COMBINE_ERR) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-      double mx = wred[0];
-      for (int w = 1; w < FT_WARPS; w++) mx = fmax(mx, wred[w]);
-      atomicMax(A.err + ep, (unsigned long long)__double_as_longlong(mx));
-    }
-  }
-  grid.sync();
-
-  // package nodes, evaluated identically by every CTA
-  const int ne = S.secondary ? 20 : 8;
-  if (threadIdx.x < ne) es_s[threadIdx.x] = A.es[sp * 20 + threadIdx.x];
-  __syncthreads();
-  if (threadIdx.x == 0) pack_slope_exact(S, xs, es_s, dv, A.spidx, A.hsidx, A.subidx, A.solderidx, A.pcbidx);
-  __syncthreads();
-  double perr = 0.0;
-  if (threadIdx.x < nx) {
-    const int q = threadIdx.x;
-    if (MODE == M_K) {
-      io.koutp[q] = dv[q];
-    } else {
-      const double yo = io.ypb[q] + io.h * (io.k1p[q] + 2.0 * io.k2p[q] + 2.0 * io.kinp[q] + dv[q]) / 6.0;
-      io.youtp[q] = yo;
-      if (MODE == M_COMBINE_ERR) perr = fabs(io.ycmpp[q] - yo);
-    }
-  }
-  sp ^= 1;
-  if (MODE == M_COMBINE_ERR) {
-    // global max of the grid cells (visible after the barrier) and of the package nodes
-    for (int o = 16; o > 0; o >>= 1) perr = fmax(perr, __shfl_down_sync(0xffffffffu, perr, o));
-    __shared__ double pmax;
-    if (threadIdx.x == 0) pmax = perr;
+    const double mx = fmax(sh.gmax, sh.pmax);
+    if (blockIdx.x == 0 && tid == 0) A.err[c.ep ^ 1] = 0ull;
+    c.ep ^= 1;
     __syncthreads();
-    const double gmax = __longlong_as_double((long long)(*(volatile unsigned long long *)(A.err + ep)));
-    const double mx = fmax(gmax, pmax);
-    __syncthreads();
-    if (blockIdx.x == 0 && threadIdx.x == 0) A.err[ep ^ 1] = 0ull;
-    ep ^= 1;
     return mx;
   }
-  __syncthreads();
   return 0.0;
 }
 
-template <bool FIELD, bool ADV>
-__device__ __forceinline__ void core(const FastArgs &A, cg::grid_group &grid, const double *yb,
-                                     const double *ypb, const float *k1, const double *k1p, double h,
-                                     double *yout, double *youtp, const double *ycmp,
-                                     const double *ycmpp, double *kp2, double *kp3, int &ep, int &sp,
-                                     double *xs, double *es_s, double *dv, double *wred, double *errp) {
-  StageIO io{};
-  io.yb = yb; io.ypb = ypb;
-  io.kin = k1; io.kinp = k1p; io.a = h / 2.0; io.kout = A.k2; io.koutp = kp2;
-  stage<FIELD, ADV, M_K>(A, grid, io, ep, sp, xs, es_s, dv, wred);
-  io.kin = A.k2; io.kinp = kp2; io.a = h / 2.0; io.kout = A.k3; io.koutp = kp3;
-  stage<FIELD, ADV, M_K>(A, grid, io, ep, sp, xs, es_s, dv, wred);
-  io.kin = A.k3; io.kinp = kp3; io.a = h;
-  io.k1 = k1; io.k2 = A.k2; io.k1p = k1p; io.k2p = kp2; io.h = h;
-  io.yout = yout; io.youtp = youtp; io.ycmp = ycmp; io.ycmpp = ycmpp;
-  if (ycmp) *errp = stage<FIELD, ADV, M_COMBINE_ERR>(A, grid, io, ep, sp, xs, es_s, dv, wred);
-  else stage<FIELD, ADV, M_COMBINE>(A, grid, io, ep, sp, xs, es_s, dv, wred);
+template <bool FIELD, bool ADV, int MODE>
+__device__ __forceinline__ void stage(const FastArgs &A, cg::grid_group &grid, const StageIO &io, Ctl &c,
+                                      Shared &sh, const DynSmem &ds) {
+  constexpr int CH = Chunk<FIELD, ADV>::n;
+  const StencilArgs &S = A.S;
+  const int nl = S.nl, nr = S.nr, nc = S.nc, nx = S.nx;
+  const long long plane = S.plane;
+  const bool hasK = io.kin != nullptr;
+  const int ne = S.secondary ? NEDGE : 8;
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const double a = io.a, amb = S.ambient;
+  const int ntj = (nc + TJ - 1) / TJ, nti = (nr + TI - 1) / TI, ntiles = ntj * nti;
+  double errl = 0.0;
+
+  // positions of this thread's interior cell and halo cell (84 of the
+  // threads own one of the halo ring's cells) in the FP64 / FP32 boxes
+  const int pd_i = (ty + 1) * DW + tx + 2, pk_i = (ty + 1) * KW + tx + 4;
+  int hr = -1, hc = 0;
+  if (tid < TJ + 2) { hr = 0; hc = tid; }
+  else if (tid < 2 * (TJ + 2)) { hr = HR - 1; hc = tid - (TJ + 2); }
+  else if (tid < 2 * (TJ + 2) + TI) { hr = tid - 2 * (TJ + 2) + 1; hc = 0; }
+  else if (tid < 2 * (TJ + 2) + 2 * TI) { hr = tid - 2 * (TJ + 2) - TI + 1; hc = TJ + 1; }
+  const int pd_h = hr * DW + hc + 1, pk_h = hr * KW + hc + 3;
+
+  // first tile's copies go out before the pending package work
+  if ((int)blockIdx.x < ntiles)
+    issue_tile<MODE>(A, io, ds, sh, (blockIdx.x / ntj) * TI, (blockIdx.x % ntj) * TJ);
+  finish_pending(A, c, sh, ds);
+  // package-node temperatures of this stage's input (each lane uses the
+  // package slopes it wrote itself; published by the barrier below)
+  if (tid < nx) {
+    const double x = hasK ? io.ypb[tid] + a * io.kinp[tid] : io.ypb[tid];
+    sh.xs[c.sp][tid] = x;
+    sh.xsf[tid] = (float)(x - amb);
+  }
+  const double *xs = sh.xs[c.sp];
+
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int ti = tile / ntj, tj = tile - ti * ntj;
+    const int i0 = ti * TI, j0 = tj * TJ;
+    const int i = i0 + ty, j = j0 + tx;
+    if (tile != (int)blockIdx.x) issue_tile<MODE>(A, io, ds, sh, i0, j0);
+    tile_wait(sh, c);
+    // stage input t = y + a*k (FP64, in place) and t - T_amb (FP32); each
+    // thread its own positions
+    for (int n = 0; n < nl; n++) {
+      double *th = ds.th + n * DP;
+      float *dn = ds.d + n * DP;
+      const float *kh = ds.kh + n * KP;
+      double v = th[pd_i];
+      if (MODE != M_K) ds.yb[n * NI + tid] = v;
+      if (hasK) {
+        v = v + a * (double)kh[pk_i];
+        th[pd_i] = v;
+      }
+      dn[pd_i] = (float)(v - amb);
+      if (hr >= 0) {
+        double w = th[pd_h];
+        if (hasK) {
+          w = w + a * (double)kh[pk_h];
+          th[pd_h] = w;
+        }
+        dn[pd_h] = (float)(w - amb);
+      }
+    }
+    __syncthreads();
+    if (i < nr && j < nc) {
+      const long long coff = (long long)i * nc + j;
+      for (int n0 = 0; n0 < nl; n0 += CH) {
+        float gN[CH], gS[CH], gE[CH], gW[CH], gA[CH], gB[CH], iC[CH];
+        float aN[CH], aS[CH], aW[CH], aE[CH], aO[CH];
+        double qn[CH];
+        if (FIELD || ADV) {
+#pragma unroll
+          for (int u = 0; u < CH; u++) {
+            const long long cc = (long long)(n0 + u) * plane + coff;
+            if (n0 + u < nl) {
+              if (FIELD) {
+                gN[u] = A.gN[cc]; gS[u] = A.gS[cc]; gE[u] = A.gE[cc]; gW[u] = A.gW[cc];
+                gA[u] = A.gA[cc]; gB[u] = A.gB[cc]; iC[u] = A.invC[cc];
+              }
+              if (ADV && ((S.uchan_mask >> (n0 + u)) & 1ull)) {
+                aN[u] = A.aN[cc]; aS[u] = A.aS[cc]; aW[u] = A.aW[cc]; aE[u] = A.aE[cc]; aO[u] = A.aO[cc];
+                qn[u] = A.qin[cc];
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < CH; u++) {
+          const int n = n0 + u;
+          if (n >= nl) break;
+          const long long cc = (long long)n * plane + coff;
+          const float *dn = ds.d + n * DP;
+          const float tc = dn[pd_i];
+          const LayerF &L = sh.L[n];
+          float psum = 0.f;
+          if (i > 0) psum += (FIELD ? gN[u] : L.gNS) * (dn[pd_i - DW] - tc);
+          if (i < nr - 1) psum += (FIELD ? gS[u] : L.gNS) * (dn[pd_i + DW] - tc);
+          if (j < nc - 1) psum += (FIELD ? gE[u] : L.gEW) * (dn[pd_i + 1] - tc);
+          if (j > 0) psum += (FIELD ? gW[u] : L.gEW) * (dn[pd_i - 1] - tc);
+          if (n > 0) psum += (FIELD ? gA[u] : sh.L[n - 1].gDown) * (dn[pd_i - DP] - tc);
+          if (n < nl - 1) psum += (FIELD ? gB[u] : L.gDown) * (dn[pd_i + DP] - tc);
+          if (L.kind != LK_PLAIN) {
+            int eN, eS, eE, eW;
+            switch (L.kind) {
+              case LK_SPREADER: eN = HSB_SP_N; eS = HSB_SP_S; eE = HSB_SP_E; eW = HSB_SP_W; break;
+              case LK_SINK:
+                psum -= L.gAmb * tc;
+                eN = HSB_SINK_C_N; eS = HSB_SINK_C_S; eE = HSB_SINK_C_E; eW = HSB_SINK_C_W; break;
+              case LK_PCB:
+                psum -= L.gAmb * tc;
+                eN = HSB_PCB_C_N; eS = HSB_PCB_C_S; eE = HSB_PCB_C_E; eW = HSB_PCB_C_W; break;
+              case LK_SUB: eN = HSB_SUB_N; eS = HSB_SUB_S; eE = HSB_SUB_E; eW = HSB_SUB_W; break;
+              default: eN = HSB_SOLDER_N; eS = HSB_SOLDER_S; eE = HSB_SOLDER_E; eW = HSB_SOLDER_W; break;
+            }
+            if (i == 0) psum += L.gEdgeNS * (sh.xsf[eN] - tc);
+            if (i == nr - 1) psum += L.gEdgeNS * (sh.xsf[eS] - tc);
+            if (j == nc - 1) psum += L.gEdgeEW * (sh.xsf[eE] - tc);
+            if (j == 0) psum += L.gEdgeEW * (sh.xsf[eW] - tc);
+          }
+          if (ADV && ((S.uchan_mask >> n) & 1ull)) {
+            // advection carries absolute temperatures: FP64
+            const double *th = ds.th + n * DP;
+            const double T = th[pd_i];
+            double adv = qn[u] + (double)aO[u] * T;
+            if (i > 0) adv += (double)aN[u] * ((th[pd_i - DW] + T) / 2.0);
+            if (i < nr - 1) adv += (double)aS[u] * ((th[pd_i + DW] + T) / 2.0);
+            if (j > 0) adv += (double)aW[u] * ((th[pd_i - 1] + T) / 2.0);
+            if (j < nc - 1) adv += (double)aE[u] * ((th[pd_i + 1] + T) / 2.0);
+            psum += (float)adv;
+          }
+          const int q = n * NI + tid;
+          const float k = (ds.pw[q] + psum) * (FIELD ? iC[u] : L.invC);
+          if (MODE == M_K) {
+            io.kout[cc] = k;
+          } else {
+            const double yo = ds.yb[q] + io.h * ((double)ds.k1[q] + 2.0 * (double)ds.k2[q] +
+                                                 2.0 * (double)ds.kh[n * KP + pk_i] + (double)k) / 6.0;
+            io.yout[cc] = yo;
+            if (MODE == M_COMBINE_ERR) errl = fmax(errl, fabs(ds.yc[q] - yo));
+          }
+        }
+      }
+    }
+    // partial edge sums of (t - x_node) over this tile's share of each edge
+    const bool onN = i0 == 0, onS = i0 + TI >= nr, onW = j0 == 0, onE = j0 + TJ >= nc;
+    for (int e = ty; e < ne; e += FT_WARPS) {
+      const int side = e & 3;
+      if (!((side == 0 && onN) || (side == 1 && onS) || (side == 2 && onW) || (side == 3 && onE))) continue;
+      int layer, which, node;
+      edge_desc(e, A.spidx, A.hsidx, A.subidx, A.solderidx, A.pcbidx, &layer, &which, &node);
+      const double *th = ds.th + layer * DP;
+      double v = 0.0;
+      if (side < 2) {
+        const int r = side == 0 ? 1 : (nr - 1 - i0) + 1;
+        if (j0 + tx < nc) v = th[r * DW + tx + 2] - xs[node];
+      } else {
+        const int col = side == 2 ? 0 : nc - 1 - j0;
+        if (tx < TI && i0 + tx < nr) v = th[(tx + 1) * DW + col + 2] - xs[node];
+      }
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (tx == 0) A.part[((long long)c.sp * NEDGE + e) * A.segmax + (side < 2 ? tj : ti)] = v;
+    }
+    __syncthreads();
+  }
+  if (MODE == M_COMBINE_ERR) {
+    for (int o = 16; o > 0; o >>= 1) errl = fmax(errl, __shfl_down_sync(0xffffffffu, errl, o));
+    if (tx == 0) sh.wred[ty] = errl;
+    __syncthreads();
+    if (tid == 0) {
+      double mx = sh.wred[0];
+      for (int w = 1; w < FT_WARPS; w++) mx = fmax(mx, sh.wred[w]);
+      atomicMax(A.err + c.ep, (unsigned long long)__double_as_longlong(mx));
+    }
+  }
+  grid.sync();
+  c.mode = MODE;
+  c.psp = c.sp;
+  c.h = io.h;
+  c.koutp = io.koutp;
+  c.youtp = io.youtp;
+  c.ypb = io.ypb;
+  c.k1p = io.k1p;
+  c.k2p = io.k2p;
+  c.kinp = io.kinp;
+  c.ycmpp = io.ycmpp;
+  c.sp ^= 1;
 }
 
+// one RK4 step of size h from (yb, ypb) with k1 given (RCutil.c:544-574)
 template <bool FIELD, bool ADV>
-__global__ void __launch_bounds__(FT_THREADS) rk4_fast_kernel(FastArgs A) {
+__device__ __forceinline__ void core(const FastArgs &A, cg::grid_group &grid, const double *yb,
+                                     const double *ypb, const double *k1p, double h, double *yout,
+                                     double *youtp, const double *ycmp, const double *ycmpp, Ctl &c,
+                                     Shared &sh, const DynSmem &ds) {
+  StageIO io{};
+  io.yb = yb; io.ypb = ypb; io.m_yb = halo_map(A, yb);
+  io.kin = A.k1; io.kinp = k1p; io.m_kin = &A.M.k1_h; io.a = h / 2.0;
+  io.kout = A.k2; io.koutp = sh.kp2;
+  stage<FIELD, ADV, M_K>(A, grid, io, c, sh, ds);
+  io.kin = A.k2; io.kinp = sh.kp2; io.m_kin = &A.M.k2_h; io.a = h / 2.0;
+  io.kout = A.k3; io.koutp = sh.kp3;
+  stage<FIELD, ADV, M_K>(A, grid, io, c, sh, ds);
+  io.kin = A.k3; io.kinp = sh.kp3; io.m_kin = &A.M.k3_h; io.a = h;
+  io.k1p = k1p; io.k2p = sh.kp2; io.h = h;
+  io.m_k1 = &A.M.k1_i; io.m_k2 = &A.M.k2_i;
+  io.yout = yout; io.youtp = youtp; io.ycmpp = ycmpp;
+  if (ycmp) {
+    io.m_yc = int_map(A, ycmp);
+    stage<FIELD, ADV, M_COMBINE_ERR>(A, grid, io, c, sh, ds);
+  } else {
+    stage<FIELD, ADV, M_COMBINE>(A, grid, io, c, sh, ds);
+  }
+}
+
+static_assert(sizeof(PackF) % 8 == 0, "package table is copied as 8-byte words");
+static_assert(NI == FT_THREADS, "one thread per cell of a tile");
+static_assert(2 * (TJ + 2) + 2 * TI <= FT_THREADS, "one thread per halo cell");
+
+template <bool FIELD, bool ADV>
+__global__ void __launch_bounds__(FT_THREADS, 2) rk4_fast_kernel(const __grid_constant__ FastArgs A) {
   cg::grid_group grid = cg::this_grid();
-  __shared__ double yp[NXMAX], kp1[NXMAX], kp2[NXMAX], kp3[NXMAX], ytp[NXMAX], t1p[NXMAX], t2p[NXMAX];
-  __shared__ double xs[NXMAX], dv[NXMAX], es_s[20], wred[FT_WARPS];
+  extern __shared__ __align__(128) unsigned char dyn_raw[];
+  __shared__ Shared sh;
   const StencilArgs &S = A.S;
-  const int nx = S.nx;
+  const int nx = S.nx, nl = S.nl;
+  DynSmem ds;
+  {
+    size_t off[9];
+    dyn_layout(nl, off);
+    unsigned char *base = dyn_raw + ((128u - (smem_u32(dyn_raw) & 127u)) & 127u);
+    ds.th = (double *)(base + off[0]);
+    ds.kh = (float *)(base + off[1]);
+    ds.pw = (float *)(base + off[2]);
+    ds.k1 = (float *)(base + off[3]);
+    ds.k2 = (float *)(base + off[4]);
+    ds.yc = (double *)(base + off[5]);
+    ds.yb = (double *)(base + off[6]);
+    ds.d = (float *)(base + off[7]);
+    ds.pk = (PackF *)(base + off[8]);
+  }
+  {
+    const double *src = (const double *)A.pk;
+    double *dst = (double *)ds.pk;
+    for (int q = threadIdx.x; q < (int)(sizeof(PackF) / 8); q += blockDim.x) dst[q] = src[q];
+    if (threadIdx.x < nl) sh.L[threadIdx.x] = A.Lf[threadIdx.x];
+    if (threadIdx.x == 0) {
+      sh.lost = 0;
+      mbar_init(&sh.bar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+  }
   // FP32 power for this interval
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < S.ncell;
        c += (long long)gridDim.x * blockDim.x)
     A.pf[c] = (float)A.pgrid[c];
-  if (threadIdx.x < nx) yp[threadIdx.x] = A.y[S.ncell + threadIdx.x];
+  if (threadIdx.x < nx) sh.yp[threadIdx.x] = A.y[S.ncell + threadIdx.x];
   if (blockIdx.x == 0 && threadIdx.x == 0) { A.err[0] = 0ull; A.err[1] = 0ull; }
   grid.sync();
   double *y = A.y, *ytemp = A.ytemp;
-  int ep = 0, sp = 0;
+  Ctl c;
+  c.mode = -1;
+  c.ep = 0;
+  c.sp = 0;
+  c.phase = 0;
   long long steps = 0, attempts = 0;
   double t, h = 0.0, new_h, mx = 0.0;
   StageIO io{};
   for (t = 0, new_h = 1e-7; t < A.T && new_h >= 1e-7 * 1.0e-6; t += h) {
     h = new_h;
-    io.yb = y; io.ypb = yp; io.kin = nullptr; io.kinp = nullptr; io.a = 0.0;
-    io.kout = A.k1; io.koutp = kp1;
-    stage<FIELD, ADV, M_K>(A, grid, io, ep, sp, xs, es_s, dv, wred);     // k1 = f(y)
+    io.yb = y; io.ypb = sh.yp; io.m_yb = halo_map(A, y);
+    io.kin = nullptr; io.kinp = nullptr; io.a = 0.0;
+    io.kout = A.k1; io.koutp = sh.kp1;
+    stage<FIELD, ADV, M_K>(A, grid, io, c, sh, ds);     // k1 = f(y)
     do {
       h = new_h;
-      core<FIELD, ADV>(A, grid, y, yp, A.k1, kp1, h, ytemp, ytp, nullptr, nullptr, kp2, kp3, ep, sp,
-                       xs, es_s, dv, wred, &mx);
-      core<FIELD, ADV>(A, grid, y, yp, A.k1, kp1, h / 2.0, A.t1, t1p, nullptr, nullptr, kp2, kp3, ep,
-                       sp, xs, es_s, dv, wred, &mx);
-      io.yb = A.t1; io.ypb = t1p; io.kin = nullptr; io.kinp = nullptr; io.a = 0.0;
-      io.kout = A.k1; io.koutp = kp1;
-      stage<FIELD, ADV, M_K>(A, grid, io, ep, sp, xs, es_s, dv, wred);   // k1 = f(t1)
-      core<FIELD, ADV>(A, grid, A.t1, t1p, A.k1, kp1, h / 2.0, A.t2, t2p, ytemp, ytp, kp2, kp3, ep,
-                       sp, xs, es_s, dv, wred, &mx);
+      core<FIELD, ADV>(A, grid, y, sh.yp, sh.kp1, h, ytemp, sh.ytp, nullptr, nullptr, c, sh, ds);
+      core<FIELD, ADV>(A, grid, y, sh.yp, sh.kp1, h / 2.0, A.t1, sh.t1p, nullptr, nullptr, c, sh, ds);
+      io.yb = A.t1; io.ypb = sh.t1p; io.m_yb = &A.M.t1_h;
+      io.kin = nullptr; io.kinp = nullptr; io.a = 0.0;
+      io.kout = A.k1; io.koutp = sh.kp1;
+      stage<FIELD, ADV, M_K>(A, grid, io, c, sh, ds);   // k1 = f(t1)
+      core<FIELD, ADV>(A, grid, A.t1, sh.t1p, sh.kp1, h / 2.0, A.t2, sh.t2p, ytemp, sh.ytp, c, sh, ds);
+      mx = finish_pending(A, c, sh, ds);
+      c.mode = -1;
       attempts++;
       if (mx <= 0.01) {
         new_h = 0.95 * h * pow(fabs(0.01 / mx), 0.2);
@@ -329,27 +630,205 @@ __global__ void __launch_bounds__(FT_THREADS) rk4_fast_kernel(FastArgs A) {
     if (attempts >= A.max_attempts) break;
     // commit: the full-step result becomes the state
     double *tmp = y; y = ytemp; ytemp = tmp;
-    if (threadIdx.x < nx) yp[threadIdx.x] = ytp[threadIdx.x];
-    __syncthreads();
+    if (threadIdx.x < nx) sh.yp[threadIdx.x] = sh.ytp[threadIdx.x];
     steps++;
     new_h = new_h < A.T - t - h ? new_h : A.T - t - h;
   }
+  __syncthreads();
+  if (sh.lost && threadIdx.x == 0) {
+    // let any copy still in flight land before the CTA exits (bounded)
+    for (int it = 0; it < WAIT_LIMIT && !mbar_try_wait(&sh.bar, c.phase & 1u); it++) {
+    }
+    A.cnt[3] = 2;
+  }
   if (blockIdx.x == 0) {
-    if (threadIdx.x < nx) y[S.ncell + threadIdx.x] = yp[threadIdx.x];
+    if (threadIdx.x < nx) y[S.ncell + threadIdx.x] = sh.yp[threadIdx.x];
     if (threadIdx.x == 0) {
       A.cnt[0] = steps;
       A.cnt[1] = attempts;
       A.cnt[2] = (y == A.y) ? 0 : 1;
-      A.cnt[3] = attempts >= A.max_attempts ? 1 : 0;
+      if (attempts >= A.max_attempts) A.cnt[3] = 1;
     }
   }
+}
+
+static const void *kernel_for(bool field, bool adv) {
+  return field ? (adv ? (const void *)rk4_fast_kernel<true, true> : (const void *)rk4_fast_kernel<true, false>)
+               : (adv ? (const void *)rk4_fast_kernel<false, true> : (const void *)rk4_fast_kernel<false, false>);
+}
+
+static size_t tile_smem(int nl) {
+  size_t off[9];
+  return dyn_layout(nl, off);
+}
+
+// co-resident grid for the cooperative launch
+static int fast_grid(hsb_dev_model *m, const void *fn, int *grid) {
+  const size_t smem = tile_smem(m->nl);
+  HSB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0, nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+  HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FT_THREADS, smem));
+  if (per_sm < 1) return set_error(HSB_E_ARG, "fast transient kernel does not fit an SM");
+  const long long tiles = (long long)((m->nc + TJ - 1) / TJ) * ((m->nr + TI - 1) / TI);
+  long long g = (long long)per_sm * nsm;
+  if (g > tiles) g = tiles;
+  *grid = (int)g;
+  return HSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// tensor maps
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  });
+  return fn;
+}
+
+// [nl][nr][nc] array of doubles (f64) or floats seen as a 3-D tensor with
+// box (bx, by, nl); out-of-range box elements read as zero
+static int make_map(CUtensorMap *map, const void *base, bool f64, const hsb_dev_model *m, unsigned bx,
+                    unsigned by) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return set_error(HSB_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  if (((uintptr_t)base & 15u) != 0) return set_error(HSB_E_ARG, "fast transient buffers must be 16-byte aligned");
+  const cuuint64_t es = f64 ? 8 : 4;
+  const cuuint64_t dims[3] = {(cuuint64_t)m->nc, (cuuint64_t)m->nr, (cuuint64_t)m->nl};
+  const cuuint64_t strides[2] = {(cuuint64_t)m->nc * es, (cuuint64_t)m->nr * m->nc * es};
+  const cuuint32_t box[3] = {bx, by, (cuuint32_t)m->nl};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(map, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                         const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(HSB_E_ARG, "tensor map encoding failed for the fast transient form");
+  return HSB_OK;
+}
+
+static int check_shape(const hsb_dev_model *m) {
+  if (m->nl > FT_MAX_LAYERS) return set_error(HSB_E_ARG, "the fast transient form supports up to 16 layers");
+  if (m->nc % 4 != 0) return set_error(HSB_E_ARG, "the fast transient form needs a multiple of 4 grid columns");
+  return HSB_OK;
+}
+
+static int build_maps(Maps *M, const hsb_dev_model *m, const double *P, const double *Q, const double *t1,
+                      const float *k1, const float *k2, const float *k3, const float *pf) {
+  int rc;
+  if ((rc = make_map(&M->yP_h, P, true, m, DW, HR))) return rc;
+  if ((rc = make_map(&M->yP_i, P, true, m, TJ, TI))) return rc;
+  if ((rc = make_map(&M->yQ_h, Q, true, m, DW, HR))) return rc;
+  if ((rc = make_map(&M->yQ_i, Q, true, m, TJ, TI))) return rc;
+  if ((rc = make_map(&M->t1_h, t1, true, m, DW, HR))) return rc;
+  if ((rc = make_map(&M->k1_h, k1, false, m, KW, HR))) return rc;
+  if ((rc = make_map(&M->k1_i, k1, false, m, TJ, TI))) return rc;
+  if ((rc = make_map(&M->k2_h, k2, false, m, KW, HR))) return rc;
+  if ((rc = make_map(&M->k2_i, k2, false, m, TJ, TI))) return rc;
+  if ((rc = make_map(&M->k3_h, k3, false, m, KW, HR))) return rc;
+  if ((rc = make_map(&M->pf_i, pf, false, m, TJ, TI))) return rc;
+  return HSB_OK;
+}
+
+// FP32 layer table and FP64 package table from the model's FP64 values
+static void host_tables(const hsb_dev_model *m, LayerF *Lf, PackF *P) {
+  for (int l = 0; l < m->nl; l++) {
+    const LayerCoef &c = m->hostL0[l];
+    Lf[l].gNS = (float)(1.0 / c.rNS);
+    Lf[l].gEW = (float)(1.0 / c.rEW);
+    Lf[l].gDown = (float)(1.0 / c.rz);
+    Lf[l].invC = c.cap != 0.0 ? (float)(1.0 / c.cap) : 0.f;
+    Lf[l].gEdgeNS = c.edgeNS != 0.0 ? (float)(1.0 / c.edgeNS) : 0.f;
+    Lf[l].gEdgeEW = c.edgeEW != 0.0 ? (float)(1.0 / c.edgeEW) : 0.f;
+    Lf[l].gAmb = c.ramb != 0.0 ? (float)(1.0 / c.ramb) : 0.f;
+    Lf[l].kind = c.kind;
+  }
+  memset(P, 0, sizeof(PackF));
+  for (int k = 0; k < NXMAX; k++) {
+    P->eidx[k] = -1;
+    for (int l = 0; l < PK_LINKS; l++) P->nb[k][l] = -1;
+  }
+  const package_RC_t &pk = m->h_pk;
+  const LayerCoef *L = m->hostL0;
+  auto edge = [&](int node, int e, double R) {
+    P->eidx[node] = e;
+    P->ge[node] = 1.0 / R;
+  };
+  auto lnk = [&](int a, int b, double R) {
+    for (int l = 0; l < PK_LINKS; l++) {
+      if (P->nb[a][l] == b || P->nb[a][l] < 0) {
+        P->nb[a][l] = b;
+        P->g[a][l] += 1.0 / R;
+        return;
+      }
+    }
+  };
+  const int cN[4] = {HSB_SINK_C_N, HSB_SINK_C_S, HSB_SINK_C_W, HSB_SINK_C_E};
+  const int oN[4] = {HSB_SINK_N, HSB_SINK_S, HSB_SINK_W, HSB_SINK_E};
+  const int sN[4] = {HSB_SP_N, HSB_SP_S, HSB_SP_W, HSB_SP_E};
+  for (int s = 0; s < 4; s++) {
+    const bool y = s < 2;
+    const double r_hs2 = (y ? pk.r_hs2_y : pk.r_hs2_x) + pk.r_hs;
+    P->gamb[oN[s]] = 1.0 / (pk.r_hs_per + pk.r_amb_per);
+    lnk(oN[s], cN[s], r_hs2);
+    P->invC[oN[s]] = 1.0 / (pk.c_hs_per + pk.c_amb_per);
+    edge(cN[s], s, y ? L[m->hsidx].edgeNS : L[m->hsidx].edgeEW);
+    P->gamb[cN[s]] = 1.0 / (y ? pk.r_hs_c_per_y + pk.r_amb_c_per_y : pk.r_hs_c_per_x + pk.r_amb_c_per_x);
+    lnk(cN[s], sN[s], y ? pk.r_sp_per_y : pk.r_sp_per_x);
+    lnk(cN[s], oN[s], r_hs2);
+    P->invC[cN[s]] = 1.0 / (y ? pk.c_hs_c_per_y + pk.c_amb_c_per_y : pk.c_hs_c_per_x + pk.c_amb_c_per_x);
+    edge(sN[s], 4 + s, y ? L[m->spidx].edgeNS : L[m->spidx].edgeEW);
+    lnk(sN[s], cN[s], y ? pk.r_sp_per_y : pk.r_sp_per_x);
+    P->invC[sN[s]] = 1.0 / (y ? pk.c_sp_per_y : pk.c_sp_per_x);
+  }
+  if (m->nx > HSB_EXTRA) {
+    const int pO[4] = {HSB_PCB_N, HSB_PCB_S, HSB_PCB_W, HSB_PCB_E};
+    const int pC[4] = {HSB_PCB_C_N, HSB_PCB_C_S, HSB_PCB_C_W, HSB_PCB_C_E};
+    const int sO[4] = {HSB_SOLDER_N, HSB_SOLDER_S, HSB_SOLDER_W, HSB_SOLDER_E};
+    const int bO[4] = {HSB_SUB_N, HSB_SUB_S, HSB_SUB_W, HSB_SUB_E};
+    for (int s = 0; s < 4; s++) {
+      const bool y = s < 2;
+      const double r_p2 = (y ? pk.r_pcb2_y : pk.r_pcb2_x) + pk.r_pcb;
+      P->gamb[pO[s]] = 1.0 / pk.r_amb_sec_per;
+      lnk(pO[s], pC[s], r_p2);
+      P->invC[pO[s]] = 1.0 / (pk.c_pcb_per + pk.c_amb_sec_per);
+      edge(pC[s], 8 + s, y ? L[m->pcbidx].edgeNS : L[m->pcbidx].edgeEW);
+      P->gamb[pC[s]] = 1.0 / (y ? pk.r_amb_sec_c_per_y : pk.r_amb_sec_c_per_x);
+      lnk(pC[s], sO[s], y ? pk.r_pcb_c_per_y : pk.r_pcb_c_per_x);
+      lnk(pC[s], pO[s], r_p2);
+      P->invC[pC[s]] = 1.0 / (y ? pk.c_pcb_c_per_y + pk.c_amb_sec_c_per_y : pk.c_pcb_c_per_x + pk.c_amb_sec_c_per_x);
+      edge(sO[s], 12 + s, y ? L[m->solderidx].edgeNS : L[m->solderidx].edgeEW);
+      lnk(sO[s], pC[s], y ? pk.r_pcb_c_per_y : pk.r_pcb_c_per_x);
+      P->invC[sO[s]] = 1.0 / (y ? pk.c_solder_per_y : pk.c_solder_per_x);
+      edge(bO[s], 16 + s, y ? L[m->subidx].edgeNS : L[m->subidx].edgeEW);
+      lnk(bO[s], sO[s], y ? pk.r_solder_per_y : pk.r_solder_per_x);
+      P->invC[bO[s]] = 1.0 / (y ? pk.c_sub_per_y : pk.c_sub_per_x);
+    }
+  }
+}
+
+static int segmax_of(const hsb_dev_model *m) {
+  const int ntj = (m->nc + TJ - 1) / TJ, nti = (m->nr + TI - 1) / TI;
+  return ntj > nti ? ntj : nti;
 }
 
 static void free_fast(void *p) {
   FastWork *w = (FastWork *)p;
   if (!w) return;
   void *bufs[] = {w->k1, w->k2, w->k3, w->pf, w->ytemp, w->t1, w->t2, w->gN, w->gS, w->gW, w->gE,
-                  w->gA, w->gB, w->invC, w->aN, w->aS, w->aW, w->aE, w->aO, w->Lf, w->es, w->err, w->cnt};
+                  w->gA, w->gB, w->invC, w->aN, w->aS, w->aW, w->aE, w->aO, w->Lf, w->pk, w->part,
+                  w->err, w->cnt};
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (w->h_cnt) cudaFreeHost(w->h_cnt);
@@ -369,6 +848,8 @@ __global__ void to_float(const double *__restrict__ r, float *__restrict__ g, lo
 static int fast_prepare(hsb_dev_model *m, FastWork **out) {
   FastWork *w = (FastWork *)m->fast;
   const long long n = m->ncell;
+  int rc;
+  if ((rc = check_shape(m))) return rc;
   if (!w) {
     w = new FastWork();
     memset(w, 0, sizeof(*w));
@@ -376,6 +857,7 @@ static int fast_prepare(hsb_dev_model *m, FastWork **out) {
     w->coef_version = -1;
     m->fast = w;
     m->fast_free = free_fast;
+    w->segmax = segmax_of(m);
     HSB_CUDA(cudaMalloc(&w->k1, sizeof(float) * n));
     HSB_CUDA(cudaMalloc(&w->k2, sizeof(float) * n));
     HSB_CUDA(cudaMalloc(&w->k3, sizeof(float) * n));
@@ -384,40 +866,29 @@ static int fast_prepare(hsb_dev_model *m, FastWork **out) {
     HSB_CUDA(cudaMalloc(&w->t1, sizeof(double) * m->vlen));
     HSB_CUDA(cudaMalloc(&w->t2, sizeof(double) * m->vlen));
     HSB_CUDA(cudaMalloc(&w->Lf, sizeof(LayerF) * HSB_MAX_LAYERS));
-    HSB_CUDA(cudaMalloc(&w->es, sizeof(double) * 40));
+    HSB_CUDA(cudaMalloc(&w->pk, sizeof(PackF)));
+    HSB_CUDA(cudaMalloc(&w->part, sizeof(double) * 2 * NEDGE * w->segmax));
     HSB_CUDA(cudaMalloc(&w->err, sizeof(unsigned long long) * 2));
     HSB_CUDA(cudaMalloc(&w->cnt, sizeof(long long) * 4));
     HSB_CUDA(cudaMallocHost(&w->h_cnt, sizeof(long long) * 4));
-    int per_sm = 0, nsm = 0, dev = m->device;
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const bool adv = m->uchan_mask != 0;
-    const void *fn = m->field ? (adv ? (const void *)rk4_fast_kernel<true, true> : (const void *)rk4_fast_kernel<true, false>)
-                              : (adv ? (const void *)rk4_fast_kernel<false, true> : (const void *)rk4_fast_kernel<false, false>);
-    HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FT_THREADS, 0));
-    const long long need = (m->plane + FT_THREADS - 1) / FT_THREADS;
-    long long g = (long long)per_sm * nsm;
-    if (g > need) g = need < 1 ? 1 : need;
-    w->grid = (int)g;
+  }
+  // the maps describe the two state buffers whichever role each has now
+  const bool same = (w->mapP == m->y && w->mapQ == w->ytemp) || (w->mapP == w->ytemp && w->mapQ == m->y);
+  if (!same) {
+    if ((rc = build_maps(&w->maps, m, m->y, w->ytemp, w->t1, w->k1, w->k2, w->k3, w->pf))) return rc;
+    w->mapP = m->y;
+    w->mapQ = w->ytemp;
   }
   if (w->coef_version == m->coef_version) {
     *out = w;
     return HSB_OK;
   }
   w->coef_version = m->coef_version;
-  // per-layer FP32 coefficients from the FP64 table
   LayerF Lf[HSB_MAX_LAYERS];
-  for (int l = 0; l < m->nl; l++) {
-    const LayerCoef &c = m->hostL0[l];
-    Lf[l].gNS = (float)(1.0 / c.rNS);
-    Lf[l].gEW = (float)(1.0 / c.rEW);
-    Lf[l].gDown = (float)(1.0 / c.rz);
-    Lf[l].invC = c.cap != 0.0 ? (float)(1.0 / c.cap) : 0.f;
-    Lf[l].gEdgeNS = c.edgeNS != 0.0 ? (float)(1.0 / c.edgeNS) : 0.f;
-    Lf[l].gEdgeEW = c.edgeEW != 0.0 ? (float)(1.0 / c.edgeEW) : 0.f;
-    Lf[l].gAmb = c.ramb != 0.0 ? (float)(1.0 / c.ramb) : 0.f;
-    Lf[l].kind = c.kind;
-  }
+  PackF P;
+  host_tables(m, Lf, &P);
   HSB_CUDA(cudaMemcpyAsync(w->Lf, Lf, sizeof(LayerF) * m->nl, cudaMemcpyHostToDevice, m->stream));
+  HSB_CUDA(cudaMemcpyAsync(w->pk, &P, sizeof(PackF), cudaMemcpyHostToDevice, m->stream));
   const int T = 256;
   const unsigned B = (unsigned)((n + T - 1) / T);
   if (m->field) {
@@ -439,7 +910,23 @@ static int fast_prepare(hsb_dev_model *m, FastWork **out) {
     }
   }
   HSB_CUDA(cudaGetLastError());
+  // a re-uploaded model may have switched between per-layer and per-cell values
+  if ((rc = fast_grid(m, kernel_for(m->field, m->uchan_mask != 0), &w->grid))) return rc;
   *out = w;
+  return HSB_OK;
+}
+
+static void fill_common(FastArgs &A, const hsb_dev_model *m) {
+  A.S = make_args(m, m->L0, m->nr, m->nc);
+  A.spidx = m->spidx; A.hsidx = m->hsidx;
+  A.subidx = m->subidx; A.solderidx = m->solderidx; A.pcbidx = m->pcbidx;
+  A.segmax = segmax_of(m);
+  A.max_attempts = 10000000;
+}
+
+static int status_error(long long status) {
+  if (status == 1) return set_error(HSB_E_NOCONV, "fast transient: RK4 attempt cap reached");
+  if (status == 2) return set_error(HSB_E_CUDA, "fast transient: a tile copy did not complete in time");
   return HSB_OK;
 }
 
@@ -449,28 +936,28 @@ int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
   if ((rc = fast_prepare(m, &w))) return rc;
   FastArgs A;
   memset(&A, 0, sizeof(A));
-  A.S = make_args(m, m->L0, m->nr, m->nc);
-  A.spidx = m->spidx; A.hsidx = m->hsidx;
-  A.subidx = m->subidx; A.solderidx = m->solderidx; A.pcbidx = m->pcbidx;
+  fill_common(A, m);
+  A.M = w->maps;
+  A.bufP = w->mapP;
+  A.bufQ = w->mapQ;
   A.Lf = w->Lf;
+  A.pk = w->pk;
   A.gN = w->gN; A.gS = w->gS; A.gW = w->gW; A.gE = w->gE; A.gA = w->gA; A.gB = w->gB;
   A.invC = w->invC;
   A.aN = w->aN; A.aS = w->aS; A.aW = w->aW; A.aE = w->aE; A.aO = w->aO; A.qin = m->qin;
   A.pgrid = m->pgrid; A.pf = w->pf;
   A.y = m->y; A.ytemp = w->ytemp; A.t1 = w->t1; A.t2 = w->t2;
   A.k1 = w->k1; A.k2 = w->k2; A.k3 = w->k3;
-  A.es = w->es; A.err = w->err; A.cnt = w->cnt;
+  A.part = w->part; A.err = w->err; A.cnt = w->cnt;
   A.T = time_elapsed;
-  A.max_attempts = 10000000;
+  HSB_CUDA(cudaMemsetAsync(w->cnt, 0, sizeof(long long) * 4, m->stream));
   void *args[] = {&A};
-  const bool adv = m->uchan_mask != 0;
-  const void *fn = m->field ? (adv ? (const void *)rk4_fast_kernel<true, true> : (const void *)rk4_fast_kernel<true, false>)
-                            : (adv ? (const void *)rk4_fast_kernel<false, true> : (const void *)rk4_fast_kernel<false, false>);
+  const void *fn = kernel_for(m->field, m->uchan_mask != 0);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, m->stream);
-  HSB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(w->grid), dim3(FT_THREADS), args, 0, m->stream));
+  HSB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(w->grid), dim3(FT_THREADS), args, tile_smem(m->nl), m->stream));
   cudaEventRecord(e1, m->stream);
   HSB_CUDA(cudaMemcpyAsync(w->h_cnt, w->cnt, sizeof(long long) * 4, cudaMemcpyDeviceToHost, m->stream));
   HSB_CUDA(cudaStreamSynchronize(m->stream));
@@ -491,17 +978,18 @@ int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
   st->rk4_attempts += w->h_cnt[1];
   st->slope_evals += w->h_cnt[0] + 10 * w->h_cnt[1];
   st->sim_time += time_elapsed;
-  if (w->h_cnt[3]) return set_error(HSB_E_NOCONV, "fast transient: RK4 attempt cap reached");
-  return HSB_OK;
+  return status_error(w->h_cnt[3]);
 }
 
 // ---------------------------------------------------------------------------
 // The same kernel on buffers the caller provides (state, power, and every
 // scratch array), for the allocation-free entry point.  Nothing here
-// allocates device memory; the per-layer FP32 table is copied into the
-// caller's buffer.
+// allocates device memory; the layer and package tables are copied into the
+// caller's buffers and the tensor maps are encoded on the host per call.
 // ---------------------------------------------------------------------------
 size_t rk4_fast_layer_table_bytes() { return sizeof(LayerF) * HSB_MAX_LAYERS; }
+size_t rk4_fast_pack_table_bytes() { return sizeof(PackF); }
+size_t rk4_fast_part_bytes(const hsb_dev_model *m) { return sizeof(double) * 2 * NEDGE * segmax_of(m); }
 
 // the state can finish in the scratch buffer: copy it back when it did
 __global__ void fast_finish(const long long *__restrict__ cnt, const double *__restrict__ ytemp,
@@ -515,40 +1003,31 @@ __global__ void fast_finish(const long long *__restrict__ cnt, const double *__r
 int rk4_fast_on_buffers(hsb_dev_model *m, const FastBuffers &b, double time_elapsed, hsb_stats *st) {
   if (m->field || m->uchan_mask)
     return set_error(HSB_E_ARG, "this entry point takes models with per-layer conductances only");
-  LayerF Lf[HSB_MAX_LAYERS];
-  for (int l = 0; l < m->nl; l++) {
-    const LayerCoef &c = m->hostL0[l];
-    Lf[l].gNS = (float)(1.0 / c.rNS);
-    Lf[l].gEW = (float)(1.0 / c.rEW);
-    Lf[l].gDown = (float)(1.0 / c.rz);
-    Lf[l].invC = c.cap != 0.0 ? (float)(1.0 / c.cap) : 0.f;
-    Lf[l].gEdgeNS = c.edgeNS != 0.0 ? (float)(1.0 / c.edgeNS) : 0.f;
-    Lf[l].gEdgeEW = c.edgeEW != 0.0 ? (float)(1.0 / c.edgeEW) : 0.f;
-    Lf[l].gAmb = c.ramb != 0.0 ? (float)(1.0 / c.ramb) : 0.f;
-    Lf[l].kind = c.kind;
-  }
-  HSB_CUDA(cudaMemcpyAsync(b.layer_table, Lf, sizeof(LayerF) * m->nl, cudaMemcpyHostToDevice, m->stream));
+  int rc;
+  if ((rc = check_shape(m))) return rc;
   FastArgs A;
   memset(&A, 0, sizeof(A));
-  A.S = make_args(m, m->L0, m->nr, m->nc);
-  A.spidx = m->spidx; A.hsidx = m->hsidx;
-  A.subidx = m->subidx; A.solderidx = m->solderidx; A.pcbidx = m->pcbidx;
+  if ((rc = build_maps(&A.M, m, b.y, b.ytemp, b.t1, b.k1, b.k2, b.k3, b.pf))) return rc;
+  LayerF Lf[HSB_MAX_LAYERS];
+  PackF P;
+  host_tables(m, Lf, &P);
+  HSB_CUDA(cudaMemcpyAsync(b.layer_table, Lf, sizeof(LayerF) * m->nl, cudaMemcpyHostToDevice, m->stream));
+  HSB_CUDA(cudaMemcpyAsync(b.pack_table, &P, sizeof(PackF), cudaMemcpyHostToDevice, m->stream));
+  fill_common(A, m);
+  A.bufP = b.y;
+  A.bufQ = b.ytemp;
   A.Lf = (const LayerF *)b.layer_table;
+  A.pk = (const PackF *)b.pack_table;
   A.pgrid = b.pgrid; A.pf = b.pf;
   A.y = b.y; A.ytemp = b.ytemp; A.t1 = b.t1; A.t2 = b.t2;
   A.k1 = b.k1; A.k2 = b.k2; A.k3 = b.k3;
-  A.es = b.es; A.err = b.err; A.cnt = b.cnt;
+  A.part = b.part; A.err = b.err; A.cnt = b.cnt;
   A.T = time_elapsed;
-  A.max_attempts = 10000000;
-  int per_sm = 0, nsm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
-  HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rk4_fast_kernel<false, false>, FT_THREADS, 0));
-  const long long need = (m->plane + FT_THREADS - 1) / FT_THREADS;
-  long long g = (long long)per_sm * nsm;
-  if (g > need) g = need < 1 ? 1 : need;
+  int g = 0;
+  const void *fn = kernel_for(false, false);
+  if ((rc = fast_grid(m, fn, &g))) return rc;
   void *args[] = {&A};
-  HSB_CUDA(cudaLaunchCooperativeKernel((const void *)rk4_fast_kernel<false, false>, dim3((unsigned)g),
-                                       dim3(FT_THREADS), args, 0, m->stream));
+  HSB_CUDA(cudaLaunchCooperativeKernel(fn, dim3((unsigned)g), dim3(FT_THREADS), args, tile_smem(m->nl), m->stream));
   fast_finish<<<64, 256, 0, m->stream>>>(b.cnt, b.ytemp, b.y, m->vlen);
   HSB_CUDA(cudaGetLastError());
   long long cnt[4];
@@ -561,8 +1040,7 @@ int rk4_fast_on_buffers(hsb_dev_model *m, const FastBuffers &b, double time_elap
     st->sim_time += time_elapsed;
     st->launches += 2;
   }
-  if (cnt[3]) return set_error(HSB_E_NOCONV, "fast transient: RK4 attempt cap reached");
-  return HSB_OK;
+  return status_error(cnt[3]);
 }
 
 }  // namespace hsb

@@ -130,9 +130,10 @@ int hsb_dev_steady(hsb_dev_model *m, const double *block_power,
  * fast transient form on a state y and a grid power vector pgrid that the
  * caller owns in device memory (nl*nr*nc + n_extra doubles each, y updated
  * in place), on the model's stream.  It calls no cudaMalloc/cudaFree: its
- * temporaries live in one static device array (about 2.6 MB, held by every
+ * temporaries live in one static device array (about 2.8 MB, held by every
  * GPU that loads the library until exit) that fits models of at most
- * HSB_NOALLOC_MAX_CELLS cells with per-layer conductances; larger or
+ * HSB_NOALLOC_MAX_CELLS cells, 4096 rows and 16384 columns, with per-layer
+ * conductances; larger, more elongated or
  * per-cell (detailed 3-D, microchannel) models are rejected with
  * HSB_E_ARG.  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress), so make that first call before any stream
