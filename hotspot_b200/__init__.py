@@ -7,6 +7,6 @@ benchmark inputs in the reference's file formats (:mod:`.workloads`), and the
 batch and serving layers.
 """
 from . import _abi  # noqa: F401
-from ._abi import FORM_FAST, FORM_PARITY, HotspotError, lib  # noqa: F401
+from ._abi import FORM_FAST, FORM_FAST_STAGES, FORM_PARITY, HotspotError, lib  # noqa: F401
 
-__all__ = ["lib", "FORM_PARITY", "FORM_FAST", "HotspotError"]
+__all__ = ["lib", "FORM_PARITY", "FORM_FAST", "FORM_FAST_STAGES", "HotspotError"]

@@ -18,7 +18,7 @@ STR = 512
 EXTRA, EXTRA_SEC = 12, 16
 
 # solver forms / methods (hsb_device.h)
-FORM_PARITY, FORM_FAST = 0, 1
+FORM_PARITY, FORM_FAST, FORM_FAST_STAGES = 0, 1, 2
 STEADY_AUTO, STEADY_GS_REPLAY, STEADY_MG, STEADY_BICGSTAB = 0, 1, 2, 3
 
 
@@ -127,7 +127,7 @@ class Stats(C.Structure):
                 ("slope_evals", C.c_longlong), ("sweeps", C.c_longlong),
                 ("cycles", C.c_longlong), ("refinements", C.c_longlong),
                 ("residual", C.c_double), ("sim_time", C.c_double), ("device_ms", C.c_double),
-                ("kernel_ms", C.c_double), ("launches", C.c_longlong)]
+                ("kernel_ms", C.c_double), ("launches", C.c_longlong), ("fallbacks", C.c_longlong)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

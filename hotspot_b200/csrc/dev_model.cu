@@ -442,8 +442,9 @@ int hsb_dev_transient(hsb_dev_model *m, const double *block_power, const double 
     st->launches += 1;
   }
   const int form = o ? o->form : HSB_FORM_PARITY;
-  rc = form == HSB_FORM_FAST ? rk4_fast_interval(m, time_elapsed, st)
-                             : rk4_exact_interval(m, time_elapsed, st);
+  rc = form == HSB_FORM_FAST          ? rk4_fast_interval(m, time_elapsed, st)
+       : form == HSB_FORM_FAST_STAGES ? rk4_fast_stages_interval(m, time_elapsed, st)
+                                      : rk4_exact_interval(m, time_elapsed, st);
   if (rc) return rc;
   if (block_temp_out) {
     if ((rc = g2b(m, m->y, m->blk_out))) return rc;
@@ -482,7 +483,7 @@ int hsb_dev_steady(hsb_dev_model *m, const double *block_power, double *block_te
   int method = o->steady_method;
   if (method == HSB_STEADY_AUTO) {
     if (m->uchan_mask) method = HSB_STEADY_BICGSTAB;
-    else if (o->form == HSB_FORM_FAST && m->nx == HSB_EXTRA) method = HSB_STEADY_MG;
+    else if (o->form != HSB_FORM_PARITY && m->nx == HSB_EXTRA) method = HSB_STEADY_MG;
     else method = HSB_STEADY_GS_REPLAY;
   }
   if (method == HSB_STEADY_GS_REPLAY && m->uchan_mask)

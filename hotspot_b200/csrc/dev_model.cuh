@@ -129,6 +129,7 @@ int gs_exact_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
 
 // fast-form solvers
 int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
+int rk4_fast_stages_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
 
 // the fast transient kernel on caller-provided state, power and scratch
 struct FastBuffers {

@@ -21,78 +21,11 @@
 //     start of the next stage while that stage's tile copies are in flight;
 //   * step-size control runs on the device: every CTA reads the global
 //     max-norm after the barrier and takes the identical decision.
-#include <cooperative_groups.h>
-#include <cuda.h>
-
-#include <cmath>
-#include <cstdint>
-#include <cstring>
-#include <mutex>
-
-#include "stencil_exact.cuh"
+#include "fast_common.cuh"
 
 namespace cg = cooperative_groups;
 
 namespace hsb {
-
-#define FT_THREADS 256
-#define FT_WARPS (FT_THREADS / 32)
-#define TJ 32                 // tile columns (j)
-#define TI 8                  // tile rows (i)
-#define NI (TI * TJ)          // cells of a tile layer, one per thread
-#define HR (TI + 2)           // halo box rows
-#define DW 36                 // FP64 halo box row: columns j0-2 .. j0+33 (x start 16-byte aligned)
-#define KW 40                 // FP32 halo box row: columns j0-4 .. j0+35
-#define DP (HR * DW)          // FP64 halo box layer
-#define KP (HR * KW)          // FP32 halo box layer
-#define NXMAX (HSB_EXTRA + HSB_EXTRA_SEC)
-#define NEDGE 20
-#define FT_MAX_LAYERS 16
-#define PK_LINKS 4
-#define WAIT_LIMIT (1 << 22)  // mbarrier polls before a tile copy is declared lost
-
-struct LayerF {
-  float gNS, gEW;       // lateral conductances
-  float gDown;          // conductance to layer n+1 (1/rz[n])
-  float invC;           // 1 / capacitance
-  float gEdgeNS, gEdgeEW, gAmb;
-  int kind;
-};
-
-// package nodes as conductances (FP64): dv_k = (ge_k * es[eidx_k] +
-// gamb_k (amb - x_k) + sum_l g[k][l] (x_nb[k][l] - x_k)) * invC_k, the
-// couplings of slope_fn_pack (temperature_grid.c:2857-3093), including its
-// one-sided solder/substrate links; every node has at most two links
-struct PackF {
-  double invC[NXMAX], gamb[NXMAX], ge[NXMAX];
-  double g[NXMAX][PK_LINKS];
-  int eidx[NXMAX];
-  int nb[NXMAX][PK_LINKS];
-};
-
-// TMA descriptors of the arrays a stage reads: halo boxes (_h) for stage
-// inputs, interior boxes (_i) for per-cell operands.  P and Q are the two
-// state buffers that swap roles (y / ytemp) as steps are accepted.
-struct Maps {
-  CUtensorMap yP_h, yP_i, yQ_h, yQ_i, t1_h, k1_h, k1_i, k2_h, k2_i, k3_h, pf_i;
-};
-
-struct FastWork {
-  long long ncell;
-  int grid, coef_version, segmax;
-  float *k1, *k2, *k3, *pf;
-  double *ytemp, *t1, *t2;
-  float *gN, *gS, *gW, *gE, *gA, *gB, *invC;
-  float *aN, *aS, *aW, *aE, *aO;
-  LayerF *Lf;
-  PackF *pk;
-  double *part;                   // [2][NEDGE][segmax] edge partial sums
-  unsigned long long *err;        // [2] max-norm bits
-  long long *cnt;                 // [0]=steps [1]=attempts [2]=final buffer [3]=status
-  long long *h_cnt;               // pinned mirror
-  Maps maps;
-  const double *mapP, *mapQ;      // the state buffers the maps describe
-};
 
 struct FastArgs {
   Maps M;
@@ -112,16 +45,8 @@ struct FastArgs {
   double *part;
   unsigned long long *err;
   long long *cnt;
-  double T;
+  double T, h0;
   long long max_attempts;
-};
-
-// Layers are processed in fixed-size chunks, so that a chunk's per-cell
-// coefficient loads (detailed 3-D and microchannel models) are all issued
-// before their first use.
-template <bool FIELD, bool ADV>
-struct Chunk {
-  static constexpr int n = (FIELD || ADV) ? 1 : 4;
 };
 
 enum { M_K = 0, M_COMBINE = 1, M_COMBINE_ERR = 2 };
@@ -180,7 +105,6 @@ struct DynSmem {
   PackF *pk;
 };
 
-__host__ __device__ inline size_t al128(size_t x) { return (x + 127) & ~(size_t)127; }
 
 // byte offsets of the DynSmem arrays; returns the bytes to request (with
 // slack for aligning the base to 128 bytes, as TMA destinations need)
@@ -198,36 +122,6 @@ __host__ __device__ inline size_t dyn_layout(int nl, size_t off[9]) {
   return o + 128;
 }
 
-// ---------------------------------------------------------------------------
-// TMA and mbarrier primitives
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// 3-D tiled load of box (x, y, z=0) into shared memory; x is 16-byte aligned
-// by construction (halo boxes start 2 doubles / 4 floats left of the tile)
-__device__ __forceinline__ void tma3(void *dst, const CUtensorMap *map, int x, int y, unsigned long long *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(0), "r"(smem_u32(bar))
-      : "memory");
-}
 
 // wait for the current tile-copy phase, bounded; a lost copy is recorded
 // and the kernel runs on to its end (the host reports the error)
@@ -547,10 +441,6 @@ __device__ __forceinline__ void core(const FastArgs &A, cg::grid_group &grid, co
   }
 }
 
-static_assert(sizeof(PackF) % 8 == 0, "package table is copied as 8-byte words");
-static_assert(NI == FT_THREADS, "one thread per cell of a tile");
-static_assert(2 * (TJ + 2) + 2 * TI <= FT_THREADS, "one thread per halo cell");
-
 template <bool FIELD, bool ADV>
 __global__ void __launch_bounds__(FT_THREADS, 2) rk4_fast_kernel(const __grid_constant__ FastArgs A) {
   cg::grid_group grid = cg::this_grid();
@@ -600,7 +490,7 @@ __global__ void __launch_bounds__(FT_THREADS, 2) rk4_fast_kernel(const __grid_co
   long long steps = 0, attempts = 0;
   double t, h = 0.0, new_h, mx = 0.0;
   StageIO io{};
-  for (t = 0, new_h = 1e-7; t < A.T && new_h >= 1e-7 * 1.0e-6; t += h) {
+  for (t = 0, new_h = A.h0; t < A.T && new_h >= 1e-7 * 1.0e-6; t += h) {
     h = new_h;
     io.yb = y; io.ypb = sh.yp; io.m_yb = halo_map(A, y);
     io.kin = nullptr; io.kinp = nullptr; io.a = 0.0;
@@ -662,67 +552,10 @@ static size_t tile_smem(int nl) {
   return dyn_layout(nl, off);
 }
 
-// co-resident grid for the cooperative launch
 static int fast_grid(hsb_dev_model *m, const void *fn, int *grid) {
-  const size_t smem = tile_smem(m->nl);
-  HSB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0, nsm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
-  HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FT_THREADS, smem));
-  if (per_sm < 1) return set_error(HSB_E_ARG, "fast transient kernel does not fit an SM");
-  const long long tiles = (long long)((m->nc + TJ - 1) / TJ) * ((m->nr + TI - 1) / TI);
-  long long g = (long long)per_sm * nsm;
-  if (g > tiles) g = tiles;
-  *grid = (int)g;
-  return HSB_OK;
+  return coop_grid(m, fn, tile_smem(m->nl), grid);
 }
 
-// ---------------------------------------------------------------------------
-// tensor maps
-// ---------------------------------------------------------------------------
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
-                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
-                                  CUtensorMapFloatOOBfill);
-
-static EncodeTiledFn encode_tiled() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (EncodeTiledFn)p;
-  });
-  return fn;
-}
-
-// [nl][nr][nc] array of doubles (f64) or floats seen as a 3-D tensor with
-// box (bx, by, nl); out-of-range box elements read as zero
-static int make_map(CUtensorMap *map, const void *base, bool f64, const hsb_dev_model *m, unsigned bx,
-                    unsigned by) {
-  EncodeTiledFn enc = encode_tiled();
-  if (!enc) return set_error(HSB_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-  if (((uintptr_t)base & 15u) != 0) return set_error(HSB_E_ARG, "fast transient buffers must be 16-byte aligned");
-  const cuuint64_t es = f64 ? 8 : 4;
-  const cuuint64_t dims[3] = {(cuuint64_t)m->nc, (cuuint64_t)m->nr, (cuuint64_t)m->nl};
-  const cuuint64_t strides[2] = {(cuuint64_t)m->nc * es, (cuuint64_t)m->nr * m->nc * es};
-  const cuuint32_t box[3] = {bx, by, (cuuint32_t)m->nl};
-  const cuuint32_t estr[3] = {1, 1, 1};
-  const CUresult r = enc(map, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
-                         const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return set_error(HSB_E_ARG, "tensor map encoding failed for the fast transient form");
-  return HSB_OK;
-}
-
-static int check_shape(const hsb_dev_model *m) {
-  if (m->nl > FT_MAX_LAYERS) return set_error(HSB_E_ARG, "the fast transient form supports up to 16 layers");
-  if (m->nc % 4 != 0) return set_error(HSB_E_ARG, "the fast transient form needs a multiple of 4 grid columns");
-  return HSB_OK;
-}
 
 static int build_maps(Maps *M, const hsb_dev_model *m, const double *P, const double *Q, const double *t1,
                       const float *k1, const float *k2, const float *k3, const float *pf) {
@@ -741,94 +574,14 @@ static int build_maps(Maps *M, const hsb_dev_model *m, const double *P, const do
   return HSB_OK;
 }
 
-// FP32 layer table and FP64 package table from the model's FP64 values
-static void host_tables(const hsb_dev_model *m, LayerF *Lf, PackF *P) {
-  for (int l = 0; l < m->nl; l++) {
-    const LayerCoef &c = m->hostL0[l];
-    Lf[l].gNS = (float)(1.0 / c.rNS);
-    Lf[l].gEW = (float)(1.0 / c.rEW);
-    Lf[l].gDown = (float)(1.0 / c.rz);
-    Lf[l].invC = c.cap != 0.0 ? (float)(1.0 / c.cap) : 0.f;
-    Lf[l].gEdgeNS = c.edgeNS != 0.0 ? (float)(1.0 / c.edgeNS) : 0.f;
-    Lf[l].gEdgeEW = c.edgeEW != 0.0 ? (float)(1.0 / c.edgeEW) : 0.f;
-    Lf[l].gAmb = c.ramb != 0.0 ? (float)(1.0 / c.ramb) : 0.f;
-    Lf[l].kind = c.kind;
-  }
-  memset(P, 0, sizeof(PackF));
-  for (int k = 0; k < NXMAX; k++) {
-    P->eidx[k] = -1;
-    for (int l = 0; l < PK_LINKS; l++) P->nb[k][l] = -1;
-  }
-  const package_RC_t &pk = m->h_pk;
-  const LayerCoef *L = m->hostL0;
-  auto edge = [&](int node, int e, double R) {
-    P->eidx[node] = e;
-    P->ge[node] = 1.0 / R;
-  };
-  auto lnk = [&](int a, int b, double R) {
-    for (int l = 0; l < PK_LINKS; l++) {
-      if (P->nb[a][l] == b || P->nb[a][l] < 0) {
-        P->nb[a][l] = b;
-        P->g[a][l] += 1.0 / R;
-        return;
-      }
-    }
-  };
-  const int cN[4] = {HSB_SINK_C_N, HSB_SINK_C_S, HSB_SINK_C_W, HSB_SINK_C_E};
-  const int oN[4] = {HSB_SINK_N, HSB_SINK_S, HSB_SINK_W, HSB_SINK_E};
-  const int sN[4] = {HSB_SP_N, HSB_SP_S, HSB_SP_W, HSB_SP_E};
-  for (int s = 0; s < 4; s++) {
-    const bool y = s < 2;
-    const double r_hs2 = (y ? pk.r_hs2_y : pk.r_hs2_x) + pk.r_hs;
-    P->gamb[oN[s]] = 1.0 / (pk.r_hs_per + pk.r_amb_per);
-    lnk(oN[s], cN[s], r_hs2);
-    P->invC[oN[s]] = 1.0 / (pk.c_hs_per + pk.c_amb_per);
-    edge(cN[s], s, y ? L[m->hsidx].edgeNS : L[m->hsidx].edgeEW);
-    P->gamb[cN[s]] = 1.0 / (y ? pk.r_hs_c_per_y + pk.r_amb_c_per_y : pk.r_hs_c_per_x + pk.r_amb_c_per_x);
-    lnk(cN[s], sN[s], y ? pk.r_sp_per_y : pk.r_sp_per_x);
-    lnk(cN[s], oN[s], r_hs2);
-    P->invC[cN[s]] = 1.0 / (y ? pk.c_hs_c_per_y + pk.c_amb_c_per_y : pk.c_hs_c_per_x + pk.c_amb_c_per_x);
-    edge(sN[s], 4 + s, y ? L[m->spidx].edgeNS : L[m->spidx].edgeEW);
-    lnk(sN[s], cN[s], y ? pk.r_sp_per_y : pk.r_sp_per_x);
-    P->invC[sN[s]] = 1.0 / (y ? pk.c_sp_per_y : pk.c_sp_per_x);
-  }
-  if (m->nx > HSB_EXTRA) {
-    const int pO[4] = {HSB_PCB_N, HSB_PCB_S, HSB_PCB_W, HSB_PCB_E};
-    const int pC[4] = {HSB_PCB_C_N, HSB_PCB_C_S, HSB_PCB_C_W, HSB_PCB_C_E};
-    const int sO[4] = {HSB_SOLDER_N, HSB_SOLDER_S, HSB_SOLDER_W, HSB_SOLDER_E};
-    const int bO[4] = {HSB_SUB_N, HSB_SUB_S, HSB_SUB_W, HSB_SUB_E};
-    for (int s = 0; s < 4; s++) {
-      const bool y = s < 2;
-      const double r_p2 = (y ? pk.r_pcb2_y : pk.r_pcb2_x) + pk.r_pcb;
-      P->gamb[pO[s]] = 1.0 / pk.r_amb_sec_per;
-      lnk(pO[s], pC[s], r_p2);
-      P->invC[pO[s]] = 1.0 / (pk.c_pcb_per + pk.c_amb_sec_per);
-      edge(pC[s], 8 + s, y ? L[m->pcbidx].edgeNS : L[m->pcbidx].edgeEW);
-      P->gamb[pC[s]] = 1.0 / (y ? pk.r_amb_sec_c_per_y : pk.r_amb_sec_c_per_x);
-      lnk(pC[s], sO[s], y ? pk.r_pcb_c_per_y : pk.r_pcb_c_per_x);
-      lnk(pC[s], pO[s], r_p2);
-      P->invC[pC[s]] = 1.0 / (y ? pk.c_pcb_c_per_y + pk.c_amb_sec_c_per_y : pk.c_pcb_c_per_x + pk.c_amb_sec_c_per_x);
-      edge(sO[s], 12 + s, y ? L[m->solderidx].edgeNS : L[m->solderidx].edgeEW);
-      lnk(sO[s], pC[s], y ? pk.r_pcb_c_per_y : pk.r_pcb_c_per_x);
-      P->invC[sO[s]] = 1.0 / (y ? pk.c_solder_per_y : pk.c_solder_per_x);
-      edge(bO[s], 16 + s, y ? L[m->subidx].edgeNS : L[m->subidx].edgeEW);
-      lnk(bO[s], sO[s], y ? pk.r_solder_per_y : pk.r_solder_per_x);
-      P->invC[bO[s]] = 1.0 / (y ? pk.c_sub_per_y : pk.c_sub_per_x);
-    }
-  }
-}
 
-static int segmax_of(const hsb_dev_model *m) {
-  const int ntj = (m->nc + TJ - 1) / TJ, nti = (m->nr + TI - 1) / TI;
-  return ntj > nti ? ntj : nti;
-}
 
 static void free_fast(void *p) {
   FastWork *w = (FastWork *)p;
   if (!w) return;
   void *bufs[] = {w->k1, w->k2, w->k3, w->pf, w->ytemp, w->t1, w->t2, w->gN, w->gS, w->gW, w->gE,
                   w->gA, w->gB, w->invC, w->aN, w->aS, w->aW, w->aE, w->aO, w->Lf, w->pk, w->part,
-                  w->err, w->cnt};
+                  w->err, w->cnt, w->N};
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (w->h_cnt) cudaFreeHost(w->h_cnt);
@@ -845,7 +598,7 @@ __global__ void to_float(const double *__restrict__ r, float *__restrict__ g, lo
 }
 
 // (re)build the FP32 coefficient tables from the device model's FP64 ones
-static int fast_prepare(hsb_dev_model *m, FastWork **out) {
+int fast_prepare(hsb_dev_model *m, FastWork **out) {
   FastWork *w = (FastWork *)m->fast;
   const long long n = m->ncell;
   int rc;
@@ -869,8 +622,8 @@ static int fast_prepare(hsb_dev_model *m, FastWork **out) {
     HSB_CUDA(cudaMalloc(&w->pk, sizeof(PackF)));
     HSB_CUDA(cudaMalloc(&w->part, sizeof(double) * 2 * NEDGE * w->segmax));
     HSB_CUDA(cudaMalloc(&w->err, sizeof(unsigned long long) * 2));
-    HSB_CUDA(cudaMalloc(&w->cnt, sizeof(long long) * 4));
-    HSB_CUDA(cudaMallocHost(&w->h_cnt, sizeof(long long) * 4));
+    HSB_CUDA(cudaMalloc(&w->cnt, sizeof(long long) * 8));
+    HSB_CUDA(cudaMallocHost(&w->h_cnt, sizeof(long long) * 8));
   }
   // the maps describe the two state buffers whichever role each has now
   const bool same = (w->mapP == m->y && w->mapQ == w->ytemp) || (w->mapP == w->ytemp && w->mapQ == m->y);
@@ -922,6 +675,7 @@ static void fill_common(FastArgs &A, const hsb_dev_model *m) {
   A.subidx = m->subidx; A.solderidx = m->solderidx; A.pcbidx = m->pcbidx;
   A.segmax = segmax_of(m);
   A.max_attempts = 10000000;
+  A.h0 = 1e-7;
 }
 
 static int status_error(long long status) {
@@ -930,10 +684,7 @@ static int status_error(long long status) {
   return HSB_OK;
 }
 
-int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
-  FastWork *w;
-  int rc;
-  if ((rc = fast_prepare(m, &w))) return rc;
+int rk4_stage_run(hsb_dev_model *m, FastWork *w, double T, double h0, hsb_stats *st) {
   FastArgs A;
   memset(&A, 0, sizeof(A));
   fill_common(A, m);
@@ -949,7 +700,8 @@ int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
   A.y = m->y; A.ytemp = w->ytemp; A.t1 = w->t1; A.t2 = w->t2;
   A.k1 = w->k1; A.k2 = w->k2; A.k3 = w->k3;
   A.part = w->part; A.err = w->err; A.cnt = w->cnt;
-  A.T = time_elapsed;
+  A.T = T;
+  A.h0 = h0;
   HSB_CUDA(cudaMemsetAsync(w->cnt, 0, sizeof(long long) * 4, m->stream));
   void *args[] = {&A};
   const void *fn = kernel_for(m->field, m->uchan_mask != 0);
@@ -977,8 +729,32 @@ int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
   st->rk4_steps += w->h_cnt[0];
   st->rk4_attempts += w->h_cnt[1];
   st->slope_evals += w->h_cnt[0] + 10 * w->h_cnt[1];
-  st->sim_time += time_elapsed;
   return status_error(w->h_cnt[3]);
+}
+
+int rk4_fast_stages_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
+  FastWork *w;
+  int rc;
+  if ((rc = fast_prepare(m, &w))) return rc;
+  rc = rk4_stage_run(m, w, time_elapsed, 1e-7, st);
+  st->sim_time += time_elapsed;
+  return rc;
+}
+
+// the Krylov form; when its rejection budget runs out inside an interval,
+// the stage form finishes the interval from the last accepted step
+int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
+  FastWork *w;
+  int rc;
+  if ((rc = fast_prepare(m, &w))) return rc;
+  double t_done = time_elapsed, h_next = 0.0;
+  if ((rc = rk4_krylov_run(m, w, time_elapsed, st, &t_done, &h_next))) return rc;
+  if (t_done < time_elapsed) {
+    st->fallbacks += 1;
+    if ((rc = rk4_stage_run(m, w, time_elapsed - t_done, h_next, st))) return rc;
+  }
+  st->sim_time += time_elapsed;
+  return HSB_OK;
 }
 
 // ---------------------------------------------------------------------------

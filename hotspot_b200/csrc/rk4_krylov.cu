@@ -1,0 +1,756 @@
+// rk4_krylov.cu -- the fast transient form (HSB_FORM_FAST), Krylov evaluation.
+//
+// Within a sampling interval the grid model's slope is affine,
+//   f(T) = L T + c   (temperature_grid.c:3130-3601 cells, 2857-3093 package),
+// with L the fixed conductance/capacitance operator (advection included) and
+// c the power and ambient terms.  Then every stage of the reference's
+// step-doubling RK4 (RCutil.c:440-640) is a polynomial in L applied to
+// F = f(y):  with K the reference's k1 (K = F, or f(t1) of the previous
+// attempt after a rejection, RCutil.c:568),
+//   rk4_core:  k2 = F + (h/2) L K,  k3 = F + (h/2) L k2,  k4 = F + h L k3,
+//              y_out - y = h (K + 2 k2 + 2 k3 + k4) / 6,
+//   f(t1) = F + L (t1 - y),  t2 - t1 = rk4_core from t1 with k1 = f(t1),
+//   error = max |ytemp - t2|,  accepted: y = ytemp.
+// The kernel keeps Krylov vectors N_m = s_m L N_{m-1}, N_0 = F (FP32 cells,
+// FP64 package nodes; s_m = the h of the attempt that first needed N_m, so
+// the vectors stay of the order of F) and represents every stage vector by
+// its coefficients over them (FP64, a few dozen per attempt).  A step is one
+// pass that evaluates F = f(y) from the FP64 state, then the stencil passes
+// that extend the sequence to the error polynomial's degree (7, +4 per
+// rejection); each of those reads one FP32 vector (TMA halo box) and writes
+// one, and the last one also forms the error norm and the candidate state
+// ytemp in the second state buffer, which becomes the state when the step
+// is accepted.
+//
+// Arithmetic: stencil passes in FP32 from FP32 vectors (F from the FP64
+// state as FP32 deviations from ambient); state y, coefficient algebra,
+// error norm, package nodes in FP64.  The step-size control is the
+// reference's (SAFETY 0.95, growth <= 5, shrink >= 1/10, PRECISION 0.01) on
+// the error norm computed as a combination of the Krylov vectors; every CTA
+// reads the same global norm and takes the same decision.  When a step needs
+// more than KRY_DMAX vectors (seven rejections in a row) the kernel stops at
+// the last accepted step and the stage form finishes the interval.
+#include "fast_common.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace hsb {
+
+#define PMAX (KRY_DMAX + 8)   // coefficient array length
+
+struct KryArgs {
+  CUtensorMap m_y, m_y2;           // FP64 halo boxes of the two state buffers
+  CUtensorMap m_pf;                // FP32 interior boxes of the power
+  CUtensorMap m_N;                 // FP32 halo boxes of the Krylov vectors (4-D: vector index last)
+  CUtensorMap m_Ni;                // FP32 interior boxes of the Krylov vectors
+  CUtensorMap m_yi, m_y2i;         // FP64 interior boxes of the two state buffers
+  StencilArgs S;
+  int spidx, hsidx, subidx, solderidx, pcbidx;
+  int segmax;
+  const LayerF *Lf;
+  const PackF *pk;
+  const float *gN, *gS, *gW, *gE, *gA, *gB, *invC;
+  const float *aN, *aS, *aW, *aE, *aO;
+  const double *pgrid;
+  float *pf;
+  double *y, *y2;                  // the two state buffers (which holds the state alternates)
+  float *N;
+  long long ns;                    // stride between Krylov vectors
+  double *part;
+  unsigned long long *err;
+  long long *cnt;                  // [0] steps [1] attempts [2] status [3] passes [4..5] tout [6] final buffer
+  double *tout;                    // [0] time reached [1] next step size
+  double T;
+  long long max_attempts;
+};
+
+enum { K_FULL = 0, K_KRY = 1 };
+
+struct Coef {
+  double c[PMAX];
+  int n;                           // number of coefficients
+};
+
+struct KShared {
+  double yp[NXMAX];                    // package part of the state
+  double Np[KRY_DMAX + 1][NXMAX];      // package parts of the Krylov vectors
+  double es[NEDGE], wred[FT_WARPS];
+  double gmax, pmax;
+  float xsf[NXMAX];                    // package inputs of the pass in FP32 (cells' edge terms)
+  Coef E, D, F1, K;                    // error, full-step increment, f(t1), k1
+  Coef E1, D1, F11;                    // E / h, D / h, F1 of a first attempt (k1 = F, uniform scale h)
+  double ps[PMAX];                     // ps[m]: scale of N_m over L N_{m-1}
+  unsigned long long bar;
+  int lost;
+  LayerF L[FT_MAX_LAYERS];
+};
+
+#define ERR_STAGED 8   // Krylov vectors the error pass stages in shared memory
+
+// dynamic shared memory; the full-slope pass and the Krylov passes use the
+// same bytes
+struct KDyn {
+  double *th;   // [nl][HR][DW]  FP64 state box (full slope pass)
+  float *pw;    // [nl][NI]      power
+  float *d;     // [nl][HR][DW]  state - T_amb in FP32
+  float *vh;    // [nl][HR][KW]  input Krylov vector box
+  float *vi;    // [ERR_STAGED][nl][NI] interior boxes of the vectors the error combines
+  double *yi;   // [nl][NI]      interior box of the state (error pass)
+};
+
+__host__ __device__ inline size_t kdyn_layout(int nl, size_t off[6]) {
+  size_t o = 0;
+  off[0] = o; o = al128(o + 8 * (size_t)nl * DP);
+  off[1] = o; o = al128(o + 4 * (size_t)nl * NI);
+  off[2] = o; o = al128(o + 4 * (size_t)nl * DP);
+  const size_t full = o;
+  o = 0;
+  off[3] = o; o = al128(o + 4 * (size_t)nl * KP);
+  off[4] = o; o = al128(o + 4 * (size_t)ERR_STAGED * nl * NI);
+  off[5] = o; o = al128(o + 8 * (size_t)nl * NI);
+  return (o > full ? o : full) + 128;
+}
+
+// control state, identical in every thread
+struct KCtl {
+  int pkind, pm;        // pending package evaluation: kind (-1 none) and output index
+  double ps;            // its scale
+  int psp, sp, ep;      // edge-partial slots, error slot
+  unsigned phase;       // completed tile-copy phases
+  long long passes;
+};
+
+// ---------------------------------------------------------------------------
+// coefficient algebra over the basis N_m = (s L)^m F (one thread)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void c_one(Coef &p) {
+  p.n = 1;
+  p.c[0] = 1.0;
+}
+__device__ __forceinline__ void c_copy(Coef &d, const Coef &s) {
+  d.n = s.n;
+  for (int j = 0; j < s.n; j++) d.c[j] = s.c[j];
+}
+// w = L v: L N_m = N_{m+1} / s_{m+1}
+__device__ __forceinline__ void c_lop(Coef &w, const Coef &v, const double *ps) {
+  const int n = v.n + 1 < PMAX ? v.n + 1 : PMAX;
+  w.c[0] = 0.0;
+  for (int j = 1; j < n; j++) w.c[j] = v.c[j - 1] / ps[j];
+  w.n = n;
+}
+// y += a x
+__device__ __forceinline__ void c_axpy(Coef &y, double a, const Coef &x) {
+  for (int j = y.n; j < x.n; j++) y.c[j] = 0.0;
+  if (x.n > y.n) y.n = x.n;
+  for (int j = 0; j < x.n; j++) y.c[j] += a * x.c[j];
+}
+// y_out - y of rk4_core(y, k1 = K, h) with f(y) = F = N_0 (RCutil.c:440-531)
+__device__ void c_core(Coef &out, const Coef &K, double h, const double *s) {
+  Coef t, k2, k3, k4;
+  c_lop(t, K, s);
+  c_one(k2);
+  c_axpy(k2, h / 2.0, t);
+  c_lop(t, k2, s);
+  c_one(k3);
+  c_axpy(k3, h / 2.0, t);
+  c_lop(t, k3, s);
+  c_one(k4);
+  c_axpy(k4, h, t);
+  int n = K.n;
+  if (k2.n > n) n = k2.n;
+  if (k3.n > n) n = k3.n;
+  if (k4.n > n) n = k4.n;
+  for (int j = 0; j < n; j++) {
+    const double a1 = j < K.n ? K.c[j] : 0.0, a2 = j < k2.n ? k2.c[j] : 0.0;
+    const double a3 = j < k3.n ? k3.c[j] : 0.0, a4 = j < k4.n ? k4.c[j] : 0.0;
+    out.c[j] = h * (a1 + 2 * a2 + 2 * a3 + a4) / 6.0;
+  }
+  out.n = n;
+}
+
+// the attempt's polynomials (one thread): D = ytemp - y, F1 = f(t1), E = ytemp - t2;
+// vectors not computed yet (index > dcomp) will be made with scale h
+__device__ void plan_attempt(KShared &sh, double h, int dcomp) {
+  for (int m = dcomp + 1; m < PMAX; m++) sh.ps[m] = h;
+  const double *s = sh.ps;
+  Coef dh, d2;
+  c_core(sh.D, sh.K, h, s);
+  c_core(dh, sh.K, h / 2.0, s);
+  Coef t;
+  c_lop(t, dh, s);
+  c_one(sh.F1);
+  c_axpy(sh.F1, 1.0, t);
+  // second half step from t1 with k1 = f(t1): its f is F1 as well
+  {
+    Coef k2, k3, k4, u;
+    const double hh = h / 2.0;
+    c_lop(u, sh.F1, s);
+    c_copy(k2, sh.F1);
+    c_axpy(k2, hh / 2.0, u);
+    c_lop(u, k2, s);
+    c_copy(k3, sh.F1);
+    c_axpy(k3, hh / 2.0, u);
+    c_lop(u, k3, s);
+    c_copy(k4, sh.F1);
+    c_axpy(k4, hh, u);
+    int n = k4.n;
+    for (int j = 0; j < n; j++) {
+      const double a1 = j < sh.F1.n ? sh.F1.c[j] : 0.0, a2 = j < k2.n ? k2.c[j] : 0.0;
+      const double a3 = j < k3.n ? k3.c[j] : 0.0, a4 = k4.c[j];
+      d2.c[j] = hh * (a1 + 2 * a2 + 2 * a3 + a4) / 6.0;
+    }
+    d2.n = n;
+  }
+  // E = D - (dh + d2); coefficients that cancel to rounding against their
+  // own terms (the low orders, exactly zero in exact arithmetic when K = F)
+  // are dropped, the degree stays that of d2
+  c_copy(sh.E, sh.D);
+  c_axpy(sh.E, -1.0, dh);
+  c_axpy(sh.E, -1.0, d2);
+  for (int j = 0; j < sh.E.n; j++) {
+    const double ref = fabs(j < sh.D.n ? sh.D.c[j] : 0.0) + fabs(j < dh.n ? dh.c[j] : 0.0) +
+                       fabs(j < d2.n ? d2.c[j] : 0.0);
+    if (fabs(sh.E.c[j]) <= 1e-12 * ref) sh.E.c[j] = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// package nodes of the pending pass (one lane of warp 0 per node)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void kfinish(const KryArgs &A, KCtl &c, KShared &sh) {
+  if (c.pkind < 0) return;
+  const StencilArgs &S = A.S;
+  const int nx = S.nx, ne = S.secondary ? NEDGE : 8;
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const int ntj = (S.nc + TJ - 1) / TJ, nti = (S.nr + TI - 1) / TI;
+  for (int e = ty; e < ne; e += FT_WARPS) {
+    const int nseg = (e & 3) < 2 ? ntj : nti;
+    const double *pp = A.part + ((long long)c.psp * NEDGE + e) * A.segmax;
+    double s = 0.0;
+    for (int q = tx; q < nseg; q += 32) s += pp[q];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (tx == 0) sh.es[e] = s;
+  }
+  __syncthreads();
+  if (ty == 0 && tx < nx) {
+    // full slope (with ambient) of the state, or s * L applied to N_{m-1}
+    const PackF &P = *A.pk;
+    const bool full = c.pkind == K_FULL;
+    const double *x = full ? sh.yp : sh.Np[c.pm - 1];
+    const double xq = x[tx];
+    double s = full ? P.gamb[tx] * (S.ambient - xq) : -P.gamb[tx] * xq;
+    if (P.eidx[tx] >= 0) s += P.ge[tx] * sh.es[P.eidx[tx]];
+#pragma unroll
+    for (int l = 0; l < PK_LINKS; l++)
+      if (P.nb[tx][l] >= 0) s += P.g[tx][l] * (x[P.nb[tx][l]] - xq);
+    sh.Np[c.pm][tx] = full ? s * P.invC[tx] : s * P.invC[tx] * c.ps;
+  }
+  c.pkind = -1;
+}
+
+__device__ __forceinline__ void kwait(KShared &sh, KCtl &c) {
+  int it = 0;
+  while (!mbar_try_wait(&sh.bar, c.phase & 1u)) {
+    if (++it >= WAIT_LIMIT) {
+      sh.lost = 1;
+      break;
+    }
+  }
+  c.phase++;
+}
+
+// the error pass stages N_j (j < min(m, ERR_STAGED), nonzero coefficient)
+// and the state's interior box along with the halo box
+__device__ __forceinline__ bool err_uses(const KShared &sh, int j) {
+  return sh.E.c[j] != 0.0 || (j < sh.D.n && sh.D.c[j] != 0.0);
+}
+
+template <bool FULL, bool ERR>
+__device__ __forceinline__ void kissue(const KryArgs &A, const KDyn &ds, KShared &sh, int m, int i0, int j0,
+                                       const CUtensorMap *my) {
+  if (threadIdx.x != 0) return;
+  const unsigned nl = (unsigned)A.S.nl;
+  asm volatile("fence.proxy.async.global;\n" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  if (FULL) {
+    mbar_expect_tx(&sh.bar, nl * (DP * 8 + NI * 4));
+    tma3(ds.th, my, j0 - 2, i0 - 1, &sh.bar);
+    tma3(ds.pw, &A.m_pf, j0, i0, &sh.bar);
+  } else {
+    unsigned bytes = nl * KP * 4;
+    if (ERR) {
+      bytes += nl * NI * 8;
+      for (int j = 0; j < m && j < ERR_STAGED; j++)
+        if (err_uses(sh, j)) bytes += nl * NI * 4;
+    }
+    mbar_expect_tx(&sh.bar, bytes);
+    tma4(ds.vh, &A.m_N, j0 - 4, i0 - 1, m - 1, &sh.bar);
+    if (ERR) {
+      tma3(ds.yi, my, j0, i0, &sh.bar);
+      for (int j = 0; j < m && j < ERR_STAGED; j++)
+        if (err_uses(sh, j)) tma4(ds.vi + (size_t)j * nl * NI, &A.m_Ni, j0, i0, j, &sh.bar);
+    }
+  }
+}
+
+// One stencil pass: N_m = s L N_{m-1} (KRY) or N_0 = f(y) (FULL).  With ERR,
+// the cells' part of the error combination sum_j E_j N_j is folded in.
+// ERR: also the candidate state ynew = yb + sum_j D_j N_j of the own cells.
+template <bool FIELD, bool ADV, bool FULL, bool ERR>
+__device__ __forceinline__ void kpass(const KryArgs &A, cg::grid_group &grid, KCtl &c, KShared &sh,
+                                      const KDyn &ds, int m, double s, const CUtensorMap *my = nullptr,
+                                      const double *yb = nullptr, double *ynew = nullptr) {
+  constexpr int CH = Chunk<FIELD, ADV>::n;
+  const StencilArgs &S = A.S;
+  const int nl = S.nl, nr = S.nr, nc = S.nc, nx = S.nx;
+  const long long plane = S.plane;
+  const int ne = S.secondary ? NEDGE : 8;
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const double amb = S.ambient;
+  const float sf = (float)s;
+  const int ntj = (nc + TJ - 1) / TJ, nti = (nr + TI - 1) / TI, ntiles = ntj * nti;
+  float *Nout = A.N + (long long)m * A.ns;
+  double errl = 0.0;
+  // positions in the boxes: FULL reads the FP64 state box (row DW), KRY the
+  // FP32 vector box (row KW)
+  constexpr int W = FULL ? DW : KW, P = FULL ? DP : KP, X0 = FULL ? 2 : 4;
+  const int p_i = (ty + 1) * W + tx + X0;
+  int hr, hc;
+  halo_cell(tid, &hr, &hc);
+  const int p_h = hr * W + hc + X0 - 1;
+
+  if ((int)blockIdx.x < ntiles)
+    kissue<FULL, ERR>(A, ds, sh, m, (blockIdx.x / ntj) * TI, (blockIdx.x % ntj) * TJ, my);
+  kfinish(A, c, sh);
+  if (tid < nx) sh.xsf[tid] = FULL ? (float)(sh.yp[tid] - amb) : (float)sh.Np[m - 1][tid];
+  const double *xin = FULL ? sh.yp : sh.Np[m > 0 ? m - 1 : 0];
+
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int ti = tile / ntj, tj = tile - ti * ntj;
+    const int i0 = ti * TI, j0 = tj * TJ;
+    const int i = i0 + ty, j = j0 + tx;
+    if (tile != (int)blockIdx.x) kissue<FULL, ERR>(A, ds, sh, m, i0, j0, my);
+    kwait(sh, c);
+    if (FULL) {
+      for (int n = 0; n < nl; n++) {
+        ds.d[n * DP + p_i] = (float)(ds.th[n * DP + p_i] - amb);
+        if (hr >= 0) ds.d[n * DP + p_h] = (float)(ds.th[n * DP + p_h] - amb);
+      }
+    }
+    __syncthreads();
+    if (i < nr && j < nc) {
+      const long long coff = (long long)i * nc + j;
+      for (int n0 = 0; n0 < nl; n0 += CH) {
+        float gN[CH], gS[CH], gE[CH], gW[CH], gA[CH], gB[CH], iC[CH];
+        float aN[CH], aS[CH], aW[CH], aE[CH], aO[CH];
+        if (FIELD || ADV) {
+#pragma unroll
+          for (int u = 0; u < CH; u++) {
+            const long long cc = (long long)(n0 + u) * plane + coff;
+            if (n0 + u < nl) {
+              if (FIELD) {
+                gN[u] = A.gN[cc]; gS[u] = A.gS[cc]; gE[u] = A.gE[cc]; gW[u] = A.gW[cc];
+                gA[u] = A.gA[cc]; gB[u] = A.gB[cc]; iC[u] = A.invC[cc];
+              }
+              if (ADV && ((S.uchan_mask >> (n0 + u)) & 1ull)) {
+                aN[u] = A.aN[cc]; aS[u] = A.aS[cc]; aW[u] = A.aW[cc]; aE[u] = A.aE[cc]; aO[u] = A.aO[cc];
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < CH; u++) {
+          const int n = n0 + u;
+          if (n >= nl) break;
+          const long long cc = (long long)n * plane + coff;
+          const float *vn = FULL ? ds.d + n * DP : ds.vh + n * KP;
+          const float tc = vn[p_i];
+          const LayerF &L = sh.L[n];
+          float psum = 0.f;
+          if (i > 0) psum += (FIELD ? gN[u] : L.gNS) * (vn[p_i - W] - tc);
+          if (i < nr - 1) psum += (FIELD ? gS[u] : L.gNS) * (vn[p_i + W] - tc);
+          if (j < nc - 1) psum += (FIELD ? gE[u] : L.gEW) * (vn[p_i + 1] - tc);
+          if (j > 0) psum += (FIELD ? gW[u] : L.gEW) * (vn[p_i - 1] - tc);
+          if (n > 0) psum += (FIELD ? gA[u] : sh.L[n - 1].gDown) * (vn[p_i - P] - tc);
+          if (n < nl - 1) psum += (FIELD ? gB[u] : L.gDown) * (vn[p_i + P] - tc);
+          if (L.kind != LK_PLAIN) {
+            int eN, eS, eE, eW;
+            switch (L.kind) {
+              case LK_SPREADER: eN = HSB_SP_N; eS = HSB_SP_S; eE = HSB_SP_E; eW = HSB_SP_W; break;
+              case LK_SINK:
+                psum -= L.gAmb * tc;
+                eN = HSB_SINK_C_N; eS = HSB_SINK_C_S; eE = HSB_SINK_C_E; eW = HSB_SINK_C_W; break;
+              case LK_PCB:
+                psum -= L.gAmb * tc;
+                eN = HSB_PCB_C_N; eS = HSB_PCB_C_S; eE = HSB_PCB_C_E; eW = HSB_PCB_C_W; break;
+              case LK_SUB: eN = HSB_SUB_N; eS = HSB_SUB_S; eE = HSB_SUB_E; eW = HSB_SUB_W; break;
+              default: eN = HSB_SOLDER_N; eS = HSB_SOLDER_S; eE = HSB_SOLDER_E; eW = HSB_SOLDER_W; break;
+            }
+            if (i == 0) psum += L.gEdgeNS * (sh.xsf[eN] - tc);
+            if (i == nr - 1) psum += L.gEdgeNS * (sh.xsf[eS] - tc);
+            if (j == nc - 1) psum += L.gEdgeEW * (sh.xsf[eE] - tc);
+            if (j == 0) psum += L.gEdgeEW * (sh.xsf[eW] - tc);
+          }
+          if (ADV && ((S.uchan_mask >> n) & 1ull)) {
+            // advection: FP64 on absolute temperatures (full slope) or on the vector
+            double adv;
+            if (FULL) {
+              const double *th = ds.th + n * DP;
+              const double T = th[p_i];
+              adv = A.S.qin[cc] + (double)aO[u] * T;
+              if (i > 0) adv += (double)aN[u] * ((th[p_i - DW] + T) / 2.0);
+              if (i < nr - 1) adv += (double)aS[u] * ((th[p_i + DW] + T) / 2.0);
+              if (j > 0) adv += (double)aW[u] * ((th[p_i - 1] + T) / 2.0);
+              if (j < nc - 1) adv += (double)aE[u] * ((th[p_i + 1] + T) / 2.0);
+            } else {
+              const double T = tc;
+              adv = (double)aO[u] * T;
+              if (i > 0) adv += (double)aN[u] * (((double)vn[p_i - W] + T) / 2.0);
+              if (i < nr - 1) adv += (double)aS[u] * (((double)vn[p_i + W] + T) / 2.0);
+              if (j > 0) adv += (double)aW[u] * (((double)vn[p_i - 1] + T) / 2.0);
+              if (j < nc - 1) adv += (double)aE[u] * (((double)vn[p_i + 1] + T) / 2.0);
+            }
+            psum += (float)adv;
+          }
+          const float ic = FIELD ? iC[u] : L.invC;
+          const float k = FULL ? (ds.pw[n * NI + tid] + psum) * ic : psum * (ic * sf);
+          Nout[cc] = k;
+          if (ERR) {
+            // the vectors the error and the candidate state combine: the
+            // first ERR_STAGED from shared memory, the rest (after rejections) from global
+            const int nD = sh.D.n, q = n * NI + tid;
+            double e = sh.E.c[m] * (double)k, dy = 0.0;
+            for (int jj = 0; jj < m && jj < ERR_STAGED; jj++) {
+              if (!err_uses(sh, jj)) continue;
+              const double w = (double)ds.vi[(size_t)jj * nl * NI + q];
+              e += sh.E.c[jj] * w;
+              if (jj < nD) dy += sh.D.c[jj] * w;
+            }
+            const double ybv = ds.yi[q];
+            for (int jj = ERR_STAGED; jj < m; jj++) {
+              const double ce = sh.E.c[jj], cd = jj < nD ? sh.D.c[jj] : 0.0;
+              if (ce != 0.0 || cd != 0.0) {
+                const double w = (double)A.N[(long long)jj * A.ns + cc];
+                e += ce * w;
+                dy += cd * w;
+              }
+            }
+            errl = fmax(errl, fabs(e));
+            ynew[cc] = ybv + dy;
+          }
+        }
+      }
+    }
+    // partial edge sums of (v - x_node) of this pass's input over this tile's
+    // share of each package edge
+    const bool onN = i0 == 0, onS = i0 + TI >= nr, onW = j0 == 0, onE = j0 + TJ >= nc;
+    for (int e = ty; e < ne; e += FT_WARPS) {
+      const int side = e & 3;
+      if (!((side == 0 && onN) || (side == 1 && onS) || (side == 2 && onW) || (side == 3 && onE))) continue;
+      int layer, which, node;
+      edge_desc(e, A.spidx, A.hsidx, A.subidx, A.solderidx, A.pcbidx, &layer, &which, &node);
+      int pos = -1;
+      if (side < 2) {
+        const int r = side == 0 ? 1 : (nr - 1 - i0) + 1;
+        if (j0 + tx < nc) pos = r * W + tx + X0;
+      } else {
+        const int col = side == 2 ? 0 : nc - 1 - j0;
+        if (tx < TI && i0 + tx < nr) pos = (tx + 1) * W + col + X0;
+      }
+      double v = 0.0;
+      if (pos >= 0) v = (FULL ? ds.th[layer * DP + pos] : (double)ds.vh[layer * KP + pos]) - xin[node];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (tx == 0) A.part[((long long)c.sp * NEDGE + e) * A.segmax + (side < 2 ? tj : ti)] = v;
+    }
+    __syncthreads();
+  }
+  if (ERR) {
+    for (int o = 16; o > 0; o >>= 1) errl = fmax(errl, __shfl_down_sync(0xffffffffu, errl, o));
+    if (tx == 0) sh.wred[ty] = errl;
+    __syncthreads();
+    if (tid == 0) {
+      double mx = sh.wred[0];
+      for (int w = 1; w < FT_WARPS; w++) mx = fmax(mx, sh.wred[w]);
+      atomicMax(A.err + c.ep, (unsigned long long)__double_as_longlong(mx));
+    }
+  }
+  grid.sync();
+  c.pkind = FULL ? K_FULL : K_KRY;
+  c.pm = m;
+  c.ps = s;
+  c.psp = c.sp;
+  c.sp ^= 1;
+  c.passes++;
+}
+
+// global error norm of the attempt: cells (already reduced) and package nodes
+__device__ __forceinline__ double kerr_finish(const KryArgs &A, KCtl &c, KShared &sh) {
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  kfinish(A, c, sh);
+  if (tid == FT_THREADS - 1)
+    sh.gmax = __longlong_as_double((long long)(*(volatile unsigned long long *)(A.err + c.ep)));
+  if (ty == 0) {
+    double perr = 0.0;
+    if (tx < A.S.nx) {
+      double e = 0.0;
+      for (int jj = 0; jj < sh.E.n; jj++) e += sh.E.c[jj] * sh.Np[jj][tx];
+      perr = fabs(e);
+    }
+    for (int o = 16; o > 0; o >>= 1) perr = fmax(perr, __shfl_down_sync(0xffffffffu, perr, o));
+    if (tx == 0) sh.pmax = perr;
+  }
+  __syncthreads();
+  const double mx = fmax(sh.gmax, sh.pmax);
+  if (blockIdx.x == 0 && tid == 0) A.err[c.ep ^ 1] = 0ull;
+  c.ep ^= 1;
+  __syncthreads();
+  return mx;
+}
+
+template <bool FIELD, bool ADV>
+__global__ void __launch_bounds__(FT_THREADS, 2) rk4_krylov_kernel(const __grid_constant__ KryArgs A) {
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ __align__(128) unsigned char dyn_raw[];
+  __shared__ KShared sh;
+  const StencilArgs &S = A.S;
+  const int nx = S.nx, nl = S.nl;
+  KDyn ds;
+  {
+    size_t off[6];
+    kdyn_layout(nl, off);
+    unsigned char *base = dyn_raw + ((128u - (smem_u32(dyn_raw) & 127u)) & 127u);
+    ds.th = (double *)(base + off[0]);
+    ds.pw = (float *)(base + off[1]);
+    ds.d = (float *)(base + off[2]);
+    ds.vh = (float *)(base + off[3]);
+    ds.vi = (float *)(base + off[4]);
+    ds.yi = (double *)(base + off[5]);
+  }
+  if (threadIdx.x < nl) sh.L[threadIdx.x] = A.Lf[threadIdx.x];
+  if (threadIdx.x == 0) {
+    sh.lost = 0;
+    mbar_init(&sh.bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < S.ncell;
+       q += (long long)gridDim.x * blockDim.x)
+    A.pf[q] = (float)A.pgrid[q];
+  if (threadIdx.x < nx) sh.yp[threadIdx.x] = A.y[S.ncell + threadIdx.x];
+  if (blockIdx.x == 0 && threadIdx.x == 0) { A.err[0] = 0ull; A.err[1] = 0ull; }
+  grid.sync();
+
+  // first-attempt coefficients for h = 1 (they scale with h)
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < PMAX; q++) sh.ps[q] = 1.0;
+    c_one(sh.K);
+    plan_attempt(sh, 1.0, 0);
+    c_copy(sh.E1, sh.E);
+    c_copy(sh.D1, sh.D);
+    c_copy(sh.F11, sh.F1);
+  }
+  KCtl c;
+  c.pkind = -1;
+  c.sp = 0;
+  c.ep = 0;
+  c.phase = 0;
+  c.passes = 0;
+  long long steps = 0, attempts = 0;
+  int status = 0;
+  double t = 0.0, h = 0.0, new_h = 1e-7;
+  double *yb = A.y, *yn = A.y2;
+  while (t < A.T && new_h >= 1e-7 * 1.0e-6) {
+    h = new_h;
+    const CUtensorMap *myb = yb == A.y ? &A.m_y : &A.m_y2;
+    kpass<FIELD, ADV, true, false>(A, grid, c, sh, ds, 0, 1.0, myb);   // N_0 = f(y)
+    int dcomp = 0;
+    if (threadIdx.x == 0) c_one(sh.K);
+    double mx = 0.0;
+    bool first = true;
+    for (;;) {
+      h = new_h;
+      if (first) {
+        // k1 = F and every vector made with scale h: the h = 1 coefficients scaled
+        if (threadIdx.x < PMAX) {
+          const int q = threadIdx.x;
+          sh.ps[q] = h;
+          if (q < sh.E1.n) sh.E.c[q] = h * sh.E1.c[q];
+          if (q < sh.D1.n) sh.D.c[q] = h * sh.D1.c[q];
+          if (q < sh.F11.n) sh.F1.c[q] = sh.F11.c[q];
+          if (q == 0) {
+            sh.E.n = sh.E1.n;
+            sh.D.n = sh.D1.n;
+            sh.F1.n = sh.F11.n;
+          }
+        }
+        first = false;
+      } else if (threadIdx.x == 0) {
+        plan_attempt(sh, h, dcomp);
+      }
+      __syncthreads();
+      const int dE = sh.E.n - 1;
+      if (dE > KRY_DMAX || dE <= dcomp) {
+        status = 3;
+        break;
+      }
+      for (int q = dcomp + 1; q < dE; q++) kpass<FIELD, ADV, false, false>(A, grid, c, sh, ds, q, sh.ps[q]);
+      kpass<FIELD, ADV, false, true>(A, grid, c, sh, ds, dE, sh.ps[dE], yb == A.y ? &A.m_yi : &A.m_y2i, yb, yn);
+      dcomp = dE;
+      mx = kerr_finish(A, c, sh);
+      attempts++;
+      if (mx <= 0.01) {
+        new_h = 0.95 * h * pow(fabs(0.01 / mx), 0.2);
+        if (new_h > 5.0 * h) new_h = 5.0 * h;
+      } else {
+        new_h = 0.95 * h * pow(fabs(0.01 / mx), 0.25);
+        if (new_h < h / 10.0) new_h = h / 10.0;
+      }
+      if (attempts >= A.max_attempts) break;
+      if (new_h >= h) break;
+      // rejected: the retry's k1 is f(t1) of this attempt
+      if (threadIdx.x == 0) c_copy(sh.K, sh.F1);
+      __syncthreads();
+    }
+    if (status || attempts >= A.max_attempts) break;
+    // accepted: the candidate buffer becomes the state
+    if (threadIdx.x < nx) {
+      double dy = 0.0;
+      for (int q = 0; q < sh.D.n; q++) dy += sh.D.c[q] * sh.Np[q][threadIdx.x];
+      sh.yp[threadIdx.x] += dy;
+    }
+    double *tmp = yb;
+    yb = yn;
+    yn = tmp;
+    steps++;
+    new_h = new_h < A.T - t - h ? new_h : A.T - t - h;
+    t += h;
+  }
+  __syncthreads();
+  if (sh.lost && threadIdx.x == 0) {
+    for (int it = 0; it < WAIT_LIMIT && !mbar_try_wait(&sh.bar, c.phase & 1u); it++) {
+    }
+    status = 2;
+  }
+  if (status == 2) A.cnt[2] = 2;
+  if (blockIdx.x == 0) {
+    if (threadIdx.x < nx) yb[S.ncell + threadIdx.x] = sh.yp[threadIdx.x];
+    if (threadIdx.x == 0) {
+      A.cnt[6] = yb == A.y ? 0 : 1;
+      A.cnt[0] = steps;
+      A.cnt[1] = attempts;
+      if (status == 3) A.cnt[2] = 3;
+      if (attempts >= A.max_attempts) A.cnt[2] = 1;
+      A.cnt[3] = c.passes;
+      A.tout[0] = t;
+      A.tout[1] = new_h;
+    }
+  }
+}
+
+static const void *kry_kernel_for(bool field, bool adv) {
+  return field ? (adv ? (const void *)rk4_krylov_kernel<true, true> : (const void *)rk4_krylov_kernel<true, false>)
+               : (adv ? (const void *)rk4_krylov_kernel<false, true> : (const void *)rk4_krylov_kernel<false, false>);
+}
+
+static size_t kry_smem(int nl) {
+  size_t off[6];
+  return kdyn_layout(nl, off);
+}
+
+static int kry_prepare(hsb_dev_model *m, FastWork *w) {
+  int rc;
+  if (!w->N) {
+    w->nstride = (m->ncell + 63) / 64 * 64;
+    HSB_CUDA(cudaMalloc(&w->N, sizeof(float) * w->nstride * (KRY_DMAX + 1)));
+    if ((rc = make_map(&w->kmap_pf, w->pf, false, m, TJ, TI))) return rc;
+    if ((rc = make_map4(&w->kmap_N, w->N, m, KW, HR, KRY_DMAX + 1, w->nstride))) return rc;
+    if ((rc = make_map4(&w->kmap_Ni, w->N, m, TJ, TI, KRY_DMAX + 1, w->nstride))) return rc;
+  }
+  if (w->kmap_ybuf != m->y) {
+    if ((rc = make_map(&w->kmap_y, m->y, true, m, DW, HR))) return rc;
+    if ((rc = make_map(&w->kmap_yi, m->y, true, m, TJ, TI))) return rc;
+    w->kmap_ybuf = m->y;
+  }
+  if (w->kmap_y2buf != w->ytemp) {
+    if ((rc = make_map(&w->kmap_y2, w->ytemp, true, m, DW, HR))) return rc;
+    if ((rc = make_map(&w->kmap_y2i, w->ytemp, true, m, TJ, TI))) return rc;
+    w->kmap_y2buf = w->ytemp;
+  }
+  return HSB_OK;
+}
+
+int rk4_krylov_run(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next) {
+  int rc;
+  if ((rc = kry_prepare(m, w))) return rc;
+  KryArgs A;
+  memset(&A, 0, sizeof(A));
+  A.m_y = w->kmap_y;
+  A.m_y2 = w->kmap_y2;
+  A.m_yi = w->kmap_yi;
+  A.m_y2i = w->kmap_y2i;
+  A.m_Ni = w->kmap_Ni;
+  A.m_pf = w->kmap_pf;
+  A.m_N = w->kmap_N;
+  A.S = make_args(m, m->L0, m->nr, m->nc);
+  A.spidx = m->spidx; A.hsidx = m->hsidx;
+  A.subidx = m->subidx; A.solderidx = m->solderidx; A.pcbidx = m->pcbidx;
+  A.segmax = w->segmax;
+  A.Lf = w->Lf;
+  A.pk = w->pk;
+  A.gN = w->gN; A.gS = w->gS; A.gW = w->gW; A.gE = w->gE; A.gA = w->gA; A.gB = w->gB;
+  A.invC = w->invC;
+  A.aN = w->aN; A.aS = w->aS; A.aW = w->aW; A.aE = w->aE; A.aO = w->aO;
+  A.pgrid = m->pgrid;
+  A.pf = w->pf;
+  A.y = m->y;
+  A.y2 = w->ytemp;
+  A.N = w->N;
+  A.ns = w->nstride;
+  A.part = w->part;
+  A.err = w->err;
+  A.cnt = w->cnt;
+  A.tout = (double *)(w->cnt + 4);
+  A.T = T;
+  A.max_attempts = 10000000;
+  const void *fn = kry_kernel_for(m->field, m->uchan_mask != 0);
+  int grid = 0;
+  if ((rc = coop_grid(m, fn, kry_smem(m->nl), &grid))) return rc;
+  HSB_CUDA(cudaMemsetAsync(w->cnt, 0, sizeof(long long) * 8, m->stream));
+  void *args[] = {&A};
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, m->stream);
+  HSB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(FT_THREADS), args, kry_smem(m->nl), m->stream));
+  cudaEventRecord(e1, m->stream);
+  HSB_CUDA(cudaMemcpyAsync(w->h_cnt, w->cnt, sizeof(long long) * 8, cudaMemcpyDeviceToHost, m->stream));
+  HSB_CUDA(cudaStreamSynchronize(m->stream));
+  {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    st->kernel_ms += ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  st->launches += 1;
+  if (w->h_cnt[6]) {   // the state ended in the second buffer
+    double *tmp = m->y;
+    m->y = w->ytemp;
+    w->ytemp = tmp;
+  }
+  st->rk4_steps += w->h_cnt[0];
+  st->rk4_attempts += w->h_cnt[1];
+  st->slope_evals += w->h_cnt[3];
+  double tout[2];
+  memcpy(tout, w->h_cnt + 4, sizeof(tout));
+  *t_done = T;
+  *h_next = 0.0;
+  if (w->h_cnt[2] == 1) return set_error(HSB_E_NOCONV, "fast transient: RK4 attempt cap reached");
+  if (w->h_cnt[2] == 2) return set_error(HSB_E_CUDA, "fast transient: a tile copy did not complete in time");
+  if (w->h_cnt[2] == 3) {
+    *t_done = tout[0];
+    *h_next = tout[1];
+  }
+  return HSB_OK;
+}
+
+}  // namespace hsb

@@ -39,6 +39,7 @@ extern "C" {
 /* solver forms */
 #define HSB_FORM_PARITY  0    /* FP64, replays the reference's operation order */
 #define HSB_FORM_FAST    1    /* FP32 stencil work, FP64 state/refinement       */
+#define HSB_FORM_FAST_STAGES 2  /* the fast transient evaluated stage by stage     */
 
 /* steady methods */
 #define HSB_STEADY_AUTO       0  /* GS replay for FORM_PARITY; MG-PCG (or BiCGStab with advection) for FORM_FAST */
@@ -81,6 +82,7 @@ typedef struct hsb_stats {
   double device_ms;          /* device time of the call (CUDA events) */
   double kernel_ms;          /* device time of the solver kernels alone (CUDA events) */
   long long launches;        /* kernels this library launched during the call */
+  long long fallbacks;       /* intervals the Krylov-form transient handed to the stage form */
 } hsb_stats;
 
 struct hsb_dev_model;

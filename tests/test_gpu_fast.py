@@ -83,3 +83,35 @@ def test_mg_steady_converged(workdir, builder, grid):
     st = m.stats()
     assert st["refinements"] >= 1
     m.close()
+
+
+@pytest.mark.parametrize("builder", ["chip2d", "stack3d", "detailed"])
+def test_krylov_form_matches_stage_form(workdir, builder):
+    """The default fast transient (step-doubling RK4 evaluated through Krylov
+    vectors of the affine slope operator) against the same fast arithmetic
+    evaluated stage by stage: same accepted steps, temperatures within 1e-3 K."""
+    from hotspot_b200 import FORM_FAST_STAGES
+    if builder == "chip2d":
+        sc = W.scenario_chip2d(workdir, seed=31, grid=64, steps=25)
+    else:
+        sc = W.scenario_stack3d(workdir, seed=32, grid=64, steps=25, n_blocks=12)
+        sc.detailed_3D = builder == "detailed"
+    runs = []
+    for form in (FORM_FAST, FORM_FAST_STAGES):
+        m = hm.from_scenario(sc)
+        m.set_solver(form)
+        t = m.vector(m.config.init_temp)
+        out = []
+        tot = {"rk4_steps": 0, "rk4_attempts": 0, "fallbacks": 0}
+        for k in range(sc.steps):
+            m.compute_temp(m.power_vector(sc.block_power[k]), t if k == 0 else None, sc.dt)
+            out.append(t.copy())
+            st = m.stats()
+            for key in tot:
+                tot[key] += st[key]
+        runs.append((np.array(out), m.grid("trans"), tot))
+        m.close()
+    (a, ga, sa), (b, gb, sb) = runs
+    assert sa["rk4_steps"] == sb["rk4_steps"] and sa["rk4_attempts"] == sb["rk4_attempts"]
+    assert sa["fallbacks"] == 0
+    assert np.max(np.abs(a - b)) <= 1e-3 and np.max(np.abs(ga - gb)) <= 1e-3
