@@ -305,10 +305,17 @@ def write_materials(path: str) -> str:
 
 
 def scenario_microchannel(workdir: str, seed: int = 0, grid: int = 512,
-                          die: float = 10e-3, channel_w: float = 100e-6,
+                          die: float = 10.24e-3, channel_w: float = 100e-6,
                           channel_h: float = 200e-6, pitch: float = 200e-6,
                           blocks: int = 64) -> Scenario:
-    """Si (0.1 mm, power) over a 0.2 mm straight-channel water layer, 10x10 mm."""
+    """Si (0.1 mm, power) over a 0.2 mm straight-channel water layer.
+
+    The default die is 10.24 mm, i.e. 20 um cells at 512x512: the channel
+    layer's floorplan is generated from the CSV with printf("%e") positions
+    (7 significant digits, microchannel.c), so cell sizes whose multiples
+    need more digits (10 mm / 512 = 19.53125 um) make the generated units
+    overrun the grid and the reference's own set_bgmap rejects them.
+    """
     rng = np.random.default_rng(seed)
     cw = die / grid
     csv, lanes = straight_channels_csv(os.path.join(workdir, f"uchan_s{seed}.csv"),

@@ -115,3 +115,43 @@ def test_krylov_form_matches_stage_form(workdir, builder):
     assert sa["rk4_steps"] == sb["rk4_steps"] and sa["rk4_attempts"] == sb["rk4_attempts"]
     assert sa["fallbacks"] == 0
     assert np.max(np.abs(a - b)) <= 1e-3 and np.max(np.abs(ga - gb)) <= 1e-3
+
+
+@pytest.mark.parametrize("grid,seed", [(32, 41), (64, 42)])
+def test_bicgstab_microchannel_steady(workdir, grid, seed):
+    """The non-symmetric steady system of a microchannel model (advection
+    terms +-Cv*flow/2, which the reference can only hand to SuperLU) by FP32
+    BiCGStab with FP64 refinement, against FP64 sparse LU of the same
+    system: bar max |dT| <= 0.01 K."""
+    from hotspot_b200 import STEADY_BICGSTAB
+    sc = W.scenario_microchannel(workdir, seed=seed, grid=grid, die=grid * 20e-6, blocks=8)
+    m = hm.from_scenario(sc)
+    m.set_solver(FORM_FAST, STEADY_BICGSTAB)
+    o = OracleModel(sc)
+    p = m.power_vector(sc.block_power[0])
+    s = m.vector()
+    m.steady(p.copy(), s)
+    T, Tb = o.steady_direct(p)
+    st = m.stats()
+    err_b = float(np.max(np.abs(s - Tb)))
+    err_g = float(np.max(np.abs(m.grid("steady") - T)))
+    m.close()
+    assert err_b <= TOL and err_g <= TOL, (err_b, err_g, st)
+    assert st["refinements"] >= 1 and st["residual"] < 1e-6
+
+
+def test_bicgstab_symmetric_model(workdir):
+    """The same solver on a model without advection agrees with the direct solve."""
+    from hotspot_b200 import STEADY_BICGSTAB
+    sc = W.scenario_stack3d(workdir, seed=43, grid=64, steps=2, n_blocks=10)
+    sc.detailed_3D = True
+    m = hm.from_scenario(sc)
+    m.set_solver(FORM_FAST, STEADY_BICGSTAB)
+    o = OracleModel(sc)
+    avg = m.power_vector(sc.block_power.mean(0))
+    s = m.vector()
+    m.steady(avg.copy(), s)
+    T, Tb = o.steady_direct(avg)
+    err = float(np.max(np.abs(m.grid("steady") - T)))
+    m.close()
+    assert np.max(np.abs(s - Tb)) <= TOL and err <= TOL, err
