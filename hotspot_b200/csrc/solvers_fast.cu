@@ -50,7 +50,7 @@ struct BcLevelDev {
   int nl, nr, nc;
   long long plane, ncell;
   const float *cN, *cS, *cW, *cE, *cA, *cB, *dg;   // A[c, neighbour] and A[c, c]
-  const float *Lf, *Uf, *Pinv;                     // plane LU factors
+  const float *LF, *UB;                            // plane LU factors (plane storage)
   float geNS[BC_MAX_NL], geEW[BC_MAX_NL];          // cell <-> package edge conductance per layer
   float escNS;                                     // N/S package rows: edge conductance scale 2^k
   int spidx, hsidx;
@@ -60,7 +60,7 @@ struct BcLevel {
   int nc;
   long long plane, ncell, n;
   float *cN, *cS, *cW, *cE, *cA, *cB, *dg;
-  float *Lf, *Uf, *Pinv;
+  float *LF, *UB;              // plane LU factors (plane storage)
   float *x, *f, *r;
   float *pr, *py;              // plane right-hand sides and forward-pass values (plane storage)
   float *pinv;                 // 12 x 12 inverse of the package block at this level
@@ -80,6 +80,8 @@ struct BcWork {
   double *red;                 // reductions and scalars
   double *h_red;
   // one refinement pass (FP64 residual, inner BiCGStab, correction) as a graph
+  int R, tpb;                  // rows per streamed chunk, planes (threads) per CTA of the plane solve
+  int *status;                 // raised by a plane solve whose chunk copy did not arrive
   cudaGraphExec_t pass_exec;
   const double *pass_T;        // the state buffer the graph was captured for
   long long pass_launches;
@@ -251,22 +253,26 @@ __global__ void bc_coarsen(BcLevelDev F, float *cN, float *cS, float *cW, float 
 }
 
 // Plane storage: plane j sits in slot (j & 1) * half + (j >> 1), half =
-// (nc + 1) / 2, so the planes of one colour are consecutive and the threads
-// of a sweep read the factors and the right-hand sides coalesced.
+// (nc + 1) / 2, so the planes of one colour are consecutive; every plane's
+// data is contiguous and its records are padded to 16 bytes, so one thread
+// can stream its plane through shared memory with bulk copies and read it
+// back with 128-bit loads.  With VP = LFP = round4(nl), UBP = round4(nl+1):
+//   LF[(slot*nq + q)*LFP + m-1]      = L(q, q-m)                 m = 1..nl
+//   UB[(slot*nq + q)*UBP + m-1]      = U(q, q+m),  UB[.. + nl] = 1 / U(q, q)
+//   right-hand sides, forward values: [(slot*nr + i)*VP + n]
+__host__ __device__ __forceinline__ int bc_r4(int v) { return (v + 3) & ~3; }
 __device__ __forceinline__ int bc_slot(int j, int nc) { return (j & 1) * ((nc + 1) / 2) + (j >> 1); }
 
-// banded LU (no pivoting) of every plane j: unknowns q = i*nl + n, band
-// entry (q, q+d) at band[(q*(2nl+1) + d+nl) * nc + slot]; FP64 in place, then
-// the factors in FP32: Lf[(q*nl + m-1)*nc + slot] = L(q, q-m),
-// Uf[(q*nl + m-1)*nc + slot] = U(q, q+m), Pinv[q*nc + slot] = 1 / U(q, q)
-__global__ void bc_factor(BcLevelDev L, double *__restrict__ band, float *__restrict__ Lf, float *__restrict__ Uf,
-                          float *__restrict__ Pinv) {
+// banded LU (no pivoting) of every plane j: band entry (q, q+d) at
+// band[(q*(2nl+1) + d+nl) * nc + slot], FP64 in place; factors out in FP32
+__global__ void bc_factor(BcLevelDev L, double *__restrict__ band, float *__restrict__ LF, float *__restrict__ UB) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= L.nc) return;
   const int nl = L.nl, W = 2 * nl + 1;
   const int nq = L.nr * nl;
   const long long np = L.nc;
   const int slot = bc_slot(j, L.nc);
+  const int LFP = bc_r4(nl), UBP = bc_r4(nl + 1);
   auto B = [&](int q, int d) -> double & { return band[((long long)q * W + d + nl) * np + slot]; };
   for (int q = 0; q < nq; q++) {
     for (int d = -nl; d <= nl; d++) B(q, d) = 0.0;
@@ -288,112 +294,251 @@ __global__ void bc_factor(BcLevelDev L, double *__restrict__ band, float *__rest
         for (int c = p + 1; c <= last; c++) B(r, c - r) -= l * B(p, c - p);
     }
   }
+  const long long base = (long long)slot * nq;
   for (int q = 0; q < nq; q++) {
-    for (int m = 1; m <= nl; m++) {
-      Lf[((long long)q * nl + m - 1) * np + slot] = q - m >= 0 ? (float)B(q, -m) : 0.f;
-      Uf[((long long)q * nl + m - 1) * np + slot] = q + m < nq ? (float)B(q, m) : 0.f;
-    }
-    Pinv[(long long)q * np + slot] = (float)(1.0 / B(q, 0));
+    for (int m = 1; m <= LFP; m++) LF[(base + q) * LFP + m - 1] = (m <= nl && q - m >= 0) ? (float)B(q, -m) : 0.f;
+    for (int m = 1; m <= UBP; m++) UB[(base + q) * UBP + m - 1] = (m <= nl && q + m < nq) ? (float)B(q, m) : 0.f;
+    UB[(base + q) * UBP + nl] = (float)(1.0 / B(q, 0));
   }
 }
 
 // right-hand sides of the planes of one colour: prhs = f - (couplings to
-// the neighbouring planes and to the package nodes) x, in plane storage
-__global__ void bc_plane_rhs(BcLevelDev L, const float *__restrict__ x, const float *__restrict__ f,
-                             float *__restrict__ prhs, int color) {
+// the neighbouring planes and to the package nodes) x, written in plane
+// storage through a shared-memory transpose (32 planes x 32 q per CTA)
+__global__ void __launch_bounds__(256) bc_plane_rhs(BcLevelDev L, const float *__restrict__ x,
+                                                    const float *__restrict__ f, float *__restrict__ prhs, int color) {
+  __shared__ float tile[32][33];
   const int half = (L.nc + 1) / 2;
   const int ncol = color ? L.nc / 2 : half;   // planes of this colour
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int nq = L.nr * L.nl;
-  if (t >= (long long)nq * ncol) return;
-  const int q = (int)(t / ncol), k = (int)(t - (long long)q * ncol);
-  const int j = 2 * k + color;
-  const int i = q / L.nl, n = q - i * L.nl;
-  const long long c = (long long)n * L.plane + (long long)i * L.nc + j;
-  float rhs = f[c];
-  if (j > 0) rhs -= L.cW[c] * x[c - 1];
-  if (j < L.nc - 1) rhs -= L.cE[c] * x[c + 1];
-  if (n == L.spidx || n == L.hsidx) {
-    const float *xp = x + L.ncell;
-    if (i == 0) rhs += L.geNS[n] * xp[bc_edge_node(n, 0, L.spidx, L.hsidx)];
-    if (i == L.nr - 1) rhs += L.geNS[n] * xp[bc_edge_node(n, 1, L.spidx, L.hsidx)];
-    if (j == 0) rhs += L.geEW[n] * xp[bc_edge_node(n, 2, L.spidx, L.hsidx)];
-    if (j == L.nc - 1) rhs += L.geEW[n] * xp[bc_edge_node(n, 3, L.spidx, L.hsidx)];
+  const int k0 = blockIdx.x * 32, q0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int qq = ty; qq < 32; qq += 8) {
+    const int q = q0 + qq, k = k0 + tx;
+    if (q < nq && k < ncol) {
+      const int j = 2 * k + color;
+      const int i = q / L.nl, n = q - i * L.nl;
+      const long long c = (long long)n * L.plane + (long long)i * L.nc + j;
+      float rhs = f[c];
+      if (j > 0) rhs -= L.cW[c] * x[c - 1];
+      if (j < L.nc - 1) rhs -= L.cE[c] * x[c + 1];
+      if (n == L.spidx || n == L.hsidx) {
+        const float *xp = x + L.ncell;
+        if (i == 0) rhs += L.geNS[n] * xp[bc_edge_node(n, 0, L.spidx, L.hsidx)];
+        if (i == L.nr - 1) rhs += L.geNS[n] * xp[bc_edge_node(n, 1, L.spidx, L.hsidx)];
+        if (j == 0) rhs += L.geEW[n] * xp[bc_edge_node(n, 2, L.spidx, L.hsidx)];
+        if (j == L.nc - 1) rhs += L.geEW[n] * xp[bc_edge_node(n, 3, L.spidx, L.hsidx)];
+      }
+      tile[qq][tx] = rhs;
+    }
   }
-  prhs[(long long)q * L.nc + color * half + k] = rhs;
+  __syncthreads();
+  for (int kk = ty; kk < 32; kk += 8) {
+    const int k = k0 + kk, q = q0 + tx;
+    if (q < nq && k < ncol) {
+      const int i = q / L.nl, n = q - i * L.nl;
+      prhs[((long long)(color * half + k) * L.nr + i) * bc_r4(L.nl) + n] = tile[tx][kk];
+    }
+  }
 }
 
-// one half sweep of plane Gauss-Seidel: planes j = 2k + color solve
+// ---- bulk-copy primitives (one thread, its own mbarriers) -----------------
+__device__ __forceinline__ unsigned bc_smem(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bc_bar_init(unsigned long long *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bc_smem(bar)) : "memory");
+}
+__device__ __forceinline__ void bc_bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   bc_smem(dst)),
+               "l"(src), "r"(bytes), "r"(bc_smem(bar))
+               : "memory");
+}
+__device__ __forceinline__ void bc_expect(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bc_smem(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bc_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bc_smem(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bc_bulk_store(void *dst, const void *src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(bc_smem(src)),
+               "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void bc_store_read_done() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bc_store_done() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bc_fence_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+#define BC_WAIT_LIMIT (1 << 22)
+
+#define BC_NB 4   // chunk buffers per plane: three copies in flight while one is computed
+
+// per-thread shared-memory stride (floats): the ring, rounded so that it is
+// 4 (mod 32): the 128-bit loads of 8 consecutive threads then hit distinct banks
+__host__ __device__ __forceinline__ int bc_thread_stride(int nl, int R) {
+  const int mx = bc_r4(nl) > bc_r4(nl + 1) ? bc_r4(nl) : bc_r4(nl + 1);
+  const int ring = BC_NB * (R * bc_r4(nl) + R * nl * mx);
+  return ring + (((4 - ring) % 32) + 32) % 32;
+}
+
+// One half sweep of plane Gauss-Seidel: planes j = 2k + color solve
 // A_jj x_j = prhs_j exactly by forward/back substitution with the band
-// factors; y is kept in plane storage between the two passes.  The loads of
-// a row (its right-hand sides and factors) do not depend on the recurrence,
-// so they are issued together ahead of it.
+// factors.  Each thread owns one plane and streams it through shared memory
+// in chunks of R rows with a ring of BC_NB buffers: the bulk copies of the
+// next BC_NB-1 chunks are in flight while one chunk is computed, so the
+// recurrence does not wait on global memory.  The forward pass writes y in
+// place of the chunk's right-hand sides and stores it with a bulk copy (the
+// buffer is refilled one iteration later, once that store has read it); the
+// backward pass streams y back the same way.  A chunk that does not arrive
+// within BC_WAIT_LIMIT polls raises *status and ends the sweep.
 template <int NL>
-__global__ void __launch_bounds__(64)
-    bc_plane_solve(const float *__restrict__ Lf, const float *__restrict__ Uf, const float *__restrict__ Pinv,
-                   const float *__restrict__ prhs, float *__restrict__ yb, float *__restrict__ x, int nr, int nc,
-                   long long pl, int color) {
+__global__ void __launch_bounds__(32)
+    bc_plane_solve(const float *__restrict__ LF, const float *__restrict__ UB, const float *__restrict__ prhs,
+                   float *__restrict__ yb, float *__restrict__ x, int nr, int nc, long long pl, int color, int R,
+                   int *status) {
+  constexpr int VP = (NL + 3) & ~3, LFP = VP, UBP = (NL + 4) & ~3, MX = LFP > UBP ? LFP : UBP;
+  extern __shared__ __align__(128) float bc_dyn[];
+  __shared__ __align__(8) unsigned long long bars[32][BC_NB];
   const int half = (nc + 1) / 2;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 * k + color;
+  const int t = threadIdx.x;
+  for (int b = 0; b < BC_NB; b++) bc_bar_init(&bars[t][b]);
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  __syncthreads();
   if (j >= nc) return;
-  const long long np = nc;
-  const int slot = color * half + k;
+  const int nq = nr * NL, nch = nr / R;
+  const long long slot = color * half + k;
+  const float *rp = prhs + slot * nr * VP;
+  float *yp = yb + slot * nr * VP;
+  const float *lp = LF + slot * nq * LFP;
+  const float *up = UB + slot * nq * UBP;
+  // per-thread ring of BC_NB x [R*VP values][R*NL*MX factors]
+  const int BUF = R * VP + R * NL * MX;
+  float *const buf0 = bc_dyn + (size_t)t * bc_thread_stride(NL, R);
+  auto buf = [&](int b) { return buf0 + b * BUF; };
+  unsigned phase = 0u;   // bit b: parity of buffer b's next completion
+  bool lost = false;
+  auto wait = [&](int b) {
+    int it = 0;
+    while (!bc_try_wait(&bars[t][b], (phase >> b) & 1u)) {
+      if (++it >= BC_WAIT_LIMIT) {
+        lost = true;
+        return;
+      }
+    }
+    phase ^= 1u << b;
+  };
+  auto issue_fwd = [&](int c, int b) {
+    const unsigned bv = R * VP * 4, bf = R * NL * LFP * 4;
+    bc_fence_smem();
+    bc_expect(&bars[t][b], bv + bf);
+    bc_bulk_load(buf(b), rp + (long long)c * R * VP, bv, &bars[t][b]);
+    bc_bulk_load(buf(b) + R * VP, lp + (long long)c * R * NL * LFP, bf, &bars[t][b]);
+  };
+  auto issue_bwd = [&](int c, int b) {
+    const unsigned bv = R * VP * 4, bf = R * NL * UBP * 4;
+    bc_fence_smem();
+    bc_expect(&bars[t][b], bv + bf);
+    bc_bulk_load(buf(b), yp + (long long)c * R * VP, bv, &bars[t][b]);
+    bc_bulk_load(buf(b) + R * VP, up + (long long)c * R * NL * UBP, bf, &bars[t][b]);
+  };
+  // ---- forward: y = L^-1 prhs; chunk c in buffer c % BC_NB ----
   float yprev[NL], ycur[NL];
 #pragma unroll
   for (int n = 0; n < NL; n++) yprev[n] = 0.f;
-  // forward: y = L^-1 prhs
-  for (int i = 0; i < nr; i++) {
-    float rb[NL], lb[NL][NL];
+  for (int c = 0; c < BC_NB - 1 && c < nch; c++) issue_fwd(c, c);
+  for (int c = 0; c < nch; c++) {
+    const int b = c % BC_NB;
+    wait(b);
+    if (lost) break;
+    float *v = buf(b);
+    const float *lf = buf(b) + R * VP;
+    for (int r = 0; r < R; r++) {
+      float rv[VP];
 #pragma unroll
-    for (int n = 0; n < NL; n++) {
-      const long long q = (long long)i * NL + n;
-      rb[n] = prhs[q * np + slot];
+      for (int u = 0; u < VP; u += 4) *reinterpret_cast<float4 *>(rv + u) = *reinterpret_cast<const float4 *>(v + r * VP + u);
 #pragma unroll
-      for (int m = 0; m < NL; m++) lb[n][m] = Lf[(q * NL + m) * np + slot];
+      for (int n = 0; n < NL; n++) {
+        float lr[LFP];
+#pragma unroll
+        for (int u = 0; u < LFP; u += 4)
+          *reinterpret_cast<float4 *>(lr + u) = *reinterpret_cast<const float4 *>(lf + (r * NL + n) * LFP + u);
+        float a = rv[n];
+#pragma unroll
+        for (int m = 1; m <= NL; m++) a -= lr[m - 1] * (m <= n ? ycur[n - m] : yprev[NL + n - m]);
+        ycur[n] = a;
+        rv[n] = a;
+      }
+#pragma unroll
+      for (int u = 0; u < VP; u += 4) *reinterpret_cast<float4 *>(v + r * VP + u) = *reinterpret_cast<const float4 *>(rv + u);
+#pragma unroll
+      for (int n = 0; n < NL; n++) yprev[n] = ycur[n];
     }
-#pragma unroll
-    for (int n = 0; n < NL; n++) {
-      // y_q -= L(q, q-m) y_{q-m}: m <= n in this row, the rest in the previous one
-      float v = rb[n];
-#pragma unroll
-      for (int m = 1; m <= NL; m++) v -= lb[n][m - 1] * (m <= n ? ycur[n - m] : yprev[NL + n - m]);
-      ycur[n] = v;
-    }
-#pragma unroll
-    for (int n = 0; n < NL; n++) {
-      yb[((long long)i * NL + n) * np + slot] = ycur[n];
-      yprev[n] = ycur[n];
+    bc_fence_smem();
+    bc_bulk_store(yp + (long long)c * R * VP, v, R * VP * 4);
+    // refill the previous chunk's buffer: its store (one group back) has read it
+    const int cn = c + BC_NB - 1;
+    if (cn < nch) {
+      asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory");
+      issue_fwd(cn, cn % BC_NB);
     }
   }
-  // backward: x = U^-1 y
+  bc_store_done();
+  // ---- backward: x = U^-1 y; the s-th chunk from the end in buffer s % BC_NB ----
   float xnext[NL], xcur[NL];
 #pragma unroll
   for (int n = 0; n < NL; n++) xnext[n] = 0.f;
-  for (int i = nr - 1; i >= 0; i--) {
-    float yv[NL], ub[NL][NL], pv[NL];
+  if (!lost)
+    for (int s = 0; s < BC_NB - 1 && s < nch; s++) issue_bwd(nch - 1 - s, s);
+  for (int s = 0; s < nch && !lost; s++) {
+    const int c = nch - 1 - s, b = s % BC_NB;
+    wait(b);
+    if (lost) break;
+    const float *v = buf(b);
+    const float *ub = buf(b) + R * VP;
+    for (int r = R - 1; r >= 0; r--) {
+      const int i = c * R + r;
+      float yv[VP];
 #pragma unroll
-    for (int n = 0; n < NL; n++) {
-      const long long q = (long long)i * NL + n;
-      yv[n] = yb[q * np + slot];
-      pv[n] = Pinv[q * np + slot];
+      for (int u = 0; u < VP; u += 4) *reinterpret_cast<float4 *>(yv + u) = *reinterpret_cast<const float4 *>(v + r * VP + u);
 #pragma unroll
-      for (int m = 0; m < NL; m++) ub[n][m] = Uf[(q * NL + m) * np + slot];
+      for (int n = NL - 1; n >= 0; n--) {
+        float ur[UBP];
+#pragma unroll
+        for (int u = 0; u < UBP; u += 4)
+          *reinterpret_cast<float4 *>(ur + u) = *reinterpret_cast<const float4 *>(ub + (r * NL + n) * UBP + u);
+        float a = yv[n];
+#pragma unroll
+        for (int m = 1; m <= NL; m++) a -= ur[m - 1] * (n + m < NL ? xcur[n + m] : xnext[n + m - NL]);
+        xcur[n] = a * ur[NL];
+      }
+#pragma unroll
+      for (int n = 0; n < NL; n++) {
+        x[(long long)n * pl + (long long)i * nc + j] = xcur[n];
+        xnext[n] = xcur[n];
+      }
     }
-#pragma unroll
-    for (int n = NL - 1; n >= 0; n--) {
-      float v = yv[n];
-#pragma unroll
-      for (int m = 1; m <= NL; m++) v -= ub[n][m - 1] * (n + m < NL ? xcur[n + m] : xnext[n + m - NL]);
-      xcur[n] = v * pv[n];
-    }
-#pragma unroll
-    for (int n = 0; n < NL; n++) {
-      x[(long long)n * pl + (long long)i * nc + j] = xcur[n];
-      xnext[n] = xcur[n];
-    }
+    const int sn = s + BC_NB - 1;
+    if (sn < nch) issue_bwd(nch - 1 - sn, sn % BC_NB);
+  }
+  if (lost) {
+    // let the copies still in flight land before the CTA exits
+    for (int b = 0; b < BC_NB; b++)
+      for (int it = 0; it < BC_WAIT_LIMIT && !bc_try_wait(&bars[t][b], (phase >> b) & 1u); it++) {
+      }
+    bc_store_done();
+    atomicAdd(status, 1);
   }
 }
+
+static size_t bc_solve_smem(int nl, int R, int tpb) { return (size_t)tpb * bc_thread_stride(nl, R) * sizeof(float); }
 
 // the package rows at level L: sums over the attached edges
 __device__ void bc_edge_sums(const BcLevelDev &L, const BcPack *pk, const float *x, float *esum) {
@@ -524,7 +669,8 @@ enum { SC_RHO = 0, SC_RHO_OLD, SC_ALPHA, SC_OMEGA, SC_D0, SC_D1, SC_D2, SC_D3, S
 #define RED_MAXBITS SC_MAX
 #define RED_PART 64
 #define RED_GE (RED_PART + 2 * BC_DOT_BLOCKS)
-#define RED_TOTAL (RED_GE + 2 * BC_MAX_NL)
+#define RED_STATUS (RED_GE + 2 * BC_MAX_NL)   // one int: plane-solve copy failures
+#define RED_TOTAL (RED_STATUS + 1)
 
 __global__ void bc_dot_partial(const float *__restrict__ a, const float *__restrict__ b,
                                const float *__restrict__ c, const float *__restrict__ d, long long n,
@@ -664,7 +810,7 @@ static BcLevelDev bc_dev(const hsb_dev_model *m, const BcWork *w, int k) {
   d.nl = m->nl; d.nr = m->nr; d.nc = L.nc;
   d.plane = L.plane; d.ncell = L.ncell;
   d.cN = L.cN; d.cS = L.cS; d.cW = L.cW; d.cE = L.cE; d.cA = L.cA; d.cB = L.cB; d.dg = L.dg;
-  d.Lf = L.Lf; d.Uf = L.Uf; d.Pinv = L.Pinv;
+  d.LF = L.LF; d.UB = L.UB;
   d.pinv = L.pinv;
   const double sc = (double)(1ll << k);
   for (int n = 0; n < m->nl && n < BC_MAX_NL; n++) {
@@ -676,11 +822,15 @@ static BcLevelDev bc_dev(const hsb_dev_model *m, const BcWork *w, int k) {
   return d;
 }
 
+typedef void (*SolveFn)(const float *, const float *, const float *, float *, float *, int, int, long long, int,
+                        int, int *);
+static SolveFn solve_for(int nl);
+
 static void free_bc(void *p) {
   BcWork *w = (BcWork *)p;
   if (!w) return;
   for (auto &L : w->lv) {
-    float *b[] = {L.cN, L.cS, L.cW, L.cE, L.cA, L.cB, L.dg, L.Lf, L.Uf, L.Pinv, L.x, L.f, L.r, L.pr, L.py, L.pinv};
+    float *b[] = {L.cN, L.cS, L.cW, L.cE, L.cA, L.cB, L.dg, L.LF, L.UB, L.x, L.f, L.r, L.pr, L.py, L.pinv};
     for (float *q : b)
       if (q) cudaFree(q);
   }
@@ -718,11 +868,12 @@ static int bc_setup(hsb_dev_model *m, BcWork **out) {
     float **arr[] = {&L.cN, &L.cS, &L.cW, &L.cE, &L.cA, &L.cB, &L.dg};
     for (float **a : arr)
       if (cudaMalloc(a, sizeof(float) * L.ncell) != cudaSuccess) return fail(set_error(HSB_E_NOMEM, "BiCGStab levels"));
-    const size_t nfac = (size_t)L.ncell * nl;
-    if (cudaMalloc(&L.Lf, sizeof(float) * nfac) != cudaSuccess || cudaMalloc(&L.Uf, sizeof(float) * nfac) != cudaSuccess ||
-        cudaMalloc(&L.Pinv, sizeof(float) * L.ncell) != cudaSuccess || cudaMalloc(&L.x, sizeof(float) * L.n) != cudaSuccess ||
+    const size_t nqa = (size_t)L.ncell;   // planes x nq
+    const size_t nva = (size_t)L.nc * m->nr * bc_r4(nl);
+    if (cudaMalloc(&L.LF, sizeof(float) * nqa * bc_r4(nl)) != cudaSuccess ||
+        cudaMalloc(&L.UB, sizeof(float) * nqa * bc_r4(nl + 1)) != cudaSuccess || cudaMalloc(&L.x, sizeof(float) * L.n) != cudaSuccess ||
         cudaMalloc(&L.f, sizeof(float) * L.n) != cudaSuccess || cudaMalloc(&L.r, sizeof(float) * L.n) != cudaSuccess ||
-        cudaMalloc(&L.pr, sizeof(float) * L.ncell) != cudaSuccess || cudaMalloc(&L.py, sizeof(float) * L.ncell) != cudaSuccess ||
+        cudaMalloc(&L.pr, sizeof(float) * nva) != cudaSuccess || cudaMalloc(&L.py, sizeof(float) * nva) != cudaSuccess ||
         cudaMalloc(&L.pinv, sizeof(float) * BNX * BNX) != cudaSuccess)
       return fail(set_error(HSB_E_NOMEM, "BiCGStab levels"));
     const size_t bm = (size_t)L.ncell * (2 * nl + 1);
@@ -739,6 +890,17 @@ static int bc_setup(hsb_dev_model *m, BcWork **out) {
   if (cudaMalloc(&w->red, sizeof(double) * RED_TOTAL) != cudaSuccess ||
       cudaMallocHost(&w->h_red, sizeof(double) * 16) != cudaSuccess)
     return fail(set_error(HSB_E_NOMEM, "BiCGStab reductions"));
+  w->status = (int *)(w->red + RED_STATUS);
+  if (cudaMemset(w->status, 0, sizeof(int)) != cudaSuccess) return fail(set_error(HSB_E_CUDA, "BiCGStab status"));
+  // plane solve: chunks of R rows, as many planes per CTA as fit ~200 KB
+  w->R = m->nr % 16 == 0 ? 16 : m->nr % 8 == 0 ? 8 : m->nr % 4 == 0 ? 4 : m->nr % 2 == 0 ? 2 : 1;
+  const size_t per = bc_solve_smem(nl, w->R, 1);
+  w->tpb = (int)(200 * 1024 / per);
+  if (w->tpb > 32) w->tpb = 32;
+  if (w->tpb < 1) w->tpb = 1;
+  if (cudaFuncSetAttribute((const void *)solve_for(nl), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)bc_solve_smem(nl, w->R, w->tpb)) != cudaSuccess)
+    return fail(set_error(HSB_E_CUDA, "BiCGStab plane solver shared memory"));
   *out = w;
   return HSB_OK;
 }
@@ -838,7 +1000,7 @@ static int bc_build(hsb_dev_model *m, BcWork *w) {
   }
   for (int k = 0; k < w->nlev; k++) {
     BcLevel &L = w->lv[k];
-    bc_factor<<<(L.nc + 63) / 64, 64, 0, m->stream>>>(bc_dev(m, w, k), w->band, L.Lf, L.Uf, L.Pinv);
+    bc_factor<<<(L.nc + 63) / 64, 64, 0, m->stream>>>(bc_dev(m, w, k), w->band, L.LF, L.UB);
   }
   HSB_CUDA(cudaGetLastError());
   return HSB_OK;
@@ -854,9 +1016,6 @@ static int bc_rhs(hsb_dev_model *m, BcWork *w) {
   HSB_CUDA(cudaGetLastError());
   return HSB_OK;
 }
-
-typedef void (*SolveFn)(const float *, const float *, const float *, const float *, float *, float *, int,
-                        int, long long, int);
 
 static SolveFn solve_for(int nl) {
   switch (nl) {
@@ -880,10 +1039,11 @@ static void bc_half_sweep(hsb_dev_model *m, BcWork *w, const BcLevelDev &d, int 
                           int color) {
   BcLevel &L = w->lv[k];
   const int ncol = color ? d.nc / 2 : (d.nc + 1) / 2;
-  const long long nt = (long long)d.nr * d.nl * ncol;
-  bc_plane_rhs<<<bnb(nt), BCT, 0, m->stream>>>(d, x, f, L.pr, color);
-  solve_for(m->nl)<<<(unsigned)((ncol + 63) / 64), 64, 0, m->stream>>>(L.Lf, L.Uf, L.Pinv, L.pr, L.py, x, d.nr, d.nc,
-                                                                        d.plane, color);
+  const int nq = d.nr * d.nl;
+  dim3 g((unsigned)((ncol + 31) / 32), (unsigned)((nq + 31) / 32));
+  bc_plane_rhs<<<g, 256, 0, m->stream>>>(d, x, f, L.pr, color);
+  solve_for(m->nl)<<<(unsigned)((ncol + w->tpb - 1) / w->tpb), w->tpb, bc_solve_smem(m->nl, w->R, w->tpb),
+                     m->stream>>>(L.LF, L.UB, L.pr, L.py, x, d.nr, d.nc, d.plane, color, w->R, w->status);
 }
 
 static void bc_smooth(hsb_dev_model *m, BcWork *w, int k, float *x, const float *f, bool pre) {
@@ -966,6 +1126,7 @@ static void bc_pass(hsb_dev_model *m, BcWork *w, double *T, int inner, long long
   bc_dot2(m, w, w->e, w->e, nullptr, nullptr, n0, sc + SC_NE, nullptr);
   *launches += 3;
   cudaMemcpyAsync(w->h_red, sc, sizeof(double) * (SC_MAX + 1), cudaMemcpyDeviceToHost, m->stream);
+  cudaMemcpyAsync(w->h_red + 12, w->status, sizeof(int), cudaMemcpyDeviceToHost, m->stream);
 }
 
 static const int BC_INNER = 10;
@@ -1023,6 +1184,9 @@ int bicgstab_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
     HSB_CUDA(cudaStreamSynchronize(m->stream));
     launches += w->pass_launches;
     emax = sqrt(w->h_red[SC_NE]);
+    int lost = 0;
+    memcpy(&lost, w->h_red + 12, sizeof(int));
+    if (lost) return set_error(HSB_E_CUDA, "BiCGStab plane solve: a chunk copy did not complete in time");
     st->refinements += 1;
     st->cycles += BC_INNER;
     if (!(emax == emax)) return set_error(HSB_E_NOCONV, "BiCGStab steady solve broke down (NaN correction)");
