@@ -217,6 +217,13 @@ _SIGS = {
     "hsb_abi_sizes": (C.c_int, [C.POINTER(C.c_longlong), C.c_int]),
     "hsb_dev_transient_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                             C.POINTER(Stats)]),
+    "hsb_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int]),
+    "hsb_batch_destroy": (None, [C.c_void_p]),
+    "hsb_batch_transient": (C.c_int, [C.c_void_p, _D, C.c_double, C.POINTER(Stats)]),
+    "hsb_batch_set_schedule": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "hsb_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong),
+                                 C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "hsb_batch_chip_steps": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
 }
 
 

@@ -1,0 +1,63 @@
+"""Batches of grid models advanced together on one GPU (libhotspot_b200's
+hsb_batch_* entry points): every model keeps its own adaptive RK4 step
+sequence, and one persistent launch per sampling interval advances them all."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import HotspotError, lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise HotspotError(lib().hsb_dev_last_error().decode(errors="replace").strip())
+
+
+class Batch:
+    """A batch over existing :class:`hotspot_b200.model.RCModel` objects."""
+
+    def __init__(self, models):
+        self.models = list(models)
+        n = len(self.models)
+        devs = (C.c_void_p * n)(*[lib().hsb_grid_device(m.ptr) for m in self.models])
+        self.ptr = C.c_void_p()
+        _check(lib().hsb_batch_create(C.byref(self.ptr), devs, n))
+        self.n_cells = sum(m.n_cells for m in self.models)
+
+    def transient(self, block_powers, dt: float) -> dict:
+        """Advance every model by one interval of ``dt`` seconds; ``block_powers``
+        is one block power vector per model (or None to keep the last powers)."""
+        st = _abi.Stats()
+        if block_powers is None:
+            _check(lib().hsb_batch_transient(self.ptr, None, dt, C.byref(st)))
+        else:
+            flat = np.ascontiguousarray(np.concatenate(block_powers), dtype=np.float64)
+            _check(lib().hsb_batch_transient(self.ptr, _abi.dptr(flat), dt, C.byref(st)))
+        return st.as_dict()
+
+    def set_schedule(self, ctas_per_sm: int, split: float = 1.0):
+        _check(lib().hsb_batch_set_schedule(self.ptr, int(ctas_per_sm), float(split)))
+
+    def info(self) -> dict:
+        g, cells, cps, split = C.c_int(), C.c_longlong(), C.c_int(), C.c_double()
+        _check(lib().hsb_batch_info(self.ptr, C.byref(g), C.byref(cells), C.byref(cps), C.byref(split)))
+        return {"grid": g.value, "cells": cells.value, "ctas_per_sm": cps.value, "split": split.value}
+
+    def chip_steps(self) -> np.ndarray:
+        out = (C.c_longlong * len(self.models))()
+        _check(lib().hsb_batch_chip_steps(self.ptr, out))
+        return np.array(out[:], dtype=np.int64)
+
+    def close(self):
+        if self.ptr:
+            lib().hsb_batch_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -97,9 +97,13 @@ __global__ void g2b_kernel(const int *__restrict__ map, const double *__restrict
 }
 
 int b2g(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type) {
+  return b2g_on(m, blk_dev, grid_dev, type, m->stream);
+}
+
+int b2g_on(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type, cudaStream_t s) {
   const long long n = m->vlen;
   const int T = 256;
-  b2g_kernel<<<(unsigned)((n + T - 1) / T), T, 0, m->stream>>>(
+  b2g_kernel<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(
       m->b2g_ptr, m->b2g_blk, m->b2g_occ, m->b2g_area, blk_dev, grid_dev, m->ncell, m->nx,
       m->total_n_blocks, m->cell_area, type);
   HSB_CUDA(cudaGetLastError());
@@ -107,8 +111,12 @@ int b2g(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type) {
 }
 
 int g2b(hsb_dev_model *m, const double *grid_dev, double *blk_dev) {
+  return g2b_on(m, grid_dev, blk_dev, m->stream);
+}
+
+int g2b_on(hsb_dev_model *m, const double *grid_dev, double *blk_dev, cudaStream_t s) {
   const int n = m->total_n_blocks + m->nx, T = 128;
-  g2b_kernel<<<(n + T - 1) / T, T, 0, m->stream>>>(m->g2b, grid_dev, blk_dev, m->total_n_blocks,
+  g2b_kernel<<<(n + T - 1) / T, T, 0, s>>>(m->g2b, grid_dev, blk_dev, m->total_n_blocks,
                                                    m->nx, m->nr, m->nc, m->ncell, m->map_mode);
   HSB_CUDA(cudaGetLastError());
   return HSB_OK;

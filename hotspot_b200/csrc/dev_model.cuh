@@ -122,6 +122,9 @@ int cuda_check(cudaError_t e, const char *what);
 // b2g / g2b on the device (temperature_grid.c:1888-2015)
 int b2g(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type);
 int g2b(hsb_dev_model *m, const double *grid_dev, double *blk_dev);
+// the same on a given stream
+int b2g_on(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type, cudaStream_t s);
+int g2b_on(hsb_dev_model *m, const double *grid_dev, double *blk_dev, cudaStream_t s);
 
 // exact-replay solvers
 int rk4_exact_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);

@@ -317,5 +317,7 @@ int rk4_stage_run(hsb_dev_model *m, FastWork *w, double T, double h0, hsb_stats 
 // rejection budget ran out there (the state is the last accepted step) and
 // *h_next is the step size to continue with
 int rk4_krylov_run(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next);
+// the Krylov vectors and their tensor maps (allocated once per model)
+int kry_prepare(hsb_dev_model *m, FastWork *w);
 
 }  // namespace hsb

@@ -31,12 +31,11 @@
 // more than KRY_DMAX vectors (seven rejections in a row) the kernel stops at
 // the last accepted step and the stage form finishes the interval.
 #include "fast_common.cuh"
+#include "krylov_coef.cuh"
 
 namespace cg = cooperative_groups;
 
 namespace hsb {
-
-#define PMAX (KRY_DMAX + 8)   // coefficient array length
 
 struct KryArgs {
   CUtensorMap m_y, m_y2;           // FP64 halo boxes of the two state buffers
@@ -65,11 +64,6 @@ struct KryArgs {
 };
 
 enum { K_FULL = 0, K_KRY = 1 };
-
-struct Coef {
-  double c[PMAX];
-  int n;                           // number of coefficients
-};
 
 struct KShared {
   double yp[NXMAX];                    // package part of the state
@@ -120,98 +114,9 @@ struct KCtl {
   long long passes;
 };
 
-// ---------------------------------------------------------------------------
-// coefficient algebra over the basis N_m = (s L)^m F (one thread)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void c_one(Coef &p) {
-  p.n = 1;
-  p.c[0] = 1.0;
-}
-__device__ __forceinline__ void c_copy(Coef &d, const Coef &s) {
-  d.n = s.n;
-  for (int j = 0; j < s.n; j++) d.c[j] = s.c[j];
-}
-// w = L v: L N_m = N_{m+1} / s_{m+1}
-__device__ __forceinline__ void c_lop(Coef &w, const Coef &v, const double *ps) {
-  const int n = v.n + 1 < PMAX ? v.n + 1 : PMAX;
-  w.c[0] = 0.0;
-  for (int j = 1; j < n; j++) w.c[j] = v.c[j - 1] / ps[j];
-  w.n = n;
-}
-// y += a x
-__device__ __forceinline__ void c_axpy(Coef &y, double a, const Coef &x) {
-  for (int j = y.n; j < x.n; j++) y.c[j] = 0.0;
-  if (x.n > y.n) y.n = x.n;
-  for (int j = 0; j < x.n; j++) y.c[j] += a * x.c[j];
-}
-// y_out - y of rk4_core(y, k1 = K, h) with f(y) = F = N_0 (RCutil.c:440-531)
-__device__ void c_core(Coef &out, const Coef &K, double h, const double *s) {
-  Coef t, k2, k3, k4;
-  c_lop(t, K, s);
-  c_one(k2);
-  c_axpy(k2, h / 2.0, t);
-  c_lop(t, k2, s);
-  c_one(k3);
-  c_axpy(k3, h / 2.0, t);
-  c_lop(t, k3, s);
-  c_one(k4);
-  c_axpy(k4, h, t);
-  int n = K.n;
-  if (k2.n > n) n = k2.n;
-  if (k3.n > n) n = k3.n;
-  if (k4.n > n) n = k4.n;
-  for (int j = 0; j < n; j++) {
-    const double a1 = j < K.n ? K.c[j] : 0.0, a2 = j < k2.n ? k2.c[j] : 0.0;
-    const double a3 = j < k3.n ? k3.c[j] : 0.0, a4 = j < k4.n ? k4.c[j] : 0.0;
-    out.c[j] = h * (a1 + 2 * a2 + 2 * a3 + a4) / 6.0;
-  }
-  out.n = n;
-}
-
-// the attempt's polynomials (one thread): D = ytemp - y, F1 = f(t1), E = ytemp - t2;
-// vectors not computed yet (index > dcomp) will be made with scale h
-__device__ void plan_attempt(KShared &sh, double h, int dcomp) {
-  for (int m = dcomp + 1; m < PMAX; m++) sh.ps[m] = h;
-  const double *s = sh.ps;
-  Coef dh, d2;
-  c_core(sh.D, sh.K, h, s);
-  c_core(dh, sh.K, h / 2.0, s);
-  Coef t;
-  c_lop(t, dh, s);
-  c_one(sh.F1);
-  c_axpy(sh.F1, 1.0, t);
-  // second half step from t1 with k1 = f(t1): its f is F1 as well
-  {
-    Coef k2, k3, k4, u;
-    const double hh = h / 2.0;
-    c_lop(u, sh.F1, s);
-    c_copy(k2, sh.F1);
-    c_axpy(k2, hh / 2.0, u);
-    c_lop(u, k2, s);
-    c_copy(k3, sh.F1);
-    c_axpy(k3, hh / 2.0, u);
-    c_lop(u, k3, s);
-    c_copy(k4, sh.F1);
-    c_axpy(k4, hh, u);
-    int n = k4.n;
-    for (int j = 0; j < n; j++) {
-      const double a1 = j < sh.F1.n ? sh.F1.c[j] : 0.0, a2 = j < k2.n ? k2.c[j] : 0.0;
-      const double a3 = j < k3.n ? k3.c[j] : 0.0, a4 = k4.c[j];
-      d2.c[j] = hh * (a1 + 2 * a2 + 2 * a3 + a4) / 6.0;
-    }
-    d2.n = n;
-  }
-  // E = D - (dh + d2); coefficients that cancel to rounding against their
-  // own terms (the low orders, exactly zero in exact arithmetic when K = F)
-  // are dropped, the degree stays that of d2
-  c_copy(sh.E, sh.D);
-  c_axpy(sh.E, -1.0, dh);
-  c_axpy(sh.E, -1.0, d2);
-  for (int j = 0; j < sh.E.n; j++) {
-    const double ref = fabs(j < sh.D.n ? sh.D.c[j] : 0.0) + fabs(j < dh.n ? dh.c[j] : 0.0) +
-                       fabs(j < d2.n ? d2.c[j] : 0.0);
-    if (fabs(sh.E.c[j]) <= 1e-12 * ref) sh.E.c[j] = 0.0;
-  }
+// the attempt's polynomials (one thread): D = ytemp - y, F1 = f(t1), E = ytemp - t2
+__device__ __forceinline__ void plan_attempt(KShared &sh, double h, int dcomp) {
+  kry_plan(sh.E, sh.D, sh.F1, sh.K, sh.ps, h, dcomp);
 }
 
 // ---------------------------------------------------------------------------
@@ -656,7 +561,7 @@ static size_t kry_smem(int nl) {
   return kdyn_layout(nl, off);
 }
 
-static int kry_prepare(hsb_dev_model *m, FastWork *w) {
+int kry_prepare(hsb_dev_model *m, FastWork *w) {
   int rc;
   if (!w->N) {
     w->nstride = (m->ncell + 63) / 64 * 64;

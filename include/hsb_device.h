@@ -145,6 +145,29 @@ int hsb_dev_steady(hsb_dev_model *m, const double *block_power,
 int hsb_dev_transient_noalloc(hsb_dev_model *m, double *y, const double *pgrid,
                               double time_elapsed, hsb_stats *st);
 
+/* ---- batches: many models advanced together (no counterpart in the
+ * reference, which simulates one chip per process; each chip's arithmetic is
+ * the fast transient form of compute_temp_grid, temperature_grid.c:3603-3704).
+ *
+ * A batch references n existing device models (per-layer conductances,
+ * primary heat path, one device); hsb_batch_transient advances all of them by
+ * one sampling interval in ONE persistent cooperative launch.  block_power
+ * holds every model's power vector (total_n_blocks + 12 entries each, model
+ * after model) or NULL to keep the grid powers of the last call.  Each model
+ * keeps its own adaptive step sequence; its state stays in its own device
+ * model (hsb_dev_get_state, g2b through the model's entry points). */
+struct hsb_batch;
+typedef struct hsb_batch hsb_batch;
+int  hsb_batch_create(hsb_batch **out, hsb_dev_model *const *models, int n);
+void hsb_batch_destroy(hsb_batch *b);
+int  hsb_batch_transient(hsb_batch *b, const double *block_power, double time_elapsed, hsb_stats *st);
+/* schedule: co-resident CTAs per SM (>= 1), and how finely large models are
+ * split over CTA groups (1.0 = in proportion to their share of the work) */
+int  hsb_batch_set_schedule(hsb_batch *b, int ctas_per_sm, double split);
+int  hsb_batch_info(hsb_batch *b, int *grid, long long *cells, int *ctas_per_sm, double *split);
+/* accepted RK4 steps of each model in the last call (n entries) */
+int  hsb_batch_chip_steps(hsb_batch *b, long long *steps);
+
 /* which: 0 = transient state (last_trans), 1 = steady state (last_steady);
  * n = nl*nr*nc + n_extra doubles */
 int hsb_dev_get_state(hsb_dev_model *m, int which, double *out);

@@ -1,0 +1,71 @@
+"""Batched fast transient (hsb_batch_transient): many models of uneven size
+in one persistent launch.  Each model's arithmetic is that of the single-model
+fast form, so the batch must reproduce the single-model results (same
+accepted steps, temperatures within 1e-9 K) for every chip, whether the chip
+runs on a CTA group (with chip-local barriers) or shares a CTA with others."""
+import numpy as np
+import pytest
+
+from hotspot_b200 import FORM_FAST
+from hotspot_b200 import model as hm
+from hotspot_b200 import workloads as W
+from hotspot_b200.batch import Batch
+
+pytestmark = pytest.mark.gpu
+
+
+def _chips(workdir, specs):
+    out = []
+    for k, (kind, grid) in enumerate(specs):
+        if kind == "chip2d":
+            sc = W.scenario_chip2d(workdir, seed=60 + k, grid=grid, steps=6)
+        else:
+            sc = W.scenario_stack3d(workdir, seed=60 + k, grid=grid, steps=6, n_blocks=10)
+        sc.dt = 3.333e-6            # one sampling interval for the whole batch
+        out.append(sc)
+    return out
+
+
+def _run(scs, intervals, schedule=None):
+    single, batched = [], []
+    for sc in scs:
+        a, b = hm.from_scenario(sc), hm.from_scenario(sc)
+        a.set_solver(FORM_FAST)
+        b.set_solver(FORM_FAST)
+        for m in (a, b):
+            t = m.vector(m.config.init_temp)
+            m.compute_temp(m.power_vector(sc.block_power[0]), t, 0.0)
+        single.append(a)
+        batched.append(b)
+    bt = Batch(batched)
+    if schedule:
+        bt.set_schedule(*schedule)
+    steps_single = np.zeros(len(scs), dtype=np.int64)
+    steps_batch = np.zeros(len(scs), dtype=np.int64)
+    for k in range(1, intervals + 1):
+        for i, (sc, a) in enumerate(zip(scs, single)):
+            a.compute_temp(a.power_vector(sc.block_power[k]), None, sc.dt)
+            steps_single[i] += a.stats()["rk4_steps"]
+        bt.transient([b.power_vector(sc.block_power[k]) for sc, b in zip(scs, batched)], scs[0].dt)
+        steps_batch += bt.chip_steps()
+    errs = [float(np.max(np.abs(a.grid("trans") - b.grid("trans")))) for a, b in zip(single, batched)]
+    info = bt.info()
+    bt.close()
+    for m in single + batched:
+        m.close()
+    return errs, steps_single, steps_batch, info
+
+
+def test_batch_matches_single_models(workdir):
+    scs = _chips(workdir, [("chip2d", 32), ("stack3d", 64), ("chip2d", 64), ("stack3d", 32), ("chip2d", 128)])
+    errs, s1, s2, info = _run(scs, 5)
+    assert np.array_equal(s1, s2), (s1, s2)
+    assert max(errs) <= 1e-9, errs
+
+
+@pytest.mark.parametrize("schedule", [(1, 1.0), (2, 4.0), (1, 0.25)])
+def test_batch_schedules(workdir, schedule):
+    """Chips split over CTA groups (chip-local barriers) and packed chips."""
+    scs = _chips(workdir, [("stack3d", 128), ("chip2d", 32), ("chip2d", 64), ("stack3d", 64)] * 2)
+    errs, s1, s2, info = _run(scs, 3, schedule)
+    assert np.array_equal(s1, s2) and max(errs) <= 1e-9, (errs, info)
