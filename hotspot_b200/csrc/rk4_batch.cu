@@ -57,6 +57,9 @@ struct alignas(128) BChip {
 // [6] state buffer index (in and out)
 #define BOUT 8
 
+#define BNB 4
+#define BCH 2   // layers per chunk of the error pass's loads
+
 struct BShared {
   double yp[NXMAX];
   double Np[KRY_DMAX + 1][NXMAX];
@@ -65,9 +68,15 @@ struct BShared {
   float xsf[NXMAX];
   Coef E, D, F1, K, E1, D1, F11;
   double ps[PMAX];
-  unsigned long long bar[2];
+  unsigned long long bar[BNB];
   int lost;
   LayerF L[FT_MAX_LAYERS];
+};
+
+// tile-buffer geometry of a launch (sized for the batch's largest layer count)
+struct BBufs {
+  size_t full, kry;   // bytes of one buffer
+  int nkry;           // Krylov-pass ring length
 };
 
 struct BCtl {
@@ -82,10 +91,14 @@ struct BCtl {
 enum { BK_FULL = 0, BK_KRY = 1 };
 #define BAR_LIMIT (1 << 25)
 
-__host__ __device__ inline size_t bbuf_bytes(int nl) {
-  const size_t full = al128(8 * (size_t)nl * DP) + 4 * (size_t)nl * NI;
-  const size_t kry = 4 * (size_t)nl * KP;
-  return al128(full > kry ? full : kry);
+// tile buffers: the full-slope pass double-buffers FP64 state boxes (plus the
+// power box); the Krylov passes use the same bytes as a deeper ring of the
+// smaller FP32 boxes (up to BNB buffers), so more copies are in flight
+__host__ __device__ inline size_t bfull_bytes(int nl) { return al128(al128(8 * (size_t)nl * DP) + 4 * (size_t)nl * NI); }
+__host__ __device__ inline size_t bkry_bytes(int nl) { return al128(4 * (size_t)nl * KP); }
+__host__ __device__ inline int bkry_count(int nl) {
+  const int k = (int)(2 * bfull_bytes(nl) / bkry_bytes(nl));
+  return k < 2 ? 2 : k > BNB ? BNB : k;
 }
 
 // chip-local barrier over `size` CTAs (bounded wait)
@@ -177,25 +190,36 @@ __device__ __forceinline__ void bwait(BShared &sh, BCtl &c, int b) {
 // or N_0 = f(y) (FULL); ERR also combines the error and the candidate state.
 template <bool FULL, bool ERR>
 __device__ __forceinline__ void bpass(const BChip &C, int rank, int size, BCtl &c, BShared &sh, unsigned char *dyn,
-                                      size_t bsz, int m, double s, int cur) {
+                                      const BBufs &bb, int m, double s, int cur) {
   const int nl = C.nl, nr = C.nr, nc = C.nc, nx = C.nx;
-  const long long plane = C.plane;
+  const long long plane = C.plane, ns = C.ns;
   const int ne = 8;
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   const double amb = C.ambient;
   const float sf = (float)s;
   const int ntj = C.ntj, ntiles = C.ntiles;
-  float *Nout = C.N + (long long)m * C.ns;
+  const float *Nv = C.N;
+  float *Nout = C.N + (long long)m * ns;
   const double *yb = C.y[cur];
   double *ynew = C.y[cur ^ 1];
+  double *part = C.part;
+  const int segmax = C.segmax, spidx = C.spidx, hsidx = C.hsidx;
   double errl = 0.0;
   constexpr int W = FULL ? DW : KW, P = FULL ? DP : KP, X0 = FULL ? 2 : 4;
   const int p_i = (ty + 1) * W + tx + X0;
-  int hr, hc;
-  halo_cell(tid, &hr, &hc);
   const size_t pw_off = al128(8 * (size_t)nl * DP);
+  const size_t bsz = FULL ? bb.full : bb.kry;
+  const int nbuf = FULL ? 2 : bb.nkry;
+  // the vectors the error pass combines (nonzero coefficient), as a bitmask
+  unsigned use = 0u;
+  if (ERR)
+    for (int jj = 0; jj < m && jj < 32; jj++)
+      if (sh.E.c[jj] != 0.0 || (jj < sh.D.n && sh.D.c[jj] != 0.0)) use |= 1u << jj;
 
-  if (tid == 0 && rank < ntiles) bissue<FULL>(C, dyn, sh, 0, rank, m, cur);
+  // prefetch: tile k of this CTA goes to buffer k % nbuf, nbuf-1 tiles ahead
+  if (tid == 0)
+    for (int k = 0; k < nbuf - 1 && rank + k * size < ntiles; k++)
+      bissue<FULL>(C, dyn + k * bsz, sh, k, rank + k * size, m, cur);
   bfinish(C, c, sh);
   if (tid < nx) sh.xsf[tid] = FULL ? (float)(sh.yp[tid] - amb) : (float)sh.Np[m - 1][tid];
   const double *xin = FULL ? sh.yp : sh.Np[m > 0 ? m - 1 : 0];
@@ -203,11 +227,14 @@ __device__ __forceinline__ void bpass(const BChip &C, int rank, int size, BCtl &
 
   int k = 0;
   for (int tile = rank; tile < ntiles && !sh.lost; tile += size, k++) {
-    const int b = k & 1;
+    const int b = k % nbuf;
     const int ti = tile / ntj, tj = tile - ti * ntj;
     const int i0 = ti * TI, j0 = tj * TJ;
     const int i = i0 + ty, j = j0 + tx;
-    if (tid == 0 && tile + size < ntiles) bissue<FULL>(C, dyn + (b ^ 1) * bsz, sh, b ^ 1, tile + size, m, cur);
+    {
+      const int kn = k + nbuf - 1, tn = rank + kn * size;
+      if (tid == 0 && tn < ntiles) bissue<FULL>(C, dyn + (kn % nbuf) * bsz, sh, kn % nbuf, tn, m, cur);
+    }
     bwait(sh, c, b);
     unsigned char *buf = dyn + b * bsz;
     const double *th = (const double *)buf;
@@ -215,63 +242,90 @@ __device__ __forceinline__ void bpass(const BChip &C, int rank, int size, BCtl &
     const float *vh = (const float *)buf;
     if (i < nr && j < nc) {
       const long long coff = (long long)i * nc + j;
-      for (int n = 0; n < nl; n++) {
-        const long long cc = (long long)n * plane + coff;
-        const LayerF &L = sh.L[n];
-        float tc, vN = 0.f, vS = 0.f, vE = 0.f, vW = 0.f, vA = 0.f, vB = 0.f;
-        const int q = n * P + p_i;
-        if (FULL) {
-          tc = (float)(th[q] - amb);
-          if (i > 0) vN = (float)(th[q - W] - amb);
-          if (i < nr - 1) vS = (float)(th[q + W] - amb);
-          if (j < nc - 1) vE = (float)(th[q + 1] - amb);
-          if (j > 0) vW = (float)(th[q - 1] - amb);
-          if (n > 0) vA = (float)(th[q - P] - amb);
-          if (n < nl - 1) vB = (float)(th[q + P] - amb);
-        } else {
-          tc = vh[q];
-          if (i > 0) vN = vh[q - W];
-          if (i < nr - 1) vS = vh[q + W];
-          if (j < nc - 1) vE = vh[q + 1];
-          if (j > 0) vW = vh[q - 1];
-          if (n > 0) vA = vh[q - P];
-          if (n < nl - 1) vB = vh[q + P];
-        }
-        float psum = 0.f;
-        if (i > 0) psum += L.gNS * (vN - tc);
-        if (i < nr - 1) psum += L.gNS * (vS - tc);
-        if (j < nc - 1) psum += L.gEW * (vE - tc);
-        if (j > 0) psum += L.gEW * (vW - tc);
-        if (n > 0) psum += sh.L[n - 1].gDown * (vA - tc);
-        if (n < nl - 1) psum += L.gDown * (vB - tc);
-        if (L.kind != LK_PLAIN) {
-          int eN, eS, eE, eW;
-          if (L.kind == LK_SPREADER) {
-            eN = HSB_SP_N; eS = HSB_SP_S; eE = HSB_SP_E; eW = HSB_SP_W;
-          } else {
-            psum -= L.gAmb * tc;
-            eN = HSB_SINK_C_N; eS = HSB_SINK_C_S; eE = HSB_SINK_C_E; eW = HSB_SINK_C_W;
-          }
-          if (i == 0) psum += L.gEdgeNS * (sh.xsf[eN] - tc);
-          if (i == nr - 1) psum += L.gEdgeNS * (sh.xsf[eS] - tc);
-          if (j == nc - 1) psum += L.gEdgeEW * (sh.xsf[eE] - tc);
-          if (j == 0) psum += L.gEdgeEW * (sh.xsf[eW] - tc);
-        }
-        const float kv = FULL ? (pw[n * NI + tid] + psum) * L.invC : psum * (L.invC * sf);
-        Nout[cc] = kv;
+      for (int n0 = 0; n0 < nl; n0 += BCH) {
+        // error pass: every load of this chunk of layers is issued before the math
+        float w[BCH][8];
+        double yv[BCH];
         if (ERR) {
-          const int nD = sh.D.n;
-          double e = sh.E.c[m] * (double)kv, dy = 0.0;
-          for (int jj = 0; jj < m; jj++) {
-            const double ce = sh.E.c[jj], cd = jj < nD ? sh.D.c[jj] : 0.0;
-            if (ce != 0.0 || cd != 0.0) {
-              const double w = (double)__ldcg(C.N + (long long)jj * C.ns + cc);
-              e += ce * w;
-              dy += cd * w;
-            }
+#pragma unroll
+          for (int u = 0; u < BCH; u++) {
+            const long long cc = (long long)(n0 + u) * plane + coff;
+            yv[u] = n0 + u < nl ? __ldcg(yb + cc) : 0.0;
+#pragma unroll
+            for (int jj = 0; jj < 8; jj++)
+              w[u][jj] = (n0 + u < nl && ((use >> jj) & 1u)) ? __ldcg(Nv + (long long)jj * ns + cc) : 0.f;
           }
-          errl = fmax(errl, fabs(e));
-          ynew[cc] = __ldcg(yb + cc) + dy;
+        }
+#pragma unroll
+        for (int u = 0; u < BCH; u++) {
+          const int n = n0 + u;
+          if (n >= nl) break;
+          const long long cc = (long long)n * plane + coff;
+          const LayerF &L = sh.L[n];
+          float tc, vN = 0.f, vS = 0.f, vE = 0.f, vW = 0.f, vA = 0.f, vB = 0.f;
+          const int q = n * P + p_i;
+          if (FULL) {
+            tc = (float)(th[q] - amb);
+            if (i > 0) vN = (float)(th[q - W] - amb);
+            if (i < nr - 1) vS = (float)(th[q + W] - amb);
+            if (j < nc - 1) vE = (float)(th[q + 1] - amb);
+            if (j > 0) vW = (float)(th[q - 1] - amb);
+            if (n > 0) vA = (float)(th[q - P] - amb);
+            if (n < nl - 1) vB = (float)(th[q + P] - amb);
+          } else {
+            tc = vh[q];
+            if (i > 0) vN = vh[q - W];
+            if (i < nr - 1) vS = vh[q + W];
+            if (j < nc - 1) vE = vh[q + 1];
+            if (j > 0) vW = vh[q - 1];
+            if (n > 0) vA = vh[q - P];
+            if (n < nl - 1) vB = vh[q + P];
+          }
+          float psum = 0.f;
+          if (i > 0) psum += L.gNS * (vN - tc);
+          if (i < nr - 1) psum += L.gNS * (vS - tc);
+          if (j < nc - 1) psum += L.gEW * (vE - tc);
+          if (j > 0) psum += L.gEW * (vW - tc);
+          if (n > 0) psum += sh.L[n - 1].gDown * (vA - tc);
+          if (n < nl - 1) psum += L.gDown * (vB - tc);
+          if (L.kind != LK_PLAIN) {
+            int eN, eS, eE, eW;
+            if (L.kind == LK_SPREADER) {
+              eN = HSB_SP_N; eS = HSB_SP_S; eE = HSB_SP_E; eW = HSB_SP_W;
+            } else {
+              psum -= L.gAmb * tc;
+              eN = HSB_SINK_C_N; eS = HSB_SINK_C_S; eE = HSB_SINK_C_E; eW = HSB_SINK_C_W;
+            }
+            if (i == 0) psum += L.gEdgeNS * (sh.xsf[eN] - tc);
+            if (i == nr - 1) psum += L.gEdgeNS * (sh.xsf[eS] - tc);
+            if (j == nc - 1) psum += L.gEdgeEW * (sh.xsf[eE] - tc);
+            if (j == 0) psum += L.gEdgeEW * (sh.xsf[eW] - tc);
+          }
+          const float kv = FULL ? (pw[n * NI + tid] + psum) * L.invC : psum * (L.invC * sf);
+          Nout[cc] = kv;
+          if (ERR) {
+            // same order as the single-model kernel: E_m N_m, then j ascending
+            const int nD = sh.D.n;
+            double e = sh.E.c[m] * (double)kv, dy = 0.0;
+#pragma unroll
+            for (int jj = 0; jj < 8; jj++) {
+              if (jj < m && ((use >> jj) & 1u)) {
+                const double wv = (double)w[u][jj];
+                e += sh.E.c[jj] * wv;
+                if (jj < nD) dy += sh.D.c[jj] * wv;
+              }
+            }
+            for (int jj = 8; jj < m; jj++) {   // after rejections only
+              const double ce = sh.E.c[jj], cd = jj < nD ? sh.D.c[jj] : 0.0;
+              if (ce != 0.0 || cd != 0.0) {
+                const double wv = (double)__ldcg(Nv + (long long)jj * ns + cc);
+                e += ce * wv;
+                dy += cd * wv;
+              }
+            }
+            errl = fmax(errl, fabs(e));
+            ynew[cc] = yv[u] + dy;
+          }
         }
       }
     }
@@ -281,7 +335,7 @@ __device__ __forceinline__ void bpass(const BChip &C, int rank, int size, BCtl &
       const int side = e & 3;
       if (!((side == 0 && onN) || (side == 1 && onS) || (side == 2 && onW) || (side == 3 && onE))) continue;
       int layer, which, node;
-      edge_desc(e, C.spidx, C.hsidx, -1, -1, -1, &layer, &which, &node);
+      edge_desc(e, spidx, hsidx, -1, -1, -1, &layer, &which, &node);
       int pos = -1;
       if (side < 2) {
         const int r = side == 0 ? 1 : (nr - 1 - i0) + 1;
@@ -293,12 +347,10 @@ __device__ __forceinline__ void bpass(const BChip &C, int rank, int size, BCtl &
       double v = 0.0;
       if (pos >= 0) v = (FULL ? th[layer * DP + pos] : (double)vh[layer * KP + pos]) - xin[node];
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if (tx == 0) C.part[((long long)c.sp * NEDGE + e) * C.segmax + (side < 2 ? tj : ti)] = v;
+      if (tx == 0) part[((long long)c.sp * NEDGE + e) * segmax + (side < 2 ? tj : ti)] = v;
     }
     __syncthreads();
   }
-  (void)hr;
-  (void)hc;
   if (ERR) {
     for (int o = 16; o > 0; o >>= 1) errl = fmax(errl, __shfl_down_sync(0xffffffffu, errl, o));
     if (tx == 0) sh.wred[ty] = errl;
@@ -341,8 +393,8 @@ __device__ __forceinline__ double berr_finish(const BChip &C, int rank, BCtl &c,
 }
 
 // one sampling interval of one chip by a group of `size` CTAs (this is `rank`)
-__device__ void bchip(const BChip &C, int rank, int size, long long *out, BShared &sh, unsigned char *dyn, size_t bsz,
-                      unsigned &phase, double T) {
+__device__ void bchip(const BChip &C, int rank, int size, long long *out, BShared &sh, unsigned char *dyn,
+                      const BBufs &bsz, unsigned &phase, double T) {
   const int tid = threadIdx.x;
   const int nx = C.nx, nl = C.nl;
   if (tid < nl) sh.L[tid] = C.Lf[tid];
@@ -444,14 +496,13 @@ __device__ void bchip(const BChip &C, int rank, int size, long long *out, BShare
 
 __global__ void __launch_bounds__(FT_THREADS, 2)
     rk4_batch_kernel(const BChip *__restrict__ chips, const int4 *__restrict__ work, const int *__restrict__ wptr,
-                     long long *__restrict__ out, size_t bsz, double T) {
+                     long long *__restrict__ out, BBufs bsz, double T) {
   extern __shared__ __align__(128) unsigned char bdyn_raw[];
   __shared__ BShared sh;
   unsigned char *dyn = bdyn_raw + ((128u - (smem_u32(bdyn_raw) & 127u)) & 127u);
   if (threadIdx.x == 0) {
     sh.lost = 0;
-    mbar_init(&sh.bar[0], 1);
-    mbar_init(&sh.bar[1], 1);
+    for (int b = 0; b < BNB; b++) mbar_init(&sh.bar[b], 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     // first-attempt coefficients for h = 1 (they scale with h; chip-independent)
     for (int q = 0; q < PMAX; q++) sh.ps[q] = 1.0;
@@ -470,7 +521,7 @@ __global__ void __launch_bounds__(FT_THREADS, 2)
   }
   if (sh.lost && threadIdx.x == 0) {
     // let a tile copy still in flight land before the CTA exits
-    for (int b = 0; b < 2; b++)
+    for (int b = 0; b < BNB; b++)
       for (int it = 0; it < WAIT_LIMIT && !mbar_try_wait(&sh.bar[b], (phase >> b) & 1u); it++) {
       }
   }
@@ -521,7 +572,8 @@ struct hsb_batch {
   long long *d_out = nullptr, *h_out = nullptr;
   unsigned *d_bar = nullptr;
   int grid = 0;
-  size_t bsz = 0, smem = 0;
+  BBufs bsz{};
+  size_t smem = 0;
   cudaStream_t stream = nullptr;
   // schedule
   int ctas_per_sm = 1;
@@ -564,8 +616,10 @@ static int batch_schedule(hsb_batch *b) {
   if (per_sm < 1) return set_error(HSB_E_ARG, "batch kernel does not fit an SM");
   if (b->ctas_per_sm < per_sm) per_sm = b->ctas_per_sm;
   const int G = per_sm * nsm;
-  // work of a chip ~ its tiles x layers; big chips get CTA groups, the rest
-  // are packed onto single CTAs (longest first, onto the least loaded)
+  // work of a chip ~ its tiles x layers.  A chip worth `split` x (or more)
+  // two CTAs' fair share gets a group of CTAs; the rest are packed onto
+  // single CTAs (longest first onto the least loaded), and the packed part
+  // always keeps the CTAs its work needs at the fair share.
   std::vector<double> wk(b->n);
   double W = 0;
   for (int c = 0; c < b->n; c++) {
@@ -575,44 +629,64 @@ static int batch_schedule(hsb_batch *b) {
   std::vector<int> order(b->n);
   for (int c = 0; c < b->n; c++) order[c] = c;
   std::sort(order.begin(), order.end(), [&](int a, int c) { return wk[a] > wk[c]; });
+  const double share = W / G;
+  std::vector<int> g(b->n, 1);
+  double w_small = 0.0, sum_g = 0.0;
+  for (int c = 0; c < b->n; c++) {
+    int q = (int)(wk[c] / share * b->split);
+    if (q > b->h_chips[c].ntiles) q = b->h_chips[c].ntiles;
+    if (q >= 2) {
+      g[c] = q;
+      sum_g += q;
+    } else {
+      g[c] = 1;
+      w_small += wk[c];
+    }
+  }
+  int g_small = (int)ceil(w_small / share);
+  if (w_small > 0 && g_small < 1) g_small = 1;
+  if (g_small > G - 1) g_small = G - 1;
+  const double avail = G - g_small;
+  if (sum_g > avail) {   // scale the groups down to the CTAs left
+    const double f = avail / sum_g;
+    for (int c = 0; c < b->n; c++)
+      if (g[c] >= 2) {
+        int q = (int)(g[c] * f);
+        if (q < 2) {
+          q = 1;
+          w_small += wk[c];
+        }
+        g[c] = q;
+      }
+  }
   std::vector<std::vector<int4>> lists;
   std::vector<double> load;
-  int used = 0;
-  double share = W / G;
-  size_t pos = 0;
-  // multi-CTA groups first
-  for (; pos < order.size(); pos++) {
-    const int c = order[pos];
-    int g = (int)(wk[c] / share * b->split);
-    if (g > b->h_chips[c].ntiles) g = b->h_chips[c].ntiles;
-    if (g < 2) break;
-    if (used + g > G - 1) g = G - 1 - used;
-    if (g < 2) break;
-    for (int r = 0; r < g; r++) {
-      lists.push_back({make_int4(c, r, g, 0)});
-      load.push_back(wk[c] / g);
-    }
-    used += g;
-  }
-  // the rest: packed, least-loaded first
-  const int remaining = G - used;
+  for (int c : order)
+    if (g[c] >= 2)
+      for (int r = 0; r < g[c]; r++) {
+        lists.push_back({make_int4(c, r, g[c], 0)});
+        load.push_back(wk[c] / g[c]);
+      }
   const int base = (int)lists.size();
+  const int remaining = G - base > 0 ? G - base : 1;
   for (int k = 0; k < remaining; k++) {
     lists.push_back({});
     load.push_back(0.0);
   }
-  for (; pos < order.size(); pos++) {
-    const int c = order[pos];
+  for (int c : order) {
+    if (g[c] >= 2) continue;
     int best = base;
     for (int k = base; k < (int)lists.size(); k++)
       if (load[k] < load[best]) best = k;
-    if (remaining == 0) {   // every CTA is in a group: append to the least loaded list
-      best = 0;
-      for (int k = 0; k < (int)lists.size(); k++)
-        if (load[k] < load[best]) best = k;
-    }
     lists[best].push_back(make_int4(c, 0, 1, 0));
     load[best] += wk[c];
+  }
+  // drop CTAs left without work
+  {
+    std::vector<std::vector<int4>> keep;
+    for (auto &l : lists)
+      if (!l.empty()) keep.push_back(l);
+    lists.swap(keep);
   }
   std::vector<int> wptr(lists.size() + 1, 0);
   std::vector<int4> work;
@@ -704,8 +778,10 @@ int hsb_batch_create(hsb_batch **out, hsb_dev_model *const *models, int n) {
   std::vector<long long> init(BOUT * (size_t)n, 0);
   if (cudaMemcpy(b->d_out, init.data(), sizeof(long long) * BOUT * n, cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(set_error(HSB_E_CUDA, "batch outputs"));
-  b->bsz = bbuf_bytes(b->nlmax);
-  b->smem = 2 * b->bsz + 128;
+  b->bsz.full = bfull_bytes(b->nlmax);
+  b->bsz.kry = bkry_bytes(b->nlmax);
+  b->bsz.nkry = bkry_count(b->nlmax);
+  b->smem = 2 * b->bsz.full + 128;
   if (cudaFuncSetAttribute((const void *)rk4_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)b->smem) != cudaSuccess)
     return fail(set_error(HSB_E_ARG, "batch kernel shared memory too large (too many layers)"));
