@@ -224,6 +224,8 @@ _SIGS = {
     "hsb_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong),
                                  C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "hsb_batch_chip_steps": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "hsb_batch_autotune": (C.c_int, [C.c_void_p, C.c_int]),
+    "hsb_batch_tuning": (C.c_int, [C.c_void_p, _D, C.c_int]),
 }
 
 

@@ -46,6 +46,16 @@ class Batch:
         _check(lib().hsb_batch_info(self.ptr, C.byref(g), C.byref(cells), C.byref(cps), C.byref(split)))
         return {"grid": g.value, "cells": cells.value, "ctas_per_sm": cps.value, "split": split.value}
 
+    def autotune(self, enable: bool = True):
+        """Let the next calls try candidate schedules on the real work and keep the fastest."""
+        _check(lib().hsb_batch_autotune(self.ptr, int(enable)))
+
+    def tuning(self) -> list[dict]:
+        buf = np.zeros(4 * 64)
+        n = lib().hsb_batch_tuning(self.ptr, _abi.dptr(buf), 64)
+        return [{"ctas_per_sm": int(buf[4 * k]), "split": float(buf[4 * k + 1]), "ring": int(buf[4 * k + 2]),
+                 "ms_per_gcell_step": float(buf[4 * k + 3])} for k in range(n)]
+
     def chip_steps(self) -> np.ndarray:
         out = (C.c_longlong * len(self.models))()
         _check(lib().hsb_batch_chip_steps(self.ptr, out))

@@ -47,6 +47,7 @@ struct MgLevelDev {
   const float *gEdgeNS, *gEdgeEW;  // per layer edge conductance per cell
   int spidx, hsidx;
   float scale;                 // 2^level: edge conductances per coarse cell
+  const float *pinv;           // 12 x 12 inverse of the package block
 };
 
 struct MgLevel {
@@ -54,6 +55,7 @@ struct MgLevel {
   long long plane, ncell, n;
   float *gE, *gS, *gB, *diag, *gAmbL, *gEdgeNS, *gEdgeEW;
   float *x, *f, *r;
+  float *pinv;                 // 12 x 12 inverse of the package block at this level
 };
 
 struct MgWork {
@@ -68,6 +70,10 @@ struct MgWork {
   float *p, *q, *z, *e, *rr;
   double *red;                   // reduction scratch
   double *h_red;
+  // one refinement pass (FP64 residual, inner PCG, correction) as a graph
+  cudaGraphExec_t pass_exec;
+  const double *pass_T;
+  int pass_version;
 };
 
 // ---------------------------------------------------------------------------
@@ -138,12 +144,10 @@ __global__ void mg_apply_pack(MgLevelDev L, const PackSys *__restrict__ ps, cons
   }
 }
 
-// red-black z-line Gauss-Seidel half sweep on level L: solve A x = f
-__global__ void mg_zline(MgLevelDev L, float *__restrict__ x, const float *__restrict__ f, int color) {
-  long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= L.plane) return;
+// exact z-line solve of column `col` of level L (tridiagonal, Thomas)
+__device__ __forceinline__ void zline_col(const MgLevelDev &L, float *__restrict__ x, const float *__restrict__ f,
+                                          long long col) {
   const int i = (int)(col / L.nc), j = (int)(col - (long long)i * L.nc);
-  if (((i + j) & 1) != color) return;
   const int nl = L.nl;
   float cp[HSB_MAX_LAYERS], dp[HSB_MAX_LAYERS];
   const float *xp = x + L.ncell;
@@ -163,9 +167,9 @@ __global__ void mg_zline(MgLevelDev L, float *__restrict__ x, const float *__res
     }
     const float a = n > 0 ? -L.gB[c - L.plane] : 0.f;   // sub-diagonal
     const float cc = n < nl - 1 ? -L.gB[c] : 0.f;        // super-diagonal
-    const float b = L.diag[c];
+    const float bd = L.diag[c];
     // Thomas forward elimination
-    const float den = b - a * prev_c;
+    const float den = bd - a * prev_c;
     const float cn = cc / den;
     const float dn = (rhs - a * prev_d) / den;
     cp[n] = cn;
@@ -181,11 +185,20 @@ __global__ void mg_zline(MgLevelDev L, float *__restrict__ x, const float *__res
   }
 }
 
-// exact solve of the package nodes with the grid fixed (Gaussian elimination)
+// red-black z-line Gauss-Seidel half sweep on level L: solve A x = f
+__global__ void mg_zline(MgLevelDev L, float *__restrict__ x, const float *__restrict__ f, int color) {
+  long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= L.plane) return;
+  const int i = (int)(col / L.nc), j = (int)(col - (long long)i * L.nc);
+  if (((i + j) & 1) != color) return;
+  zline_col(L, x, f, col);
+}
+
+// exact solve of the package nodes with the grid fixed: x_pk = M^-1 (f_pk +
+// ge * edge sums), M^-1 precomputed per level
 __global__ void mg_pack_solve(MgLevelDev L, const PackSys *__restrict__ ps, float *__restrict__ x,
                               const float *__restrict__ f) {
-  __shared__ float esum[NXP];
-  __shared__ float M[NXP][NXP + 1];
+  __shared__ float esum[NXP], rhs[NXP];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int k = w; k < NXP; k += blockDim.x >> 5) {
     float s = 0.f;
@@ -203,54 +216,118 @@ __global__ void mg_pack_solve(MgLevelDev L, const PackSys *__restrict__ ps, floa
   __syncthreads();
   if (threadIdx.x < NXP) {
     const int k = threadIdx.x;
-    const int cnt = ps->elayer[k] < 0 ? 0 : (ps->eside[k] < 2 ? L.nc : L.nr);
-    const float ge = ps->ge0[k] * L.scale;
-    float D = cnt * ge + ps->gamb[k];
-    for (int o = 0; o < NXP; o++) {
-      D += ps->link[k][o];
-      M[k][o] = -ps->link[k][o];
-    }
-    M[k][k] = D;
-    M[k][NXP] = f[L.ncell + k] + ge * esum[k];
+    rhs[k] = f[L.ncell + k] + ps->ge0[k] * L.scale * esum[k];
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int p = 0; p < NXP; p++) {           // diagonally dominant: no pivoting
-      const float inv = 1.f / M[p][p];
-      for (int r = p + 1; r < NXP; r++) {
-        const float fct = M[r][p] * inv;
-        if (fct != 0.f)
-          for (int c = p; c <= NXP; c++) M[r][c] -= fct * M[p][c];
-      }
-    }
-    for (int p = NXP - 1; p >= 0; p--) {
-      float s = M[p][NXP];
-      for (int c = p + 1; c < NXP; c++) s -= M[p][c] * x[L.ncell + c];
-      x[L.ncell + p] = s / M[p][p];
-    }
+  if (threadIdx.x < NXP) {
+    const int k = threadIdx.x;
+    float s = 0.f;
+#pragma unroll
+    for (int o = 0; o < NXP; o++) s += L.pinv[k * NXP + o] * rhs[o];
+    x[L.ncell + k] = s;
   }
 }
 
-// coarse f = sum of the 2x2 fine residuals; package residuals carried over
+// the coarsest level in one CTA, from x = 0: `sweeps` pre-smoothing sweeps
+// (red, black z-lines, package) then `sweeps` post-smoothing sweeps
+// (package, black, red), the symmetric pattern of the per-kernel smoother
+__global__ void __launch_bounds__(1024) mg_coarse_solve(MgLevelDev L, const PackSys *__restrict__ ps,
+                                                        float *__restrict__ x, const float *__restrict__ f,
+                                                        int sweeps) {
+  __shared__ float esum[NXP], rhs[NXP];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto zl = [&](int color) {
+    for (long long col = threadIdx.x; col < L.plane; col += blockDim.x) {
+      const int i = (int)(col / L.nc), j = (int)(col - (long long)i * L.nc);
+      if (((i + j) & 1) == color) zline_col(L, x, f, col);
+    }
+    __syncthreads();
+  };
+  auto pk = [&]() {
+    for (int k = w; k < NXP; k += blockDim.x >> 5) {
+      float sm = 0.f;
+      const int layer = ps->elayer[k], side = ps->eside[k];
+      if (layer >= 0) {
+        const int len = side < 2 ? L.nc : L.nr;
+        const long long base = (long long)layer * L.plane +
+                               (side == 0 ? 0 : side == 1 ? (long long)(L.nr - 1) * L.nc : side == 2 ? 0 : L.nc - 1);
+        const long long st = side < 2 ? 1 : L.nc;
+        for (int q = lane; q < len; q += 32) sm += x[base + q * st];
+        for (int o = 16; o > 0; o >>= 1) sm += __shfl_down_sync(0xffffffffu, sm, o);
+      }
+      if (lane == 0) esum[k] = sm;
+    }
+    __syncthreads();
+    if (threadIdx.x < NXP) rhs[threadIdx.x] = f[L.ncell + threadIdx.x] + ps->ge0[threadIdx.x] * L.scale * esum[threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x < NXP) {
+      float v = 0.f;
+      for (int o = 0; o < NXP; o++) v += L.pinv[threadIdx.x * NXP + o] * rhs[o];
+      x[L.ncell + threadIdx.x] = v;
+    }
+    __syncthreads();
+  };
+  __syncthreads();
+  for (int s = 0; s < sweeps; s++) {
+    zl(0);
+    zl(1);
+    pk();
+  }
+  for (int s = 0; s < sweeps; s++) {
+    pk();
+    zl(1);
+    zl(0);
+  }
+}
+
+// Transfers: cell-centred bilinear prolongation (each fine cell takes 9/16 of
+// its parent, 3/16 of the two nearest coarse neighbours and 1/16 of the
+// diagonal one, the pattern of the reference's multigrid_prolong_temp,
+// temperature_grid.c:2616-2715; a neighbour outside the grid is replaced by
+// the parent) and its transpose as restriction, so the V-cycle stays a
+// symmetric preconditioner.  Layers are not coarsened; package values are
+// carried over unchanged.
+
+// 1-D weight with which fine index f contributes to coarse index c
+__device__ __forceinline__ float bl_w(int f, int c, int cn) {
+  const int par = f >> 1;
+  int nb = par + ((f & 1) ? 1 : -1);
+  nb = nb < 0 ? 0 : nb >= cn ? cn - 1 : nb;
+  return (par == c ? 0.75f : 0.f) + (nb == c ? 0.25f : 0.f);
+}
+
+// coarse f = P^T r (each coarse cell gathers the 4x4 fine cells around it)
 __global__ void mg_restrict_f(const float *__restrict__ rf, float *__restrict__ fc, int nl, int cnr,
                               int cnc, int nx) {
   const long long cpl = (long long)cnr * cnc, ncell = cpl * nl;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int fnc = 2 * cnc;
+  const int fnr = 2 * cnr, fnc = 2 * cnc;
   const long long fpl = 4 * cpl;
   if (t < ncell) {
     const int n = (int)(t / cpl);
     const long long r = t - n * cpl;
     const int i = (int)(r / cnc), j = (int)(r - (long long)i * cnc);
     const float *s = rf + n * fpl;
-    fc[t] = s[(2 * i) * fnc + 2 * j] + s[(2 * i + 1) * fnc + 2 * j] + s[(2 * i) * fnc + 2 * j + 1] +
-            s[(2 * i + 1) * fnc + 2 * j + 1];
+    float acc = 0.f;
+    for (int fi = 2 * i - 1; fi <= 2 * i + 2; fi++) {
+      if (fi < 0 || fi >= fnr) continue;
+      const float wi = bl_w(fi, i, cnr);
+      if (wi == 0.f) continue;
+      float row = 0.f;
+      for (int fj = 2 * j - 1; fj <= 2 * j + 2; fj++) {
+        if (fj < 0 || fj >= fnc) continue;
+        const float wj = bl_w(fj, j, cnc);
+        if (wj != 0.f) row += wj * s[(long long)fi * fnc + fj];
+      }
+      acc += wi * row;
+    }
+    fc[t] = acc;
   } else if (t < ncell + nx) {
     fc[t] = rf[fpl * nl + (t - ncell)];
   }
 }
 
-// fine x += injected coarse correction
+// fine x += P xc
 __global__ void mg_prolong_add(const float *__restrict__ xc, float *__restrict__ xf, int nl, int cnr,
                                int cnc, int nx) {
   const int fnr = 2 * cnr, fnc = 2 * cnc;
@@ -260,7 +337,13 @@ __global__ void mg_prolong_add(const float *__restrict__ xc, float *__restrict__
     const int n = (int)(t / fpl);
     const long long r = t - n * fpl;
     const int fi = (int)(r / fnc), fj = (int)(r - (long long)fi * fnc);
-    xf[t] += xc[n * cpl + (fi / 2) * cnc + fj / 2];
+    const int ci = fi >> 1, cj = fj >> 1;
+    int ci2 = ci + ((fi & 1) ? 1 : -1), cj2 = cj + ((fj & 1) ? 1 : -1);
+    ci2 = ci2 < 0 ? 0 : ci2 >= cnr ? cnr - 1 : ci2;
+    cj2 = cj2 < 0 ? 0 : cj2 >= cnc ? cnc - 1 : cj2;
+    const float *c = xc + n * cpl;
+    xf[t] += 0.5625f * c[(long long)ci * cnc + cj] + 0.1875f * c[(long long)ci2 * cnc + cj] +
+             0.1875f * c[(long long)ci * cnc + cj2] + 0.0625f * c[(long long)ci2 * cnc + cj2];
   } else if (t < fpl * nl + nx) {
     xf[t] += xc[cpl * nl + (t - fpl * nl)];
   }
@@ -442,9 +525,17 @@ __global__ void shift_scalars(double *sc) {
   sc[0] = sc[2];
 }
 
-__global__ void add_correction(double *__restrict__ T, const float *__restrict__ e, long long n) {
+// T += e; the max |e| (K) into *emax_bits (zeroed by the caller)
+__global__ void add_correction(double *__restrict__ T, const float *__restrict__ e, long long n,
+                               unsigned long long *emax_bits) {
   long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) T[k] += (double)e[k];
+  double a = 0.0;
+  if (k < n) {
+    T[k] += (double)e[k];
+    a = fabs((double)e[k]);
+  }
+  for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
+  if ((threadIdx.x & 31) == 0 && a > 0.0) atomicMax(emax_bits, (unsigned long long)__double_as_longlong(a));
 }
 
 __global__ void copy_f(const float *__restrict__ a, float *__restrict__ b, long long n) {
@@ -523,6 +614,7 @@ static MgLevelDev dev_level(const hsb_dev_model *m, const MgLevel &L, int lvl) {
   d.gAmbL = L.gAmbL; d.gEdgeNS = L.gEdgeNS; d.gEdgeEW = L.gEdgeEW;
   d.spidx = m->spidx; d.hsidx = m->hsidx;
   d.scale = (float)(1 << lvl);
+  d.pinv = L.pinv;
   return d;
 }
 
@@ -541,7 +633,7 @@ static int mg_setup(hsb_dev_model *m, MgWork **out) {
     L.ncell = L.plane * nl;
     L.n = L.ncell + nx;
     w->lv.push_back(L);
-    if (nr < 4 || nc < 4 || (nr & 1) || (nc & 1) || L.ncell <= 4096) break;
+    if (nr < 8 || nc < 8 || (nr & 1) || (nc & 1) || L.plane <= 16) break;
     nr /= 2; nc /= 2;
   }
   w->nlev = (int)w->lv.size();
@@ -557,6 +649,7 @@ static int mg_setup(hsb_dev_model *m, MgWork **out) {
     HSB_CUDA(cudaMalloc(&L.x, sizeof(float) * L.n));
     HSB_CUDA(cudaMalloc(&L.f, sizeof(float) * L.n));
     HSB_CUDA(cudaMalloc(&L.r, sizeof(float) * L.n));
+    HSB_CUDA(cudaMalloc(&L.pinv, sizeof(float) * NXP * NXP));
   }
   const long long n0 = w->lv[0].n, ncell = m->ncell;
   HSB_CUDA(cudaMalloc(&w->gE64, sizeof(double) * ncell));
@@ -583,7 +676,7 @@ static void free_mg(void *p) {
   MgWork *w = (MgWork *)p;
   if (!w) return;
   for (auto &L : w->lv) {
-    float *b[] = {L.gE, L.gS, L.gB, L.diag, L.gAmbL, L.gEdgeNS, L.gEdgeEW, L.x, L.f, L.r};
+    float *b[] = {L.gE, L.gS, L.gB, L.diag, L.gAmbL, L.gEdgeNS, L.gEdgeEW, L.x, L.f, L.r, L.pinv};
     for (float *q : b)
       if (q) cudaFree(q);
   }
@@ -592,6 +685,7 @@ static void free_mg(void *p) {
   for (void *q : b2)
     if (q) cudaFree(q);
   if (w->h_red) cudaFreeHost(w->h_red);
+  if (w->pass_exec) cudaGraphExecDestroy(w->pass_exec);
   delete w;
 }
 
@@ -645,6 +739,45 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
   }
   w->ps = ps;
   HSB_CUDA(cudaMemcpyAsync(w->d_ps, &ps, sizeof(ps), cudaMemcpyHostToDevice, m->stream));
+  // the package block of every level (FP64 Gauss-Jordan, partial pivoting),
+  // as the smoother's package solve uses it: D = cells * ge0 * 2^l + gamb + links
+  for (int l = 0; l < w->nlev; l++) {
+    const MgLevel &L = w->lv[l];
+    double M[NXP][2 * NXP];
+    for (int a = 0; a < NXP; a++) {
+      const int cnt = ps.elayer[a] < 0 ? 0 : (ps.eside[a] < 2 ? L.nc : L.nr);
+      const double ge = (double)ps.ge0[a] * (double)(1 << l);
+      double D = cnt * ge + ps.gamb[a];
+      for (int o = 0; o < NXP; o++) {
+        D += ps.link[a][o];
+        M[a][o] = -(double)ps.link[a][o];
+        M[a][NXP + o] = a == o ? 1.0 : 0.0;
+      }
+      M[a][a] = D;
+    }
+    for (int c = 0; c < NXP; c++) {
+      int piv = c;
+      for (int r = c + 1; r < NXP; r++)
+        if (fabs(M[r][c]) > fabs(M[piv][c])) piv = r;
+      if (piv != c)
+        for (int q = 0; q < 2 * NXP; q++) {
+          const double t = M[c][q];
+          M[c][q] = M[piv][q];
+          M[piv][q] = t;
+        }
+      const double inv = 1.0 / M[c][c];
+      for (int q = 0; q < 2 * NXP; q++) M[c][q] *= inv;
+      for (int r = 0; r < NXP; r++)
+        if (r != c && M[r][c] != 0.0) {
+          const double fct = M[r][c];
+          for (int q = 0; q < 2 * NXP; q++) M[r][q] -= fct * M[c][q];
+        }
+    }
+    float inv32[NXP * NXP];
+    for (int a = 0; a < NXP; a++)
+      for (int o = 0; o < NXP; o++) inv32[a * NXP + o] = (float)M[a][NXP + o];
+    HSB_CUDA(cudaMemcpy(L.pinv, inv32, sizeof(inv32), cudaMemcpyHostToDevice));
+  }
   double pack64[HSB_MAX_LAYERS + 3 * NXP + NXP * NXP];
   memcpy(pack64, gamb, sizeof(double) * HSB_MAX_LAYERS);
   memcpy(pack64 + HSB_MAX_LAYERS, ge_p, sizeof(double) * NXP);
@@ -701,8 +834,7 @@ static void vcycle(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f)
   const MgLevel &L = w->lv[l];
   mg_zero<<<nb(L.n), MGT, 0, m->stream>>>(x, L.n);
   if (l == w->nlev - 1) {
-    smooth(m, w, l, x, f, 1, 16);
-    smooth(m, w, l, x, f, 0, 16);
+    mg_coarse_solve<<<1, 1024, 0, m->stream>>>(dev_level(m, L, l), w->d_ps, x, f, 8);
     return;
   }
   const MgLevelDev d = dev_level(m, L, l);
@@ -749,19 +881,18 @@ int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
   HSB_CUDA(cudaGetLastError());
   const MgLevel &L0 = w->lv[0];
   const MgLevelDev d0 = dev_level(m, L0, 0);
-  double *sc = w->red;   // [0] rz, [1] pq, [2] rz_new, [3] |e|^2, [4] max|r| bits
+  double *sc = w->red;   // [0] rz, [1] pq, [2] rz_new, [3] max|e| bits, [4] max|r| bits
   unsigned long long *maxbits = (unsigned long long *)(w->red + 4);
-  int refine = 0;
-  double rmax = 0.0, emax = 1e300;
-  for (refine = 0; refine < max_ref; refine++) {
-    // FP64 residual r = b - G T
-    HSB_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), m->stream));
+  const int inner = 6;
+  // one refinement pass: r = b - G T (FP64), `inner` PCG iterations on
+  // G e = r (FP32), T += e, |e|_2^2 to the host; the same kernel sequence
+  // every time, so it is captured once as a CUDA graph and replayed
+  auto pass = [&]() {
+    cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), m->stream);
     fine_residual64<<<nb(m->ncell), MGT, 0, m->stream>>>(S, w->gE64, w->gS64, w->gB64, gambL, w->gEdgeNS64,
                                                          w->gEdgeEW64, T, w->b64, w->r64, w->rr, maxbits);
     pack_residual64<<<1, 384, 0, m->stream>>>(S, w->d_ps, ge_p, link64, gamb_p, T, w->b64, w->r64, w->rr, maxbits);
-    // inner FP32 PCG on G e = r, a fixed number of iterations
     mg_zero<<<nb(n0), MGT, 0, m->stream>>>(w->e, n0);
-    const int inner = 6;
     for (int it = 0; it < inner; it++) {
       vcycle(m, w, 0, w->z, w->rr);
       dot(m, w, w->rr, w->z, n0, sc + 2);
@@ -772,13 +903,40 @@ int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
       dot(m, w, w->p, w->q, n0, sc + 1);
       pcg_update_xr<<<nb(n0), MGT, 0, m->stream>>>(w->e, w->rr, w->p, w->q, sc, n0);
     }
-    add_correction<<<nb(n0), MGT, 0, m->stream>>>(T, w->e, n0);
-    // the l2 norm of this correction (>= its max norm, in K) decides convergence
-    dot(m, w, w->e, w->e, n0, sc + 3);
-    HSB_CUDA(cudaGetLastError());
-    HSB_CUDA(cudaMemcpyAsync(w->h_red, sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, m->stream));
+    // the max norm of this correction (K) decides convergence
+    cudaMemsetAsync(sc + 3, 0, sizeof(double), m->stream);
+    add_correction<<<nb(n0), MGT, 0, m->stream>>>(T, w->e, n0, (unsigned long long *)(sc + 3));
+    cudaMemcpyAsync(w->h_red, sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, m->stream);
+  };
+  if (!w->pass_exec || w->pass_T != T || w->pass_version != m->coef_version) {
+    if (w->pass_exec) {
+      cudaGraphExecDestroy(w->pass_exec);
+      w->pass_exec = nullptr;
+    }
+    cudaGraph_t g;
+    HSB_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+    pass();
+    const cudaError_t ce = cudaStreamEndCapture(m->stream, &g);
+    if (ce != cudaSuccess) return cuda_check(ce, "capturing the multigrid refinement pass");
+    const cudaError_t ie = cudaGraphInstantiate(&w->pass_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      w->pass_exec = nullptr;
+      return cuda_check(ie, "instantiating the multigrid refinement pass");
+    }
+    w->pass_T = T;
+    w->pass_version = m->coef_version;
+  }
+  int refine = 0;
+  double rmax = 0.0, emax = 1e300;
+  for (refine = 0; refine < max_ref; refine++) {
+    HSB_CUDA(cudaGraphLaunch(w->pass_exec, m->stream));
     HSB_CUDA(cudaStreamSynchronize(m->stream));
-    emax = sqrt(w->h_red[3]);
+    {
+      unsigned long long bits;
+      memcpy(&bits, w->h_red + 3, sizeof(bits));
+      memcpy(&emax, &bits, sizeof(emax));
+    }
     st->refinements += 1;
     st->cycles += inner;
     if (emax < tol) break;

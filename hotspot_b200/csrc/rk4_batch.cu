@@ -24,7 +24,9 @@
 // computes the current one, so HBM latency overlaps the stencil arithmetic.
 // Vectors the error pass combines are read with coalesced plain loads.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "fast_common.cuh"
@@ -70,13 +72,13 @@ struct BShared {
   double ps[PMAX];
   unsigned long long bar[BNB];
   int lost;
-  LayerF L[FT_MAX_LAYERS];
+  alignas(16) LayerF L[FT_MAX_LAYERS];
 };
 
 // tile-buffer geometry of a launch (sized for the batch's largest layer count)
 struct BBufs {
   size_t full, kry;   // bytes of one buffer
-  int nkry;           // Krylov-pass ring length
+  int nfull, nkry;    // full-slope buffers (1 or 2), Krylov-pass ring length
 };
 
 struct BCtl {
@@ -96,8 +98,8 @@ enum { BK_FULL = 0, BK_KRY = 1 };
 // smaller FP32 boxes (up to BNB buffers), so more copies are in flight
 __host__ __device__ inline size_t bfull_bytes(int nl) { return al128(al128(8 * (size_t)nl * DP) + 4 * (size_t)nl * NI); }
 __host__ __device__ inline size_t bkry_bytes(int nl) { return al128(4 * (size_t)nl * KP); }
-__host__ __device__ inline int bkry_count(int nl) {
-  const int k = (int)(2 * bfull_bytes(nl) / bkry_bytes(nl));
+__host__ __device__ inline int bkry_count(int nl, int nfull) {
+  const int k = (int)(nfull * bfull_bytes(nl) / bkry_bytes(nl));
   return k < 2 ? 2 : k > BNB ? BNB : k;
 }
 
@@ -209,7 +211,7 @@ __device__ __forceinline__ void bpass(const BChip &C, int rank, int size, BCtl &
   const int p_i = (ty + 1) * W + tx + X0;
   const size_t pw_off = al128(8 * (size_t)nl * DP);
   const size_t bsz = FULL ? bb.full : bb.kry;
-  const int nbuf = FULL ? 2 : bb.nkry;
+  const int nbuf = FULL ? bb.nfull : bb.nkry;
   // the vectors the error pass combines (nonzero coefficient), as a bitmask
   unsigned use = 0u;
   if (ERR)
@@ -242,6 +244,11 @@ __device__ __forceinline__ void bpass(const BChip &C, int rank, int size, BCtl &
     const float *vh = (const float *)buf;
     if (i < nr && j < nc) {
       const long long coff = (long long)i * nc + j;
+      const bool hN = i > 0, hS = i < nr - 1, hE = j < nc - 1, hW = j > 0;
+      // input value at smem index q: FP32 deviation from ambient (FULL) or the vector
+      auto val = [&](int q) -> float { return FULL ? (float)(th[q] - amb) : vh[q]; };
+      // the column is walked top-down; the vertical neighbours come from registers
+      float t_prev = 0.f, t_cur = val(p_i), g_up = 0.f;
       for (int n0 = 0; n0 < nl; n0 += BCH) {
         // error pass: every load of this chunk of layers is issued before the math
         float w[BCH][8];
@@ -261,33 +268,18 @@ __device__ __forceinline__ void bpass(const BChip &C, int rank, int size, BCtl &
           const int n = n0 + u;
           if (n >= nl) break;
           const long long cc = (long long)n * plane + coff;
-          const LayerF &L = sh.L[n];
-          float tc, vN = 0.f, vS = 0.f, vE = 0.f, vW = 0.f, vA = 0.f, vB = 0.f;
           const int q = n * P + p_i;
-          if (FULL) {
-            tc = (float)(th[q] - amb);
-            if (i > 0) vN = (float)(th[q - W] - amb);
-            if (i < nr - 1) vS = (float)(th[q + W] - amb);
-            if (j < nc - 1) vE = (float)(th[q + 1] - amb);
-            if (j > 0) vW = (float)(th[q - 1] - amb);
-            if (n > 0) vA = (float)(th[q - P] - amb);
-            if (n < nl - 1) vB = (float)(th[q + P] - amb);
-          } else {
-            tc = vh[q];
-            if (i > 0) vN = vh[q - W];
-            if (i < nr - 1) vS = vh[q + W];
-            if (j < nc - 1) vE = vh[q + 1];
-            if (j > 0) vW = vh[q - 1];
-            if (n > 0) vA = vh[q - P];
-            if (n < nl - 1) vB = vh[q + P];
-          }
+          const float4 La = *reinterpret_cast<const float4 *>(&sh.L[n]);   // gNS, gEW, gDown, invC
+          const float tc = t_cur;
+          const float t_next = n < nl - 1 ? val(q + P) : 0.f;
           float psum = 0.f;
-          if (i > 0) psum += L.gNS * (vN - tc);
-          if (i < nr - 1) psum += L.gNS * (vS - tc);
-          if (j < nc - 1) psum += L.gEW * (vE - tc);
-          if (j > 0) psum += L.gEW * (vW - tc);
-          if (n > 0) psum += sh.L[n - 1].gDown * (vA - tc);
-          if (n < nl - 1) psum += L.gDown * (vB - tc);
+          if (hN) psum += La.x * (val(q - W) - tc);
+          if (hS) psum += La.x * (val(q + W) - tc);
+          if (hE) psum += La.y * (val(q + 1) - tc);
+          if (hW) psum += La.y * (val(q - 1) - tc);
+          if (n > 0) psum += g_up * (t_prev - tc);
+          if (n < nl - 1) psum += La.z * (t_next - tc);
+          const LayerF &L = sh.L[n];
           if (L.kind != LK_PLAIN) {
             int eN, eS, eE, eW;
             if (L.kind == LK_SPREADER) {
@@ -301,7 +293,10 @@ __device__ __forceinline__ void bpass(const BChip &C, int rank, int size, BCtl &
             if (j == nc - 1) psum += L.gEdgeEW * (sh.xsf[eE] - tc);
             if (j == 0) psum += L.gEdgeEW * (sh.xsf[eW] - tc);
           }
-          const float kv = FULL ? (pw[n * NI + tid] + psum) * L.invC : psum * (L.invC * sf);
+          t_prev = tc;
+          t_cur = t_next;
+          g_up = La.z;
+          const float kv = FULL ? (pw[n * NI + tid] + psum) * La.w : psum * (La.w * sf);
           Nout[cc] = kv;
           if (ERR) {
             // same order as the single-model kernel: E_m N_m, then j ascending
@@ -576,8 +571,14 @@ struct hsb_batch {
   size_t smem = 0;
   cudaStream_t stream = nullptr;
   // schedule
-  int ctas_per_sm = 1;
+  int ctas_per_sm = 2;
   double split = 1.0;        // a chip gets about split * (its share of the work) CTAs
+  int ring = 0;              // Krylov-pass ring length (0: as many as fit)
+  // online autotuning: candidate k runs on call k; the fastest per cell-step wins
+  struct Cand { int cps; double split; int ring; double ms_per_gcs; };
+  std::vector<Cand> cands;
+  int tune_next = -1;        // index of the candidate of the next call, -1: not tuning
+  unsigned long long signature = 0;
   // batched b2g tables
   int *d_cta_off = nullptr;
   int b2g_ctas = 0;
@@ -610,6 +611,18 @@ static void batch_free(hsb_batch *b) {
 static int batch_schedule(hsb_batch *b) {
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
+  // three or more CTAs per SM: one FP64 box buffer (no prefetch in the
+  // full-slope pass) so that the shared memory of three CTAs fits an SM
+  b->bsz.nfull = b->ctas_per_sm >= 3 ? 1 : 2;
+  b->bsz.full = bfull_bytes(b->nlmax);
+  b->bsz.kry = bkry_bytes(b->nlmax);
+  b->bsz.nkry = bkry_count(b->nlmax, b->bsz.nfull);
+  if (b->ring > 0 && b->ring < b->bsz.nkry) b->bsz.nkry = b->ring;
+  size_t ring = b->bsz.kry * b->bsz.nkry;
+  size_t dyn = b->bsz.nfull * b->bsz.full;
+  b->smem = (ring > dyn ? ring : dyn) + 128;
+  HSB_CUDA(cudaFuncSetAttribute((const void *)rk4_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)b->smem));
   int per_sm = 0;
   HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)rk4_batch_kernel, FT_THREADS,
                                                          b->smem));
@@ -778,13 +791,6 @@ int hsb_batch_create(hsb_batch **out, hsb_dev_model *const *models, int n) {
   std::vector<long long> init(BOUT * (size_t)n, 0);
   if (cudaMemcpy(b->d_out, init.data(), sizeof(long long) * BOUT * n, cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(set_error(HSB_E_CUDA, "batch outputs"));
-  b->bsz.full = bfull_bytes(b->nlmax);
-  b->bsz.kry = bkry_bytes(b->nlmax);
-  b->bsz.nkry = bkry_count(b->nlmax);
-  b->smem = 2 * b->bsz.full + 128;
-  if (cudaFuncSetAttribute((const void *)rk4_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)b->smem) != cudaSuccess)
-    return fail(set_error(HSB_E_ARG, "batch kernel shared memory too large (too many layers)"));
   if ((rc = batch_schedule(b))) return fail(rc);
   // batched b2g tables
   {
@@ -848,6 +854,51 @@ int hsb_batch_set_schedule(hsb_batch *b, int ctas_per_sm, double split) {
   return batch_schedule(b);
 }
 
+// schedules chosen by the autotuner, by batch shape (process-wide)
+static std::mutex g_tune_mu;
+static std::vector<std::pair<unsigned long long, hsb_batch::Cand>> g_tuned;
+
+static unsigned long long batch_signature(const hsb_batch *b) {
+  std::vector<unsigned long long> keys;
+  for (auto &C : b->h_chips) keys.push_back(((unsigned long long)C.nl << 40) | ((unsigned long long)C.nr << 20) | C.nc);
+  std::sort(keys.begin(), keys.end());
+  unsigned long long h = 1469598103934665603ull;
+  for (auto k : keys) {
+    h ^= k;
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+int hsb_batch_autotune(hsb_batch *b, int enable) {
+  if (!b) return set_error(HSB_E_ARG, "null batch");
+  if (!enable) {
+    b->tune_next = -1;
+    return HSB_OK;
+  }
+  b->signature = batch_signature(b);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (auto &e : g_tuned)
+      if (e.first == b->signature) {   // tuned before: reuse
+        b->ctas_per_sm = e.second.cps;
+        b->split = e.second.split;
+        b->ring = e.second.ring;
+        b->tune_next = -1;
+        return batch_schedule(b);
+      }
+  }
+  b->cands.clear();
+  const int cps[2] = {2, 1};
+  const double split[3] = {1.0, 1.5, 0.75};
+  const int ring[2] = {0, 2};
+  for (int a : cps)
+    for (double sp : split)
+      for (int r : ring) b->cands.push_back({a, sp, r, 0.0});
+  b->tune_next = 0;
+  return HSB_OK;
+}
+
 int hsb_batch_info(hsb_batch *b, int *grid, long long *cells, int *ctas_per_sm, double *split) {
   if (!b) return set_error(HSB_E_ARG, "null batch");
   long long n = 0;
@@ -864,6 +915,17 @@ int hsb_batch_transient(hsb_batch *b, const double *block_power, double time_ela
   hsb_stats local;
   if (!st) st = &local;
   cudaSetDevice(b->device);
+  const int tuning = b->tune_next;
+  if (tuning >= 0) {
+    const hsb_batch::Cand &c = b->cands[tuning];
+    b->ctas_per_sm = c.cps;
+    b->split = c.split;
+    b->ring = c.ring;
+    int rc0;
+    if ((rc0 = batch_schedule(b))) return rc0;
+  }
+  const long long steps0 = st->rk4_steps;
+  const double kms0 = st->kernel_ms;
   cudaEvent_t e0, e1, k0, k1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -942,7 +1004,44 @@ int hsb_batch_transient(hsb_batch *b, const double *block_power, double time_ela
   cudaEventDestroy(e1);
   cudaEventDestroy(k0);
   cudaEventDestroy(k1);
+  if (tuning >= 0 && rc == HSB_OK) {
+    // kernel time per 10^9 cell-steps of this call
+    double cs = 0.0;
+    for (int c = 0; c < b->n; c++) cs += (double)b->h_out[(size_t)c * BOUT] * b->models[c]->ncell;
+    (void)steps0;
+    b->cands[tuning].ms_per_gcs = cs > 0 ? (st->kernel_ms - kms0) / (cs / 1e9) : 1e300;
+    b->tune_next = tuning + 1;
+    if (b->tune_next >= (int)b->cands.size()) {
+      int best = 0;
+      for (int k = 1; k < (int)b->cands.size(); k++)
+        if (b->cands[k].ms_per_gcs < b->cands[best].ms_per_gcs) best = k;
+      const hsb_batch::Cand c = b->cands[best];
+      b->ctas_per_sm = c.cps;
+      b->split = c.split;
+      b->ring = c.ring;
+      b->tune_next = -1;
+      {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned.push_back({b->signature, c});
+      }
+      rc = batch_schedule(b);
+    }
+  }
   return rc;
+}
+
+// the autotuner's measurements: up to n candidates as (ctas_per_sm, split,
+// ring, ms per 10^9 cell-steps); returns how many were measured
+int hsb_batch_tuning(hsb_batch *b, double *out, int n) {
+  if (!b) return set_error(HSB_E_ARG, "null batch");
+  int k = 0;
+  for (; k < (int)b->cands.size() && k < n; k++) {
+    out[4 * k] = b->cands[k].cps;
+    out[4 * k + 1] = b->cands[k].split;
+    out[4 * k + 2] = b->cands[k].ring;
+    out[4 * k + 3] = b->cands[k].ms_per_gcs;
+  }
+  return k;
 }
 
 // per-chip accepted steps of the last call (n entries)

@@ -787,9 +787,17 @@ __global__ void bc_shift_scalars(double *sc) {
   sc[SC_RHO_OLD] = sc[SC_RHO];
 }
 
-__global__ void bc_add_correction(double *__restrict__ T, const float *__restrict__ e, long long n) {
+// T += e; the max |e| (K) into *emax_bits (zeroed by the caller)
+__global__ void bc_add_correction(double *__restrict__ T, const float *__restrict__ e, long long n,
+                                  unsigned long long *emax_bits) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) T[k] += (double)e[k];
+  double a = 0.0;
+  if (k < n) {
+    T[k] += (double)e[k];
+    a = fabs((double)e[k]);
+  }
+  for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
+  if ((threadIdx.x & 31) == 0 && a > 0.0) atomicMax(emax_bits, (unsigned long long)__double_as_longlong(a));
 }
 
 // heuristic start: the ambient temperature everywhere
@@ -1122,8 +1130,9 @@ static void bc_pass(hsb_dev_model *m, BcWork *w, double *T, int inner, long long
     bc_shift_scalars<<<1, 1, 0, m->stream>>>(sc);
     *launches += 16;
   }
-  bc_add_correction<<<bnb(n0), BCT, 0, m->stream>>>(T, w->e, n0);
-  bc_dot2(m, w, w->e, w->e, nullptr, nullptr, n0, sc + SC_NE, nullptr);
+  // the max norm of this correction (K) decides convergence
+  cudaMemsetAsync(sc + SC_NE, 0, sizeof(double), m->stream);
+  bc_add_correction<<<bnb(n0), BCT, 0, m->stream>>>(T, w->e, n0, (unsigned long long *)(sc + SC_NE));
   *launches += 3;
   cudaMemcpyAsync(w->h_red, sc, sizeof(double) * (SC_MAX + 1), cudaMemcpyDeviceToHost, m->stream);
   cudaMemcpyAsync(w->h_red + 12, w->status, sizeof(int), cudaMemcpyDeviceToHost, m->stream);
@@ -1183,7 +1192,11 @@ int bicgstab_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
     HSB_CUDA(cudaGraphLaunch(w->pass_exec, m->stream));
     HSB_CUDA(cudaStreamSynchronize(m->stream));
     launches += w->pass_launches;
-    emax = sqrt(w->h_red[SC_NE]);
+    {
+      unsigned long long bits;
+      memcpy(&bits, w->h_red + SC_NE, sizeof(bits));
+      memcpy(&emax, &bits, sizeof(emax));
+    }
     int lost = 0;
     memcpy(&lost, w->h_red + 12, sizeof(int));
     if (lost) return set_error(HSB_E_CUDA, "BiCGStab plane solve: a chunk copy did not complete in time");

@@ -167,6 +167,14 @@ int  hsb_batch_set_schedule(hsb_batch *b, int ctas_per_sm, double split);
 int  hsb_batch_info(hsb_batch *b, int *grid, long long *cells, int *ctas_per_sm, double *split);
 /* accepted RK4 steps of each model in the last call (n entries) */
 int  hsb_batch_chip_steps(hsb_batch *b, long long *steps);
+/* autotuner: when enabled, the next calls each run one candidate schedule
+ * (CTAs per SM, split, Krylov-pass ring length) on the real work -- the
+ * schedule never changes the results -- and the fastest per cell-step is
+ * kept, and remembered for batches of the same shape in this process */
+int  hsb_batch_autotune(hsb_batch *b, int enable);
+/* the autotuner's measurements: 4 doubles per candidate (ctas_per_sm, split,
+ * ring, ms per 1e9 cell-steps), up to n candidates; returns the count */
+int  hsb_batch_tuning(hsb_batch *b, double *out, int n);
 
 /* which: 0 = transient state (last_trans), 1 = steady state (last_steady);
  * n = nl*nr*nc + n_extra doubles */

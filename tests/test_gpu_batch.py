@@ -69,3 +69,35 @@ def test_batch_schedules(workdir, schedule):
     scs = _chips(workdir, [("stack3d", 128), ("chip2d", 32), ("chip2d", 64), ("stack3d", 64)] * 2)
     errs, s1, s2, info = _run(scs, 3, schedule)
     assert np.array_equal(s1, s2) and max(errs) <= 1e-9, (errs, info)
+
+
+def test_batch_autotuner(workdir):
+    """The autotuner runs each candidate schedule on a real interval; results
+    stay bit-identical to the single-model form and a measured candidate wins."""
+    scs = _chips(workdir, [("stack3d", 64), ("chip2d", 32), ("chip2d", 64)] * 2)
+    for sc in scs:
+        sc.block_power = np.repeat(sc.block_power, 3, axis=0)
+    single, batched = [], []
+    for sc in scs:
+        for lst in (single, batched):
+            m = hm.from_scenario(sc)
+            m.set_solver(FORM_FAST)
+            t = m.vector(m.config.init_temp)
+            m.compute_temp(m.power_vector(sc.block_power[0]), t, 0.0)
+            lst.append(m)
+    bt = Batch(batched)
+    bt.autotune(True)
+    for k in range(1, 15):
+        for sc, a in zip(scs, single):
+            a.compute_temp(a.power_vector(sc.block_power[k]), None, sc.dt)
+        bt.transient([b.power_vector(sc.block_power[k]) for sc, b in zip(scs, batched)], scs[0].dt)
+    tun = bt.tuning()
+    info = bt.info()
+    errs = [float(np.max(np.abs(a.grid("trans") - b.grid("trans")))) for a, b in zip(single, batched)]
+    bt.close()
+    for m in single + batched:
+        m.close()
+    assert len(tun) == 12 and all(t["ms_per_gcell_step"] > 0 for t in tun)
+    best = min(tun, key=lambda t: t["ms_per_gcell_step"])
+    assert info["ctas_per_sm"] == best["ctas_per_sm"] and info["split"] == best["split"]
+    assert max(errs) <= 1e-9, errs
