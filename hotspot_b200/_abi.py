@@ -133,6 +133,17 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Request(C.Structure):
+    """hsb_request (hsb_device.h)."""
+    _fields_ = [("model", C.c_int), ("kind", C.c_int), ("steps", C.c_int), ("dt", C.c_double),
+                ("power", C.c_void_p), ("temp_in", C.c_void_p), ("out", C.c_void_p),
+                ("arrival", C.c_double), ("start", C.c_double), ("finish", C.c_double),
+                ("status", C.c_int), ("worker", C.c_int)]
+
+
+REQ_STEADY, REQ_TRANSIENT = 0, 1
+
+
 class GridDesc(C.Structure):
     """hsb_grid_desc (hsb_device.h)."""
     _fields_ = [("nl", C.c_int), ("nr", C.c_int), ("nc", C.c_int), ("n_extra", C.c_int),
@@ -225,6 +236,10 @@ _SIGS = {
                                  C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "hsb_batch_chip_steps": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     "hsb_batch_autotune": (C.c_int, [C.c_void_p, C.c_int]),
+    "hsb_server_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_longlong]),
+    "hsb_server_destroy": (None, [C.c_void_p]),
+    "hsb_server_add_model": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_longlong]),
+    "hsb_server_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "hsb_batch_tuning": (C.c_int, [C.c_void_p, _D, C.c_int]),
 }
 

@@ -1,0 +1,186 @@
+// serve.cu -- the serving loop: steady and transient requests over resident
+// models, with continuous admission.
+//
+// Models are registered once and stay resident on the device (state,
+// coefficients and solver workspaces).  hsb_server_run() releases every
+// request at its arrival time (seconds after the run starts) and keeps
+// `workers` requests in flight: as soon as one finishes, the next request
+// that has arrived, whose model is idle, and that passes admission starts
+// on the freed worker.  Each request runs on its own model's CUDA stream,
+// so the work of the requests in flight overlaps on the device.
+//
+// Admission: a model's first request allocates its solver workspace, so it
+// is admitted only while the device's free memory (cudaMemGetInfo) exceeds
+// the model's declared workspace plus the reserve; later requests of that
+// model allocate nothing.  Among admissible requests the one with the least
+// estimated work (cells x passes) goes first, so short requests are not
+// held behind long ones; ties go to the earlier arrival.
+//
+// Each request's result depends only on its model and inputs: the kernels
+// are deterministic and models share no mutable device state, so a result
+// is the same alone and in any mix.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "dev_model.cuh"
+
+struct hsb_server {
+  int workers = 1;
+  long long reserve = 0;
+  struct Model {
+    hsb_dev_model *m;
+    hsb_solver_opts opts;
+    long long workspace;
+    bool warm = false;   // workspace allocated by an earlier request
+    bool busy = false;
+  };
+  std::vector<Model> models;
+};
+
+using namespace hsb;
+
+extern "C" {
+
+int hsb_server_create(hsb_server **out, int workers, long long reserve_bytes) {
+  if (!out || workers < 1) return set_error(HSB_E_ARG, "bad server arguments");
+  hsb_server *s = new hsb_server();
+  s->workers = workers;
+  s->reserve = reserve_bytes;
+  *out = s;
+  return HSB_OK;
+}
+
+void hsb_server_destroy(hsb_server *s) { delete s; }
+
+int hsb_server_add_model(hsb_server *s, hsb_dev_model *m, int form, double steady_tol, long long workspace_bytes) {
+  if (!s || !m) return set_error(HSB_E_ARG, "null argument");
+  hsb_server::Model e;
+  e.m = m;
+  e.opts.form = form;
+  e.opts.steady_method = HSB_STEADY_AUTO;
+  e.opts.steady_tol = steady_tol;
+  e.opts.max_iters = 0;
+  e.workspace = workspace_bytes;
+  s->models.push_back(e);
+  return (int)s->models.size() - 1;
+}
+
+// one request, synchronously, on the calling thread
+static int run_request(hsb_server::Model &M, hsb_request *r) {
+  hsb_dev_model *m = M.m;
+  const size_t nb = (size_t)m->total_n_blocks + m->nx;
+  hsb_stats st;
+  memset(&st, 0, sizeof(st));
+  if (cudaSetDevice(m->device) != cudaSuccess) return set_error(HSB_E_CUDA, "cudaSetDevice");
+  if (r->kind == HSB_REQ_STEADY) return hsb_dev_steady(m, r->power, r->out, &M.opts, &st);
+  if (r->kind != HSB_REQ_TRANSIENT || r->steps < 1) return set_error(HSB_E_ARG, "bad request kind or step count");
+  for (int k = 0; k < r->steps; k++) {
+    const int rc = hsb_dev_transient(m, r->power + (size_t)k * nb, k == 0 ? r->temp_in : nullptr, r->dt,
+                                     k == r->steps - 1 ? r->out : nullptr, &M.opts, &st);
+    if (rc) return rc;
+  }
+  return HSB_OK;
+}
+
+int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
+  if (!s || (!reqs && n > 0)) return set_error(HSB_E_ARG, "null argument");
+  for (int k = 0; k < n; k++)
+    if (reqs[k].model < 0 || reqs[k].model >= (int)s->models.size())
+      return set_error(HSB_E_ARG, "request names an unknown model");
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<int> state(n, 0);   // 0 pending, 1 running, 2 done
+  int done = 0, running = 0;
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
+  auto now = [&]() { return std::chrono::duration<double>(clk::now() - t0).count(); };
+  auto cost = [&](const hsb_request &r) {
+    const double cells = (double)s->models[r.model].m->ncell;
+    return cells * (r.kind == HSB_REQ_STEADY ? 40.0 : 8.0 * 4.0 * r.steps);
+  };
+  auto worker = [&](int wid) {
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+      if (done == n) return;
+      const double t = now();
+      int best = -1;
+      double next_arrival = 1e300;
+      size_t free_b = 0, total_b = 0;
+      bool mem_known = false;
+      for (int k = 0; k < n; k++) {
+        if (state[k] != 0) continue;
+        const hsb_request &r = reqs[k];
+        if (r.arrival > t) {
+          next_arrival = std::min(next_arrival, r.arrival);
+          continue;
+        }
+        hsb_server::Model &M = s->models[r.model];
+        if (M.busy) continue;
+        if (!M.warm) {   // first use: admission by free device memory
+          if (!mem_known) {
+            cudaSetDevice(M.m->device);
+            cudaMemGetInfo(&free_b, &total_b);
+            mem_known = true;
+          }
+          if ((long long)free_b < M.workspace + s->reserve) continue;
+        }
+        if (best < 0 || cost(r) < cost(reqs[best]) ||
+            (cost(r) == cost(reqs[best]) && r.arrival < reqs[best].arrival))
+          best = k;
+      }
+      if (best < 0 && running == 0 && next_arrival >= 1e300) {
+        // nothing runs, nothing more arrives: what is left waits on memory
+        // that no request will free -- fail those requests
+        for (int k = 0; k < n; k++)
+          if (state[k] == 0 && reqs[k].arrival <= t && !s->models[reqs[k].model].busy) {
+            reqs[k].status = set_error(HSB_E_NOMEM, "request not admitted: not enough free device memory");
+            reqs[k].start = reqs[k].finish = t;
+            state[k] = 2;
+            done++;
+          }
+        cv.notify_all();
+        continue;
+      }
+      if (best < 0) {
+        if (next_arrival < 1e300)
+          cv.wait_until(lk, t0 + std::chrono::duration_cast<clk::duration>(std::chrono::duration<double>(next_arrival)));
+        else
+          cv.wait(lk);
+        continue;
+      }
+      hsb_request &r = reqs[best];
+      hsb_server::Model &M = s->models[r.model];
+      state[best] = 1;
+      running++;
+      M.busy = true;
+      r.start = t;
+      r.worker = wid;
+      lk.unlock();
+      const int rc = run_request(M, &r);
+      lk.lock();
+      r.finish = now();
+      r.status = rc;
+      if (rc == HSB_OK) M.warm = true;
+      M.busy = false;
+      state[best] = 2;
+      running--;
+      done++;
+      cv.notify_all();
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int w = 0; w < s->workers; w++) pool.emplace_back(worker, w);
+  for (auto &th : pool) th.join();
+  int failed = 0;
+  for (int k = 0; k < n; k++)
+    if (reqs[k].status != HSB_OK) failed++;
+  if (failed) return set_error(HSB_E_CUDA, "some requests failed (see their status)");
+  return HSB_OK;
+}
+
+}  // extern "C"

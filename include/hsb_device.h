@@ -176,6 +176,41 @@ int  hsb_batch_autotune(hsb_batch *b, int enable);
  * ring, ms per 1e9 cell-steps), up to n candidates; returns the count */
 int  hsb_batch_tuning(hsb_batch *b, double *out, int n);
 
+/* ---- serving (no counterpart in the reference): steady and transient
+ * requests over resident models, admitted continuously.  Each request runs
+ * on its model's stream, so the requests in flight overlap on the device; a
+ * model serves one request at a time.  A request starts once it has arrived,
+ * its model is idle, a worker is free and -- on the model's first request,
+ * which allocates its solver workspace -- the device's free memory exceeds
+ * that workspace plus the reserve; the least estimated work goes first. */
+#define HSB_REQ_STEADY    0
+#define HSB_REQ_TRANSIENT 1
+
+typedef struct hsb_request {
+  int model;                 /* index from hsb_server_add_model */
+  int kind;                  /* HSB_REQ_STEADY or HSB_REQ_TRANSIENT */
+  int steps;                 /* transient: sampling intervals */
+  double dt;                 /* transient: interval length (s) */
+  const double *power;       /* host block powers: 1 vector (steady) or `steps` vectors (transient) */
+  const double *temp_in;     /* transient: initial block temperatures, or NULL to continue the state */
+  double *out;               /* host block temperatures at the end (total_n_blocks + n_extra) */
+  double arrival;            /* seconds after the start of hsb_server_run */
+  double start, finish;      /* written by the server: seconds after the start */
+  int status;                /* written by the server: HSB_OK or an HSB_E_* code */
+  int worker;                /* written by the server */
+} hsb_request;
+
+struct hsb_server;
+typedef struct hsb_server hsb_server;
+int  hsb_server_create(hsb_server **out, int workers, long long reserve_bytes);
+void hsb_server_destroy(hsb_server *s);
+/* register a resident model; form HSB_FORM_*, steady_tol (K, 0 = default),
+ * workspace_bytes = device memory its first solve allocates; returns its index */
+int  hsb_server_add_model(hsb_server *s, hsb_dev_model *m, int form, double steady_tol,
+                          long long workspace_bytes);
+/* serve n requests (released at their arrival times); returns when all are done */
+int  hsb_server_run(hsb_server *s, hsb_request *reqs, int n);
+
 /* which: 0 = transient state (last_trans), 1 = steady state (last_steady);
  * n = nl*nr*nc + n_extra doubles */
 int hsb_dev_get_state(hsb_dev_model *m, int which, double *out);

@@ -1,0 +1,81 @@
+"""Serving loop (hsb_server_run): requests over resident models, admitted
+continuously, several in flight on their models' streams.  Every result must
+be the same alone and in the mix (bit for bit: the kernels are
+deterministic and models share no device state), and the steady results
+must meet the 0.01 K bar against the converged FP64 solution."""
+import numpy as np
+import pytest
+
+from hotspot_b200 import _abi
+from hotspot_b200 import model as hm
+from hotspot_b200 import workloads as W
+from hotspot_b200.serving import Request, Server, latency_report
+from oracle.restatement import OracleModel
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(server, scs, models, rng, n, rate):
+    reqs, t = [], 0.0
+    for k in range(n):
+        t += rng.exponential(1.0 / rate)
+        mi = int(rng.integers(0, len(models)))
+        m, sc = models[mi], scs[mi]
+        nblk = sum(m.layer_units[l] for l in range(m.n_layers) if m.layer_power[l])
+        if mi < 2:
+            reqs.append(Request(mi, _abi.REQ_STEADY, m.power_vector(rng.uniform(0.5, 20.0, nblk)), t,
+                                tag=f"steady{mi}"))
+        else:
+            trace = W.ar1_power(rng, rng.uniform(0.5, 20.0, nblk), 12)
+            p = np.stack([m.power_vector(trace[s]) for s in range(12)])
+            reqs.append(Request(mi, _abi.REQ_TRANSIENT, p, t, temp_in=m.vector(m.config.init_temp), steps=12,
+                                dt=3.333e-6, tag="transient"))
+    return reqs
+
+
+def test_alone_equals_mixed(workdir):
+    rng = np.random.default_rng(90)
+    scs = [W.scenario_random_chip(workdir, rng, "a", side=64, chip_layers=2, steps=0),
+           W.scenario_random_chip(workdir, rng, "b", side=128, chip_layers=3, steps=0),
+           W.scenario_random_chip(workdir, rng, "c", side=64, chip_layers=4, steps=0)]
+    models = [hm.from_scenario(sc) for sc in scs]
+    srv = Server(workers=4)
+    for m in models:
+        srv.add_model(m, _abi.FORM_FAST, 1e-6)
+    mixed = _requests(srv, scs, models, np.random.default_rng(91), 24, 4000.0)
+    # alone: the same requests one at a time
+    alone = [Request(r.model, r.kind, r.power, 0.0, r.temp_in, r.steps, r.dt, r.tag) for r in mixed]
+    for r in alone:
+        srv.run([r])
+    srv.run(mixed)
+    for a, b in zip(alone, mixed):
+        assert a.status == 0 and b.status == 0
+        assert np.array_equal(a.out, b.out), (a.tag, np.max(np.abs(a.out - b.out)))
+    # overlap: some requests were in flight together
+    spans = sorted((r.start, r.finish) for r in mixed)
+    assert any(spans[k + 1][0] < spans[k][1] for k in range(len(spans) - 1))
+    # the steady answers against the converged FP64 solution
+    for r in mixed[:6]:
+        if r.kind == _abi.REQ_STEADY:
+            T, Tb = OracleModel(scs[r.model]).steady_direct(r.power)
+            assert np.max(np.abs(r.out - Tb)) <= 0.01
+    rep = latency_report(mixed)
+    assert rep["n"] == len(mixed) and rep["p99_ms"] >= rep["p50_ms"] > 0
+    srv.close()
+    for m in models:
+        m.close()
+
+
+def test_admission_refuses_what_does_not_fit(workdir):
+    rng = np.random.default_rng(92)
+    sc = W.scenario_random_chip(workdir, rng, "d", side=64, chip_layers=2, steps=0)
+    m = hm.from_scenario(sc)
+    srv = Server(workers=2, reserve_bytes=1 << 62)      # no request can be admitted
+    srv.add_model(m, _abi.FORM_FAST, 1e-6)
+    nblk = sum(m.layer_units[l] for l in range(m.n_layers) if m.layer_power[l])
+    r = Request(0, _abi.REQ_STEADY, m.power_vector(np.ones(nblk)), 0.0)
+    with pytest.raises(Exception):
+        srv.run([r])
+    assert r.status == -3                               # HSB_E_NOMEM
+    srv.close()
+    m.close()
