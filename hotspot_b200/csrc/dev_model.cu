@@ -3,6 +3,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "dev_model.cuh"
@@ -19,6 +21,24 @@ int set_error(int code, const std::string &msg) {
 int cuda_check(cudaError_t e, const char *what) {
   return set_error(e == cudaErrorMemoryAllocation ? HSB_E_NOMEM : HSB_E_CUDA,
                    std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// The dynamic shared memory limit is a per-function (per-device) setting
+// shared by every thread and model: it is only ever raised, under a lock, so
+// a model needing less can never lower it below what another model in
+// flight launched with.
+int raise_smem_limit(const void *fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, size_t> cur;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  size_t &have = cur[{dev, fn}];
+  if (bytes <= have) return HSB_OK;
+  const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return cuda_check(e, "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
+  have = bytes;
+  return HSB_OK;
 }
 
 StencilArgs make_args(const hsb_dev_model *m, const LayerCoef *L, int nr, int nc) {

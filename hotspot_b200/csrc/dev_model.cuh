@@ -118,6 +118,8 @@ namespace hsb {
 StencilArgs make_args(const hsb_dev_model *m, const LayerCoef *L, int nr, int nc);
 int set_error(int code, const std::string &msg);
 int cuda_check(cudaError_t e, const char *what);
+// raise (never lower) a kernel's dynamic shared memory limit, thread-safe
+int raise_smem_limit(const void *fn, size_t bytes);
 
 // b2g / g2b on the device (temperature_grid.c:1888-2015)
 int b2g(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type);

@@ -298,7 +298,7 @@ static int segmax_of(const hsb_dev_model *m) {
 
 // co-resident grid of a cooperative launch over the model's tiles
 static int coop_grid(const hsb_dev_model *m, const void *fn, size_t smem, int *grid) {
-  HSB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  { const int rc0 = raise_smem_limit(fn, smem); if (rc0) return rc0; }
   int per_sm = 0, nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
   HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FT_THREADS, smem));

@@ -435,7 +435,7 @@ static int gs_level(hsb_dev_model *m, const StencilArgs &A, double *v, const dou
     const int ms = (int)((cap - total) < chunk ? (cap - total) : chunk);
     if (A.field) {
       if (use_smem) {
-        cudaFuncSetAttribute(gs_sweeps<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        raise_smem_limit((const void *)gs_sweeps<true, true>, smem);
         gs_sweeps<true, true><<<1, GS_THREADS, smem, m->stream>>>(A, v, p, ms, m->gs_status, m->gs_delta,
             m->spidx, m->hsidx, m->subidx, m->solderidx, m->pcbidx);
       } else {
@@ -444,7 +444,7 @@ static int gs_level(hsb_dev_model *m, const StencilArgs &A, double *v, const dou
       }
     } else {
       if (use_smem) {
-        cudaFuncSetAttribute(gs_sweeps<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        raise_smem_limit((const void *)gs_sweeps<false, true>, smem);
         gs_sweeps<false, true><<<1, GS_THREADS, smem, m->stream>>>(A, v, p, ms, m->gs_status, m->gs_delta,
             m->spidx, m->hsidx, m->subidx, m->solderidx, m->pcbidx);
       } else {

@@ -621,8 +621,10 @@ static int batch_schedule(hsb_batch *b) {
   size_t ring = b->bsz.kry * b->bsz.nkry;
   size_t dyn = b->bsz.nfull * b->bsz.full;
   b->smem = (ring > dyn ? ring : dyn) + 128;
-  HSB_CUDA(cudaFuncSetAttribute((const void *)rk4_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)b->smem));
+  {
+    const int rc0 = raise_smem_limit((const void *)rk4_batch_kernel, b->smem);
+    if (rc0) return rc0;
+  }
   int per_sm = 0;
   HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)rk4_batch_kernel, FT_THREADS,
                                                          b->smem));

@@ -24,6 +24,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -96,6 +97,7 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
   std::condition_variable cv;
   std::vector<int> state(n, 0);   // 0 pending, 1 running, 2 done
   int done = 0, running = 0;
+  std::string first_error;        // message of the first failed request
   using clk = std::chrono::steady_clock;
   const auto t0 = clk::now();
   auto now = [&]() { return std::chrono::duration<double>(clk::now() - t0).count(); };
@@ -165,6 +167,7 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
       lk.lock();
       r.finish = now();
       r.status = rc;
+      if (rc != HSB_OK && first_error.empty()) first_error = hsb_dev_last_error();
       if (rc == HSB_OK) M.warm = true;
       M.busy = false;
       state[best] = 2;
@@ -179,7 +182,9 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
   int failed = 0;
   for (int k = 0; k < n; k++)
     if (reqs[k].status != HSB_OK) failed++;
-  if (failed) return set_error(HSB_E_CUDA, "some requests failed (see their status)");
+  if (failed)
+    return set_error(HSB_E_CUDA, std::to_string(failed) + " request(s) failed (see their status); first: " +
+                                     (first_error.empty() ? std::string("not admitted") : first_error));
   return HSB_OK;
 }
 

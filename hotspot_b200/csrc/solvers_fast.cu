@@ -906,8 +906,7 @@ static int bc_setup(hsb_dev_model *m, BcWork **out) {
   w->tpb = (int)(200 * 1024 / per);
   if (w->tpb > 32) w->tpb = 32;
   if (w->tpb < 1) w->tpb = 1;
-  if (cudaFuncSetAttribute((const void *)solve_for(nl), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)bc_solve_smem(nl, w->R, w->tpb)) != cudaSuccess)
+  if (raise_smem_limit((const void *)solve_for(nl), bc_solve_smem(nl, w->R, w->tpb)) != HSB_OK)
     return fail(set_error(HSB_E_CUDA, "BiCGStab plane solver shared memory"));
   *out = w;
   return HSB_OK;
