@@ -16,6 +16,16 @@ seeded 40-block floorplan per silicon layer with 0.1-2 W/mm^2, power rows at
              the plain FP64 form (exact replay of the reference's solver)
   accuracy   max |dT| of the fast form against the plain FP64 form
 
+Further legs on one GPU (skipped under torchrun and with --headline-only):
+  batched       512 synthetic chips of uneven size (sides 32..512, 1..8 chip
+                layers) advanced together, one persistent launch per interval
+                (autotuned schedule), cell-steps/s and its HBM roofline
+  microchannel  512x512 Si + water-channel stack, non-symmetric steady system
+                by FP32 BiCGStab + FP64 refinement, solves/s and residual
+  serving       the seeded request mix (Poisson arrivals at 2000 req/s, 70%
+                steady 64..1024 sides, 30% 500-interval transients), latency
+                percentiles and throughput of the serving loop
+
 Multi-GPU: independent replicas (one chip per rank, weak scaling); the
 timed region is bracketed by barriers and the max over ranks is reported.
 
@@ -46,13 +56,18 @@ ALG_BYTES_FP64 = 200   # per cell-step, all FP64
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", type=int, default=256)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison legs")
     ap.add_argument("--profile", action="store_true",
                     help="transient intervals of the fast form only (the case profiled with ncu)")
+    ap.add_argument("--headline-only", action="store_true", help="skip the batched / microchannel / serving legs")
+    ap.add_argument("--batch-chips", type=int, default=512)
+    ap.add_argument("--batch-intervals", type=int, default=10)
+    ap.add_argument("--serving-seconds", type=float, default=0.25,
+                    help="length of the request arrival window of the serving leg")
     return ap.parse_args()
 
 
@@ -201,6 +216,143 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# further legs (one GPU)
+# ---------------------------------------------------------------------------
+def leg_batched(args, flush):
+    """512 synthetic chips advanced together by hsb_batch_transient."""
+    import torch
+    from hotspot_b200 import FORM_FAST
+    from hotspot_b200 import model as hm
+    from hotspot_b200 import workloads as W
+    from hotspot_b200.batch import Batch
+    K = args.batch_intervals
+    rng = np.random.default_rng(2024)
+    d = tempfile.mkdtemp(prefix="hsb_batch_")
+    t0 = time.perf_counter()
+    scs = [W.scenario_random_chip(d, rng, f"c{i}", steps=K + 16) for i in range(args.batch_chips)]
+    models = []
+    for sc in scs:
+        m = hm.from_scenario(sc)
+        m.set_solver(FORM_FAST)
+        t = m.vector(m.config.init_temp)
+        m.compute_temp(m.power_vector(sc.block_power[0]), t, 0.0)
+        models.append(m)
+    setup_s = time.perf_counter() - t0
+    cells = np.array([m.n_cells for m in models], dtype=np.float64)
+    bt = Batch(models)
+    dt = scs[0].dt
+
+    def pw(k):
+        return [m.power_vector(sc.block_power[k]) for sc, m in zip(scs, models)]
+    bt.autotune(True)
+    k = 1
+    for _ in range(len(bt.tuning())):      # the autotuner tries one candidate schedule per call
+        bt.transient(pw(k), dt)
+        k += 1
+    tuned = dict(bt.info(), candidates=len(bt.tuning()))
+    kms = cs = 0.0
+    launches = 0
+    for j in range(k, k + K):
+        flush.fill_(float(j))
+        torch.cuda.synchronize()
+        st = bt.transient(pw(j), dt)
+        kms += st["kernel_ms"]
+        launches += st["launches"]
+        cs += float(np.sum(bt.chip_steps() * cells))
+    rate = cs / (kms / 1e3)
+    peak, peak_kind = measured_peak()
+    achieved = ALG_BYTES_FP32 * rate / 1e9
+    bt.close()
+    for m in models:
+        m.close()
+    return {"workload": f"{args.batch_chips} chips, sides 2^5..2^9, 1..8 chip layers + spreader/sink, "
+                        "10..100 blocks, 3.333 us intervals", "cells": int(cells.sum()),
+            "cell_steps_per_s": rate, "intervals": K, "ms_per_interval": kms / K,
+            "schedule": tuned, "setup_s": setup_s, "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "rk4_batch_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": profiled_traffic("rk4_batch_kernel.md"),
+                         "note": "108 B per cell-step (FP32 stages, FP64 state); traffic per launch of the "
+                                 "profiled small batch"},
+            "l2": "256 MB buffer rewritten between intervals; 265M cells >> L2 anyway"}
+
+
+def leg_microchannel(args):
+    """512x512 microchannel steady state by BiCGStab, and the CPU direct solve on 128x128."""
+    from hotspot_b200 import FORM_FAST, STEADY_BICGSTAB
+    from hotspot_b200 import model as hm
+    from hotspot_b200 import workloads as W
+    d = tempfile.mkdtemp(prefix="hsb_uchan_")
+    out = {}
+    for grid in (512, 128):
+        kw = {} if grid == 512 else {"die": grid * 20e-6, "blocks": 8}
+        sc = W.scenario_microchannel(d, seed=3, grid=grid, **kw)
+        m = hm.from_scenario(sc)
+        m.set_solver(FORM_FAST, STEADY_BICGSTAB)
+        p = m.power_vector(sc.block_power[0])
+        s = m.vector()
+        m.steady(p.copy(), s)                 # set-up solve: operators, factorisation, graph
+        ms = []
+        for _ in range(3):
+            m.steady(p.copy(), s)
+            ms.append(m.stats()["device_ms"])
+        st = m.stats()
+        rec = {"ms_per_solve": statistics.median(ms), "refinements": st["refinements"],
+               "fp64_residual_W": st["residual"], "cells": m.n_cells, "flow_ml_min": sc.flow_ml_min}
+        if grid == 128:
+            from oracle.restatement import OracleModel
+            o = OracleModel(sc)
+            t0 = time.perf_counter()
+            T, Tb = o.steady_direct(p)
+            rec["cpu_direct_s"] = time.perf_counter() - t0
+            rec["max_dT_K_vs_fp64_direct"] = float(np.max(np.abs(m.grid("steady") - T)))
+        out[f"{grid}x{grid}"] = rec
+        m.close()
+    return {"workload": "Si 0.1 mm + 0.2 mm water-channel layer (100 um channels, 200 um pitch) + spreader/sink, "
+                        "512x512 over 10.24x10.24 mm", "solves_per_s": 1e3 / out["512x512"]["ms_per_solve"],
+            "sizes": out,
+            "cpu_baseline": {"kind": "port", "what": "FP64 sparse LU (scipy splu) of the restated system, 1 thread",
+                             "sample": "128x128 model", "s_per_solve": out["128x128"]["cpu_direct_s"]}}
+
+
+def leg_serving(args):
+    """The serving mix through hsb_server_run."""
+    from hotspot_b200.serving import Request, Server, latency_report, serving_mix
+    d = tempfile.mkdtemp(prefix="hsb_srv_")
+    srv = Server(workers=8)
+    t0 = time.perf_counter()
+    mix = serving_mix(d, srv, seed=4, rate=2000.0, duration=args.serving_seconds)
+    # every resident model serves one request before the clock starts
+    warm = []
+    for _, mi in mix.classes.items():
+        r0 = next(r for r in mix.requests if r.model == mi)
+        steps = 1 if r0.kind == 0 else 2
+        warm.append(Request(r0.model, r0.kind, r0.power if steps == 1 else r0.power[:2], 0.0, r0.temp_in,
+                            steps, r0.dt, r0.tag))
+    srv.run(warm)
+    setup_s = time.perf_counter() - t0
+    srv.run(mix.requests)
+    span = max(r.finish for r in mix.requests)
+    steady = [r for r in mix.requests if r.kind == 0]
+    trans = [r for r in mix.requests if r.kind == 1]
+    res = {"workload": f"Poisson arrivals at 2000 req/s for {args.serving_seconds} s: 70% steady (sides 64..1024, "
+                       "1..8 chip layers), 30% 500-interval transients (sides 64..256); one resident model per class",
+           "requests": len(mix.requests), "models": len(mix.models), "workers": 8,
+           "throughput_req_per_s": len(mix.requests) / span, "span_s": span,
+           "latency_all": latency_report(mix.requests),
+           "latency_steady": latency_report(steady), "latency_transient": latency_report(trans),
+           "latency_steady_256x256_4layers": latency_report(mix.requests, "steady_256_4"),
+           "service_ms_steady_256x256_4layers": (float(np.median([(r.finish - r.start) * 1e3 for r in mix.requests
+                                                                   if r.tag == "steady_256_4"]))
+                                                  if any(r.tag == "steady_256_4" for r in mix.requests) else None),
+           "setup_s": setup_s}
+    srv.close()
+    for m in mix.models:
+        m.close()
+    return res
+
+
 def run_ours(args):
     import torch
     from hotspot_b200 import FORM_FAST, FORM_PARITY, _abi
@@ -223,7 +375,8 @@ def run_ours(args):
 
     K, Wm = args.steps, max(3, args.warmup)
     work = tempfile.mkdtemp(prefix="hsb_bench_")
-    sc = W.scenario_stack3d(work, seed=100 + rank, grid=args.grid, steps=Wm + K + 1)
+    LOAD = 4000    # trace rows reserved for the clock-sampling load window
+    sc = W.scenario_stack3d(work, seed=100 + rank, grid=args.grid, steps=LOAD + Wm + K + 1)
     m = hm.from_scenario(sc)
     m.set_solver(FORM_FAST)
     ncell = m.n_cells
@@ -234,13 +387,22 @@ def run_ours(args):
     for k in range(1, Wm + 1):
         m.compute_temp(m.power_vector(sc.block_power[k]), None, sc.dt)
 
-    # ---- timed: device time of each interval, L2 flushed in between ----
+    # ---- clocks: nvidia-smi samples every 200 ms over a load window of the
+    # same workload (about 1 s, untimed) and the timed region that follows
     clocks = Clocks(local)
     barrier()
     clocks.start()
+    t_load = time.perf_counter()
+    k0 = Wm + 1
+    while time.perf_counter() - t_load < 1.0 and k0 < Wm + 1 + LOAD:
+        m.compute_temp(m.power_vector(sc.block_power[k0]), None, sc.dt)
+        k0 += 1
+    barrier()
+
+    # ---- timed: device time of each interval, L2 flushed in between ----
     dev_ms = ker_ms = 0.0
     steps_total = launches = 0
-    for k in range(Wm + 1, Wm + K + 1):
+    for k in range(k0, k0 + K):
         flush.fill_(float(k))
         torch.cuda.synchronize()
         m.compute_temp(m.power_vector(sc.block_power[k]), None, sc.dt)
@@ -273,7 +435,7 @@ def run_ours(args):
 
     # ---- e2e: the C-ABI call with host buffers (copies inside), wall clock ----
     L = _abi.lib()
-    powers = [np.ascontiguousarray(m.power_vector(sc.block_power[1 + (k % K)])) for k in range(K)]
+    powers = [np.ascontiguousarray(m.power_vector(sc.block_power[k0 + k])) for k in range(K)]
     h2d = powers[0].nbytes
     d2h = temp.nbytes
     barrier()
@@ -293,7 +455,7 @@ def run_ours(args):
         e2e_value = ncell * e2e_steps / e2e_s
 
     # ---- steady solves: fast MG-PCG ----
-    avg = m.power_vector(sc.block_power[: Wm + K + 1].mean(0))
+    avg = m.power_vector(sc.block_power[: k0 + K].mean(0))
     st_fast = m.vector()
     for _ in range(2):
         m.steady(avg.copy(), st_fast)
@@ -315,10 +477,10 @@ def run_ours(args):
         mp_.set_solver(FORM_PARITY)
         tp = mp_.vector(mp_.config.init_temp)
         mp_.compute_temp(mp_.power_vector(sc.block_power[0]), tp, sc.dt)
-        for k in range(1, Wm + 1):
+        for k in range(1, k0):      # the same rows the fast form ran before its timed region
             mp_.compute_temp(mp_.power_vector(sc.block_power[k]), None, sc.dt)
         pdev, psteps = 0.0, 0
-        for k in range(Wm + 1, Wm + K + 1):
+        for k in range(k0, k0 + K):
             flush.fill_(float(k))
             torch.cuda.synchronize()
             mp_.compute_temp(mp_.power_vector(sc.block_power[k]), None, sc.dt)
@@ -352,7 +514,7 @@ def run_ours(args):
     peak, peak_kind = measured_peak()
     alg_bytes_launch = ALG_BYTES_FP32 * ncell * steps_total / K
     achieved = alg_bytes_launch / ((ker_ms / K) / 1e3) / 1e9
-    traffic = profiled_traffic("rk4_fast_kernel_stack256.md")
+    traffic = profiled_traffic("rk4_krylov_kernel_stack256.md")
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": K,
         "warmup": Wm, "ms_per_step": dev_ms_max / K, "higher_is_better": True, "scaling": "weak",
@@ -365,13 +527,16 @@ def run_ours(args):
                 "d2h_bytes_per_step": d2h},
         "steady_solves_per_s": {"fast": steady_fast, "unit": "solves/s",
                                 "fast_final_fp64_residual_W": steady_fast_residual},
-        "roofline": {"bound": "hbm", "kernel": "rk4_fast_kernel", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "rk4_krylov_kernel", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic,
                      "alg_bytes_per_launch": alg_bytes_launch,
-                     "note": "one launch = one sampling interval; 108 B per cell-step (FP32 stages)"},
+                     "note": "one launch = one sampling interval; 108 B per cell-step (FP32 stages, FP64 "
+                             "state); the 393k-cell state fits the 126 MB L2, so the kernel is latency-bound, "
+                             "not HBM-bound"},
         "gpu_launches": launches,
-        "clocks": clk,
+        "clocks": dict(clk, window="nvidia-smi every 200 ms over ~1 s of this workload just before the timed "
+                                  "region and over the timed region"),
         "rk4_steps_per_interval": steps_total / K,
     }
     line.update(extra)
@@ -381,6 +546,13 @@ def run_ours(args):
         line["cpu_baseline"] = {"value": rate, "unit": "cell-steps/s", "cores": cores, "kind": kind,
                                 "sample": f"2 rows of the same workload x {cores} independent "
                                           "single-threaded replicas"}
+    if ws == 1 and not args.headline_only:
+        for name, fn in (("batched", lambda: leg_batched(args, flush)), ("microchannel", lambda: leg_microchannel(args)),
+                         ("serving", lambda: leg_serving(args))):
+            try:
+                line[name] = fn()
+            except Exception as e:      # a failed leg is reported, the headline still prints
+                line[name] = {"error": f"{type(e).__name__}: {e}"}
     print(json.dumps(line), flush=True)
     m.close()
     if pg:
