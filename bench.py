@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="transient intervals of the fast form only (the case profiled with ncu)")
     ap.add_argument("--headline-only", action="store_true", help="skip the batched / microchannel / serving legs")
+    ap.add_argument("--profile-case", choices=["batch", "microchannel"], default=None,
+                    help="small cases of the other kernels, for ncu captures (a few GB at most)")
     ap.add_argument("--batch-chips", type=int, default=512)
     ap.add_argument("--batch-intervals", type=int, default=10)
     ap.add_argument("--serving-seconds", type=float, default=0.25,
@@ -129,12 +131,12 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(name: str):
-    """DRAM bytes per launch from the committed ncu summary, if present."""
+def profiled_traffic(name: str, key: str = "dram_bytes_per_launch"):
+    """A figure (DRAM bytes per launch, or per cell-step) from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
-            if line.strip().startswith("dram_bytes_per_launch:"):
+            if line.strip().startswith(key + ":"):
                 return float(line.split(":")[1].split()[0])
     except OSError:
         pass
@@ -272,9 +274,10 @@ def leg_batched(args, flush):
             "schedule": tuned, "setup_s": setup_s, "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": "rk4_batch_kernel", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": profiled_traffic("rk4_batch_kernel.md"),
-                         "note": "108 B per cell-step (FP32 stages, FP64 state); traffic per launch of the "
-                                 "profiled small batch"},
+                         "traffic": (lambda b: b * cs / K if b else None)(
+                             profiled_traffic("rk4_batch_kernel.md", "dram_bytes_per_cell_step")),
+                         "note": "108 B per cell-step (FP32 stages, FP64 state); traffic = DRAM bytes per "
+                                 "cell-step of the profiled 16-chip batch x this leg's cell-steps per launch"},
             "l2": "256 MB buffer rewritten between intervals; 265M cells >> L2 anyway"}
 
 
@@ -394,7 +397,7 @@ def run_ours(args):
     clocks.start()
     t_load = time.perf_counter()
     k0 = Wm + 1
-    while time.perf_counter() - t_load < 1.0 and k0 < Wm + 1 + LOAD:
+    while time.perf_counter() - t_load < 1.0 and k0 < Wm + 1 + LOAD and not args.profile:
         m.compute_temp(m.power_vector(sc.block_power[k0]), None, sc.dt)
         k0 += 1
     barrier()
@@ -559,8 +562,53 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
+def profile_case(args):
+    """Small cases of the batched transient and of the BiCGStab solver, sized
+    for ncu (inputs above the L2 size, a few GB on the device at most)."""
+    from hotspot_b200 import FORM_FAST, STEADY_BICGSTAB
+    from hotspot_b200 import model as hm
+    from hotspot_b200 import workloads as W
+    d = tempfile.mkdtemp(prefix="hsb_prof_")
+    if args.profile_case == "batch":
+        from hotspot_b200.batch import Batch
+        rng = np.random.default_rng(7)
+        specs = [(256, 8)] * 6 + [(128, 4)] * 6 + [(64, 2)] * 4
+        scs = [W.scenario_random_chip(d, rng, f"p{i}", side=s, chip_layers=l, steps=8)
+               for i, (s, l) in enumerate(specs)]
+        models = []
+        for sc in scs:
+            m = hm.from_scenario(sc)
+            m.set_solver(FORM_FAST)
+            t = m.vector(m.config.init_temp)
+            m.compute_temp(m.power_vector(sc.block_power[0]), t, 0.0)
+            models.append(m)
+        bt = Batch(models)
+        bt.set_schedule(2, 1.0)
+        out = []
+        for k in range(1, 4):
+            st = bt.transient([m.power_vector(sc.block_power[k]) for sc, m in zip(scs, models)], scs[0].dt)
+            out.append({"kernel_ms": st["kernel_ms"], "rk4_steps": st["rk4_steps"]})
+        print(json.dumps({"profile_case": "batch", "cells": int(sum(m.n_cells for m in models)), "intervals": out}))
+        bt.close()
+    else:
+        sc = W.scenario_microchannel(d, seed=3, grid=128, die=128 * 20e-6, blocks=8)
+        m = hm.from_scenario(sc)
+        m.set_solver(FORM_FAST, STEADY_BICGSTAB)
+        p = m.power_vector(sc.block_power[0])
+        s = m.vector()
+        res = []
+        for _ in range(2):
+            m.steady(p.copy(), s)
+            res.append(m.stats()["device_ms"])
+        print(json.dumps({"profile_case": "microchannel", "cells": m.n_cells, "device_ms": res}))
+        m.close()
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        profile_case(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
