@@ -219,7 +219,7 @@ static void free_model(hsb_dev_model *m) {
   double **bufs[] = {&m->y, &m->ys, &m->pgrid, &m->k1, &m->k2, &m->k3, &m->ytemp, &m->t1, &m->t2,
                      &m->rN, &m->rS, &m->rW, &m->rE, &m->rA, &m->rB, &m->cap, &m->aN, &m->aS,
                      &m->aW, &m->aE, &m->aO, &m->qin, &m->b2g_occ, &m->b2g_area, &m->blk_in,
-                     &m->blk_out, &m->gs_delta};
+                     &m->blk_out, &m->gs_delta, &m->trace_buf};
   for (double **b : bufs)
     if (*b) cudaFree(*b);
   if (m->errbits) cudaFree(m->errbits);
@@ -479,6 +479,57 @@ int hsb_dev_transient(hsb_dev_model *m, const double *block_power, const double 
     st->launches += 1;
     HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb,
                              cudaMemcpyDeviceToHost, m->stream));
+  }
+  cudaEventRecord(e1, m->stream);
+  HSB_CUDA(cudaStreamSynchronize(m->stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  st->device_ms += ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return HSB_OK;
+}
+
+int hsb_dev_transient_trace(hsb_dev_model *m, const double *block_powers, int K, const double *block_temp_in,
+                            double time_elapsed, double *block_temp_out, const hsb_solver_opts *o, hsb_stats *st) {
+  if (!m || !block_powers || K < 1) return set_error(HSB_E_ARG, "null argument or no intervals");
+  if (!m->b2g_ptr) return set_error(HSB_E_ARG, "block-grid maps not set");
+  const int form = o ? o->form : HSB_FORM_PARITY;
+  const size_t nb = (size_t)m->total_n_blocks + m->nx;
+  hsb_stats local;
+  if (!st) st = &local;
+  if (form != HSB_FORM_FAST) {   // the other forms: one interval per call
+    for (int k = 0; k < K; k++) {
+      const int rc = hsb_dev_transient(m, block_powers + k * nb, k == 0 ? block_temp_in : nullptr, time_elapsed,
+                                       k == K - 1 ? block_temp_out : nullptr, o, st);
+      if (rc) return rc;
+    }
+    return HSB_OK;
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, m->stream);
+  int rc;
+  // the block powers of all intervals, in a device buffer kept with the model
+  if (m->trace_cap < (long long)(K * nb)) {
+    if (m->trace_buf) cudaFree(m->trace_buf);
+    m->trace_buf = nullptr;
+    m->trace_cap = 0;
+    HSB_CUDA(cudaMalloc(&m->trace_buf, sizeof(double) * K * nb));
+    m->trace_cap = (long long)K * nb;
+  }
+  HSB_CUDA(cudaMemcpyAsync(m->trace_buf, block_powers, sizeof(double) * K * nb, cudaMemcpyHostToDevice, m->stream));
+  if (block_temp_in) {
+    HSB_CUDA(cudaMemcpyAsync(m->blk_in + nb, block_temp_in, sizeof(double) * nb, cudaMemcpyHostToDevice, m->stream));
+    if ((rc = b2g(m, m->blk_in + nb, m->y, HSB_V_TEMP))) return rc;
+    st->launches += 1;
+  }
+  if ((rc = rk4_fast_trace(m, m->trace_buf, K, time_elapsed, st))) return rc;
+  if (block_temp_out) {
+    if ((rc = g2b(m, m->y, m->blk_out))) return rc;
+    st->launches += 1;
+    HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb, cudaMemcpyDeviceToHost, m->stream));
   }
   cudaEventRecord(e1, m->stream);
   HSB_CUDA(cudaStreamSynchronize(m->stream));

@@ -92,6 +92,8 @@ struct hsb_dev_model {
   double cell_area;
   int *g2b;
   double *blk_in, *blk_out;      // device block vectors (total_n_blocks + nx)
+  double *trace_buf;             // block powers of a multi-interval call (trace_cap doubles)
+  long long trace_cap;
   double *h_blk;                 // pinned staging (2 * (total_n_blocks + nx))
 
   // multigrid levels for the exact nested-iteration replay
@@ -135,6 +137,8 @@ int gs_exact_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
 // fast-form solvers
 int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
 int rk4_fast_stages_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
+// K consecutive intervals of the fast form from K block-power vectors in device memory
+int rk4_fast_trace(hsb_dev_model *m, const double *bpow_dev, int K, double time_elapsed, hsb_stats *st);
 
 // the fast transient kernel on caller-provided state, power and scratch
 struct FastBuffers {

@@ -319,5 +319,10 @@ int rk4_stage_run(hsb_dev_model *m, FastWork *w, double T, double h0, hsb_stats 
 int rk4_krylov_run(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next);
 // the Krylov vectors and their tensor maps (allocated once per model)
 int kry_prepare(hsb_dev_model *m, FastWork *w);
+// K intervals in one launch from K device block-power vectors; *done = the
+// intervals completed (< K: the rejection budget ran out in interval *done at
+// *t_done, continue with step size *h_next)
+int rk4_krylov_trace(hsb_dev_model *m, FastWork *w, const double *bpow, int K, double T, hsb_stats *st, int *done,
+                     double *t_done, double *h_next);
 
 }  // namespace hsb

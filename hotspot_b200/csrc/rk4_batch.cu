@@ -177,14 +177,20 @@ __device__ __forceinline__ void bissue(const BChip &C, unsigned char *buf, BShar
   }
 }
 
+// one warp polls the tile copy's mbarrier; the others wait at the CTA
+// barrier, issuing nothing (the barrier also makes the copied tile visible
+// to them)
 __device__ __forceinline__ void bwait(BShared &sh, BCtl &c, int b) {
-  int it = 0;
-  while (!mbar_try_wait(&sh.bar[b], (c.phase >> b) & 1u)) {
-    if (++it >= WAIT_LIMIT) {
-      sh.lost = 1;
-      break;
+  if (threadIdx.x < 32) {
+    int it = 0;
+    while (!mbar_try_wait(&sh.bar[b], (c.phase >> b) & 1u)) {
+      if (++it >= WAIT_LIMIT) {
+        sh.lost = 1;
+        break;
+      }
     }
   }
+  __syncthreads();
   c.phase ^= 1u << b;
 }
 

@@ -757,6 +757,35 @@ int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
   return HSB_OK;
 }
 
+// K intervals in as few launches as possible: one Krylov-form launch runs
+// them back to back; an interval whose rejection budget runs out is finished
+// by the stage form (from its own grid power) and the launches resume after it
+int rk4_fast_trace(hsb_dev_model *m, const double *bpow_dev, int K, double time_elapsed, hsb_stats *st) {
+  FastWork *w;
+  int rc;
+  if ((rc = fast_prepare(m, &w))) return rc;
+  const long long nb = (long long)m->total_n_blocks + m->nx;
+  int i0 = 0;
+  while (i0 < K) {
+    int done = 0;
+    double t_done = time_elapsed, h_next = 0.0;
+    if ((rc = rk4_krylov_trace(m, w, bpow_dev + i0 * nb, K - i0, time_elapsed, st, &done, &t_done, &h_next)))
+      return rc;
+    if (done >= K - i0) break;
+    const int k = i0 + done;
+    if ((rc = b2g(m, bpow_dev + (long long)k * nb, m->pgrid, HSB_V_POWER))) return rc;
+    st->launches += 1;
+    st->fallbacks += 1;
+    if ((rc = rk4_stage_run(m, w, time_elapsed - t_done, h_next, st))) return rc;
+    i0 = k + 1;
+  }
+  // later single-interval calls find the last interval's grid power in place
+  if ((rc = b2g(m, bpow_dev + (long long)(K - 1) * nb, m->pgrid, HSB_V_POWER))) return rc;
+  st->launches += 1;
+  st->sim_time += time_elapsed * K;
+  return HSB_OK;
+}
+
 // ---------------------------------------------------------------------------
 // The same kernel on buffers the caller provides (state, power, and every
 // scratch array), for the allocation-free entry point.  Nothing here

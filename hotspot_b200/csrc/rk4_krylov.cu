@@ -61,6 +61,15 @@ struct KryArgs {
   double *tout;                    // [0] time reached [1] next step size
   double T;
   long long max_attempts;
+  // trace mode (K > 0): K intervals in one launch, the power of interval k
+  // from block powers bpow + k*nbv mapped to the grid in the kernel (the
+  // arithmetic of xlate_vector_b2g, temperature_grid.c:1888-1929)
+  int K;
+  long long nbv;
+  const double *bpow;
+  const int *b2g_ptr, *b2g_blk;
+  const double *b2g_occ, *b2g_area;
+  double cell_area;
 };
 
 enum { K_FULL = 0, K_KRY = 1 };
@@ -153,14 +162,20 @@ __device__ __forceinline__ void kfinish(const KryArgs &A, KCtl &c, KShared &sh) 
   c.pkind = -1;
 }
 
+// one warp polls the tile copy's mbarrier; the others wait at the CTA
+// barrier, issuing nothing (the barrier also makes the copied tile visible
+// to them)
 __device__ __forceinline__ void kwait(KShared &sh, KCtl &c) {
-  int it = 0;
-  while (!mbar_try_wait(&sh.bar, c.phase & 1u)) {
-    if (++it >= WAIT_LIMIT) {
-      sh.lost = 1;
-      break;
+  if (threadIdx.x < 32) {
+    int it = 0;
+    while (!mbar_try_wait(&sh.bar, c.phase & 1u)) {
+      if (++it >= WAIT_LIMIT) {
+        sh.lost = 1;
+        break;
+      }
     }
   }
+  __syncthreads();
   c.phase++;
 }
 
@@ -412,6 +427,23 @@ __device__ __forceinline__ double kerr_finish(const KryArgs &A, KCtl &c, KShared
   return mx;
 }
 
+// FP32 grid power of interval iv: from A.pgrid (single interval), or mapped
+// from the interval's block powers exactly as b2g_kernel does in FP64
+__device__ __forceinline__ void kpower(const KryArgs &A, int iv) {
+  const long long n = A.S.ncell, stride = (long long)gridDim.x * blockDim.x;
+  if (A.K == 0) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride)
+      A.pf[q] = (float)A.pgrid[q];
+    return;
+  }
+  const double *b = A.bpow + (long long)iv * A.nbv;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+    double val = 0.0;
+    for (int e = A.b2g_ptr[q]; e < A.b2g_ptr[q + 1]; e++) val += A.b2g_occ[e] * b[A.b2g_blk[e]] / A.b2g_area[e];
+    A.pf[q] = (float)(val * A.cell_area);
+  }
+}
+
 template <bool FIELD, bool ADV>
 __global__ void __launch_bounds__(FT_THREADS, 2) rk4_krylov_kernel(const __grid_constant__ KryArgs A) {
   cg::grid_group grid = cg::this_grid();
@@ -437,9 +469,7 @@ __global__ void __launch_bounds__(FT_THREADS, 2) rk4_krylov_kernel(const __grid_
     mbar_init(&sh.bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < S.ncell;
-       q += (long long)gridDim.x * blockDim.x)
-    A.pf[q] = (float)A.pgrid[q];
+  kpower(A, 0);
   if (threadIdx.x < nx) sh.yp[threadIdx.x] = A.y[S.ncell + threadIdx.x];
   if (blockIdx.x == 0 && threadIdx.x == 0) { A.err[0] = 0ull; A.err[1] = 0ull; }
   grid.sync();
@@ -463,71 +493,83 @@ __global__ void __launch_bounds__(FT_THREADS, 2) rk4_krylov_kernel(const __grid_
   int status = 0;
   double t = 0.0, h = 0.0, new_h = 1e-7;
   double *yb = A.y, *yn = A.y2;
-  while (t < A.T && new_h >= 1e-7 * 1.0e-6) {
-    h = new_h;
-    const CUtensorMap *myb = yb == A.y ? &A.m_y : &A.m_y2;
-    kpass<FIELD, ADV, true, false>(A, grid, c, sh, ds, 0, 1.0, myb);   // N_0 = f(y)
-    int dcomp = 0;
-    if (threadIdx.x == 0) c_one(sh.K);
-    double mx = 0.0;
-    bool first = true;
-    for (;;) {
+  const int nint = A.K > 0 ? A.K : 1;
+  int iv = 0;
+  for (iv = 0; iv < nint; iv++) {
+    if (iv > 0) {
+      // the next interval: its power, and h restarts as in compute_temp_grid
+      kpower(A, iv);
+      grid.sync();
+      t = 0.0;
+      new_h = 1e-7;
+    }
+    while (t < A.T && new_h >= 1e-7 * 1.0e-6) {
       h = new_h;
-      if (first) {
-        // k1 = F and every vector made with scale h: the h = 1 coefficients scaled
-        if (threadIdx.x < PMAX) {
-          const int q = threadIdx.x;
-          sh.ps[q] = h;
-          if (q < sh.E1.n) sh.E.c[q] = h * sh.E1.c[q];
-          if (q < sh.D1.n) sh.D.c[q] = h * sh.D1.c[q];
-          if (q < sh.F11.n) sh.F1.c[q] = sh.F11.c[q];
-          if (q == 0) {
-            sh.E.n = sh.E1.n;
-            sh.D.n = sh.D1.n;
-            sh.F1.n = sh.F11.n;
+      const CUtensorMap *myb = yb == A.y ? &A.m_y : &A.m_y2;
+      kpass<FIELD, ADV, true, false>(A, grid, c, sh, ds, 0, 1.0, myb);   // N_0 = f(y)
+      int dcomp = 0;
+      if (threadIdx.x == 0) c_one(sh.K);
+      double mx = 0.0;
+      bool first = true;
+      for (;;) {
+        h = new_h;
+        if (first) {
+          // k1 = F and every vector made with scale h: the h = 1 coefficients scaled
+          if (threadIdx.x < PMAX) {
+            const int q = threadIdx.x;
+            sh.ps[q] = h;
+            if (q < sh.E1.n) sh.E.c[q] = h * sh.E1.c[q];
+            if (q < sh.D1.n) sh.D.c[q] = h * sh.D1.c[q];
+            if (q < sh.F11.n) sh.F1.c[q] = sh.F11.c[q];
+            if (q == 0) {
+              sh.E.n = sh.E1.n;
+              sh.D.n = sh.D1.n;
+              sh.F1.n = sh.F11.n;
+            }
           }
+          first = false;
+        } else if (threadIdx.x == 0) {
+          plan_attempt(sh, h, dcomp);
         }
-        first = false;
-      } else if (threadIdx.x == 0) {
-        plan_attempt(sh, h, dcomp);
+        __syncthreads();
+        const int dE = sh.E.n - 1;
+        if (dE > KRY_DMAX || dE <= dcomp) {
+          status = 3;
+          break;
+        }
+        for (int q = dcomp + 1; q < dE; q++) kpass<FIELD, ADV, false, false>(A, grid, c, sh, ds, q, sh.ps[q]);
+        kpass<FIELD, ADV, false, true>(A, grid, c, sh, ds, dE, sh.ps[dE], yb == A.y ? &A.m_yi : &A.m_y2i, yb, yn);
+        dcomp = dE;
+        mx = kerr_finish(A, c, sh);
+        attempts++;
+        if (mx <= 0.01) {
+          new_h = 0.95 * h * pow(fabs(0.01 / mx), 0.2);
+          if (new_h > 5.0 * h) new_h = 5.0 * h;
+        } else {
+          new_h = 0.95 * h * pow(fabs(0.01 / mx), 0.25);
+          if (new_h < h / 10.0) new_h = h / 10.0;
+        }
+        if (attempts >= A.max_attempts) break;
+        if (new_h >= h) break;
+        // rejected: the retry's k1 is f(t1) of this attempt
+        if (threadIdx.x == 0) c_copy(sh.K, sh.F1);
+        __syncthreads();
       }
-      __syncthreads();
-      const int dE = sh.E.n - 1;
-      if (dE > KRY_DMAX || dE <= dcomp) {
-        status = 3;
-        break;
+      if (status || attempts >= A.max_attempts) break;
+      // accepted: the candidate buffer becomes the state
+      if (threadIdx.x < nx) {
+        double dy = 0.0;
+        for (int q = 0; q < sh.D.n; q++) dy += sh.D.c[q] * sh.Np[q][threadIdx.x];
+        sh.yp[threadIdx.x] += dy;
       }
-      for (int q = dcomp + 1; q < dE; q++) kpass<FIELD, ADV, false, false>(A, grid, c, sh, ds, q, sh.ps[q]);
-      kpass<FIELD, ADV, false, true>(A, grid, c, sh, ds, dE, sh.ps[dE], yb == A.y ? &A.m_yi : &A.m_y2i, yb, yn);
-      dcomp = dE;
-      mx = kerr_finish(A, c, sh);
-      attempts++;
-      if (mx <= 0.01) {
-        new_h = 0.95 * h * pow(fabs(0.01 / mx), 0.2);
-        if (new_h > 5.0 * h) new_h = 5.0 * h;
-      } else {
-        new_h = 0.95 * h * pow(fabs(0.01 / mx), 0.25);
-        if (new_h < h / 10.0) new_h = h / 10.0;
-      }
-      if (attempts >= A.max_attempts) break;
-      if (new_h >= h) break;
-      // rejected: the retry's k1 is f(t1) of this attempt
-      if (threadIdx.x == 0) c_copy(sh.K, sh.F1);
-      __syncthreads();
+      double *tmp = yb;
+      yb = yn;
+      yn = tmp;
+      steps++;
+      new_h = new_h < A.T - t - h ? new_h : A.T - t - h;
+      t += h;
     }
-    if (status || attempts >= A.max_attempts) break;
-    // accepted: the candidate buffer becomes the state
-    if (threadIdx.x < nx) {
-      double dy = 0.0;
-      for (int q = 0; q < sh.D.n; q++) dy += sh.D.c[q] * sh.Np[q][threadIdx.x];
-      sh.yp[threadIdx.x] += dy;
-    }
-    double *tmp = yb;
-    yb = yn;
-    yn = tmp;
-    steps++;
-    new_h = new_h < A.T - t - h ? new_h : A.T - t - h;
-    t += h;
+    if (status || attempts >= A.max_attempts || sh.lost) break;
   }
   __syncthreads();
   if (sh.lost && threadIdx.x == 0) {
@@ -547,6 +589,7 @@ __global__ void __launch_bounds__(FT_THREADS, 2) rk4_krylov_kernel(const __grid_
       A.cnt[3] = c.passes;
       A.tout[0] = t;
       A.tout[1] = new_h;
+      A.cnt[7] = iv;   // intervals completed
     }
   }
 }
@@ -583,7 +626,21 @@ int kry_prepare(hsb_dev_model *m, FastWork *w) {
   return HSB_OK;
 }
 
+static int krylov_launch(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next,
+                         const double *bpow, int K, int *done);
+
 int rk4_krylov_run(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next) {
+  int done = 0;
+  return krylov_launch(m, w, T, st, t_done, h_next, nullptr, 0, &done);
+}
+
+int rk4_krylov_trace(hsb_dev_model *m, FastWork *w, const double *bpow, int K, double T, hsb_stats *st, int *done,
+                     double *t_done, double *h_next) {
+  return krylov_launch(m, w, T, st, t_done, h_next, bpow, K, done);
+}
+
+static int krylov_launch(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next,
+                         const double *bpow, int K, int *done) {
   int rc;
   if ((rc = kry_prepare(m, w))) return rc;
   KryArgs A;
@@ -616,6 +673,14 @@ int rk4_krylov_run(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, doubl
   A.tout = (double *)(w->cnt + 4);
   A.T = T;
   A.max_attempts = 10000000;
+  A.K = K;
+  A.bpow = bpow;
+  A.nbv = (long long)m->total_n_blocks + m->nx;
+  A.b2g_ptr = m->b2g_ptr;
+  A.b2g_blk = m->b2g_blk;
+  A.b2g_occ = m->b2g_occ;
+  A.b2g_area = m->b2g_area;
+  A.cell_area = m->cell_area;
   const void *fn = kry_kernel_for(m->field, m->uchan_mask != 0);
   int grid = 0;
   if ((rc = coop_grid(m, fn, kry_smem(m->nl), &grid))) return rc;
@@ -649,6 +714,7 @@ int rk4_krylov_run(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, doubl
   memcpy(tout, w->h_cnt + 4, sizeof(tout));
   *t_done = T;
   *h_next = 0.0;
+  *done = (int)w->h_cnt[7];
   if (w->h_cnt[2] == 1) return set_error(HSB_E_NOCONV, "fast transient: RK4 attempt cap reached");
   if (w->h_cnt[2] == 2) return set_error(HSB_E_CUDA, "fast transient: a tile copy did not complete in time");
   if (w->h_cnt[2] == 3) {

@@ -80,12 +80,9 @@ static int run_request(hsb_server::Model &M, hsb_request *r) {
   if (cudaSetDevice(m->device) != cudaSuccess) return set_error(HSB_E_CUDA, "cudaSetDevice");
   if (r->kind == HSB_REQ_STEADY) return hsb_dev_steady(m, r->power, r->out, &M.opts, &st);
   if (r->kind != HSB_REQ_TRANSIENT || r->steps < 1) return set_error(HSB_E_ARG, "bad request kind or step count");
-  for (int k = 0; k < r->steps; k++) {
-    const int rc = hsb_dev_transient(m, r->power + (size_t)k * nb, k == 0 ? r->temp_in : nullptr, r->dt,
-                                     k == r->steps - 1 ? r->out : nullptr, &M.opts, &st);
-    if (rc) return rc;
-  }
-  return HSB_OK;
+  (void)nb;
+  // all intervals of the request in one call (one persistent launch in the fast form)
+  return hsb_dev_transient_trace(m, r->power, r->steps, r->temp_in, r->dt, r->out, &M.opts, &st);
 }
 
 int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {

@@ -224,6 +224,21 @@ class RCModel:
     def steady(self, power: np.ndarray, temp: np.ndarray):
         check(lib().hsb_grid_steady(self.ptr, dptr(power), dptr(temp)))
 
+    def compute_trace(self, powers: np.ndarray, temp_in: np.ndarray | None, dt: float,
+                      form: int = _abi.FORM_FAST) -> tuple[np.ndarray, dict]:
+        """K consecutive intervals (rows of ``powers``) in one call; returns the
+        block temperatures after the last interval and the call's statistics."""
+        p = np.ascontiguousarray(powers, dtype=np.float64)
+        out = self.vector()
+        opts = _abi.SolverOpts(form, _abi.STEADY_AUTO, 0.0, 0)
+        st = _abi.Stats()
+        rc = lib().hsb_dev_transient_trace(lib().hsb_grid_device(self.ptr), dptr(p), int(p.shape[0]),
+                                           dptr(temp_in) if temp_in is not None else None, dt, dptr(out),
+                                           C.byref(opts), C.byref(st))
+        if rc != 0:
+            raise _abi.HotspotError(lib().hsb_dev_last_error().decode(errors="replace").strip())
+        return out, st.as_dict()
+
     def close(self):
         if self.ptr:
             lib().delete_grid_model(self.ptr)

@@ -124,6 +124,17 @@ int hsb_dev_transient(hsb_dev_model *m, const double *block_power,
 int hsb_dev_steady(hsb_dev_model *m, const double *block_power,
                    double *block_temp_out, const hsb_solver_opts *o,
                    hsb_stats *st);
+/* K consecutive sampling intervals (compute_temp_grid called K times,
+ * temperature_grid.c:3603-3704) in one call: block_powers holds K block
+ * power vectors (total_n_blocks + n_extra each, host), block_temp_in seeds
+ * the state (or NULL), block_temp_out receives the block temperatures after
+ * the last interval (or NULL).  With HSB_FORM_FAST the intervals run back
+ * to back in one persistent launch, no host round trip between them; the
+ * results equal K single-interval calls. */
+int hsb_dev_transient_trace(hsb_dev_model *m, const double *block_powers, int K,
+                            const double *block_temp_in, double time_elapsed,
+                            double *block_temp_out, const hsb_solver_opts *o,
+                            hsb_stats *st);
 
 /* No counterpart in the reference.  For callers that may not allocate
  * device memory while they run (a simulator that reserves its GPU memory at

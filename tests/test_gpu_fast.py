@@ -155,3 +155,28 @@ def test_bicgstab_symmetric_model(workdir):
     err = float(np.max(np.abs(m.grid("steady") - T)))
     m.close()
     assert np.max(np.abs(s - Tb)) <= TOL and err <= TOL, err
+
+
+@pytest.mark.parametrize("builder", ["chip2d", "stack3d", "detailed"])
+def test_trace_equals_single_intervals(workdir, builder):
+    """K intervals in one persistent launch (hsb_dev_transient_trace) give the
+    results of K single-interval calls of the fast form, bit for bit."""
+    if builder == "chip2d":
+        sc = W.scenario_chip2d(workdir, seed=51, grid=64, steps=12)
+    else:
+        sc = W.scenario_stack3d(workdir, seed=52, grid=64, steps=12, n_blocks=12)
+        sc.detailed_3D = builder == "detailed"
+    a, b = hm.from_scenario(sc), hm.from_scenario(sc)
+    a.set_solver(FORM_FAST)
+    t = a.vector(a.config.init_temp)
+    powers = np.stack([a.power_vector(sc.block_power[k]) for k in range(sc.steps)])
+    steps_a = 0
+    for k in range(sc.steps):
+        a.compute_temp(powers[k].copy(), t if k == 0 else None, sc.dt)
+        steps_a += a.stats()["rk4_steps"]
+    out, st = b.compute_trace(powers, b.vector(b.config.init_temp), sc.dt)
+    assert st["rk4_steps"] == steps_a
+    assert np.array_equal(out, t)
+    assert np.array_equal(a.grid("trans"), b.grid("trans"))
+    a.close()
+    b.close()
