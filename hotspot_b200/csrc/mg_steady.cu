@@ -19,6 +19,7 @@
 // 12 package nodes given the grid.  Pre-smoothing runs red, black, package;
 // post-smoothing package, black, red, so the preconditioner is symmetric.
 // Restriction sums the 2x2 children, prolongation injects (its transpose).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -74,6 +75,10 @@ struct MgWork {
   cudaGraphExec_t pass_exec;
   const double *pass_T;
   int pass_version;
+  // exact solve of the coarsest level: its dense FP64 inverse (cn x cn), or
+  // none when the level is too large (then smoothing sweeps stand in)
+  double *cinv;
+  int cn;
 };
 
 // ---------------------------------------------------------------------------
@@ -277,6 +282,24 @@ __global__ void __launch_bounds__(1024) mg_coarse_solve(MgLevelDev L, const Pack
     pk();
     zl(1);
     zl(0);
+  }
+}
+
+// exact solve of the coarsest level, x = A^-1 f, with its dense FP64 inverse
+// (one CTA; the level has at most MG_COARSE_MAX unknowns)
+#define MG_COARSE_MAX 2048
+__global__ void __launch_bounds__(1024) mg_coarse_direct(const double *__restrict__ inv, int n,
+                                                         float *__restrict__ x, const float *__restrict__ f) {
+  __shared__ double fs[MG_COARSE_MAX];
+  for (int k = threadIdx.x; k < n; k += blockDim.x) fs[k] = (double)f[k];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r = w; r < n; r += nw) {   // one warp per row, coalesced along the row
+    double s = 0.0;
+    const double *row = inv + (long long)r * n;
+    for (int c = lane; c < n; c += 32) s += row[c] * fs[c];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) x[r] = (float)s;
   }
 }
 
@@ -681,7 +704,7 @@ static void free_mg(void *p) {
       if (q) cudaFree(q);
   }
   void *b2[] = {w->gE64, w->gS64, w->gB64, w->gAmb64, w->gEdgeNS64, w->gEdgeEW64, w->r64, w->b64,
-                w->p, w->q, w->z, w->e, w->rr, w->red, w->d_ps};
+                w->p, w->q, w->z, w->e, w->rr, w->red, w->d_ps, w->cinv};
   for (void *q : b2)
     if (q) cudaFree(q);
   if (w->h_red) cudaFreeHost(w->h_red);
@@ -810,6 +833,100 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
     mg_diag<<<nb(L.ncell), MGT, 0, m->stream>>>(dev_level(m, L, l), L.diag);
   }
   HSB_CUDA(cudaGetLastError());
+  // the coarsest level exactly: the smoother cannot resolve the near-null
+  // mode of the system (the overall temperature level, tied to ambient only
+  // through the weak convection), so its operator is assembled on the host,
+  // as mg_apply_cells / mg_apply_pack apply it, and inverted once
+  {
+    const int lc = w->nlev - 1;
+    const MgLevel &C = w->lv[lc];
+    const long long n = C.ncell + NXP;
+    if (w->cinv) {
+      cudaFree(w->cinv);
+      w->cinv = nullptr;
+    }
+    w->cn = 0;
+    if (n <= MG_COARSE_MAX) {
+      std::vector<float> gE(C.ncell), gS(C.ncell), gB(C.ncell), dg(C.ncell);
+      HSB_CUDA(cudaMemcpyAsync(gE.data(), C.gE, sizeof(float) * C.ncell, cudaMemcpyDeviceToHost, m->stream));
+      HSB_CUDA(cudaMemcpyAsync(gS.data(), C.gS, sizeof(float) * C.ncell, cudaMemcpyDeviceToHost, m->stream));
+      HSB_CUDA(cudaMemcpyAsync(gB.data(), C.gB, sizeof(float) * C.ncell, cudaMemcpyDeviceToHost, m->stream));
+      HSB_CUDA(cudaMemcpyAsync(dg.data(), C.diag, sizeof(float) * C.ncell, cudaMemcpyDeviceToHost, m->stream));
+      HSB_CUDA(cudaStreamSynchronize(m->stream));
+      const double scale = (double)(1ll << lc);
+      std::vector<double> A((size_t)n * 2 * n, 0.0);   // [A | I], Gauss-Jordan in place
+      auto at = [&](long long r, long long c) -> double & { return A[(size_t)r * 2 * n + c]; };
+      const long long N = C.ncell, pl = C.plane;
+      auto node_of = [&](int layer, int side) -> int {
+        if (layer == m->hsidx) return side == 0 ? HSB_SINK_C_N : side == 1 ? HSB_SINK_C_S : side == 2 ? HSB_SINK_C_W : HSB_SINK_C_E;
+        if (layer == m->spidx) return side == 0 ? HSB_SP_N : side == 1 ? HSB_SP_S : side == 2 ? HSB_SP_W : HSB_SP_E;
+        return -1;
+      };
+      for (long long c = 0; c < N; c++) {
+        const int ln = (int)(c / pl);
+        const long long q = c - ln * pl;
+        const int i = (int)(q / C.nc), j = (int)(q - (long long)i * C.nc);
+        at(c, c) = dg[c];
+        if (j < C.nc - 1) at(c, c + 1) -= gE[c];
+        if (j > 0) at(c, c - 1) -= gE[c - 1];
+        if (i < C.nr - 1) at(c, c + C.nc) -= gS[c];
+        if (i > 0) at(c, c - C.nc) -= gS[c - C.nc];
+        if (ln < nl - 1) at(c, c + pl) -= gB[c];
+        if (ln > 0) at(c, c - pl) -= gB[c - pl];
+        if (ln == m->spidx || ln == m->hsidx) {
+          const float gn = (float)(gens[ln] * scale), gw = (float)(geew[ln] * scale);
+          if (i == 0) at(c, N + node_of(ln, 0)) -= gn;
+          if (i == C.nr - 1) at(c, N + node_of(ln, 1)) -= gn;
+          if (j == 0) at(c, N + node_of(ln, 2)) -= gw;
+          if (j == C.nc - 1) at(c, N + node_of(ln, 3)) -= gw;
+        }
+      }
+      for (int k = 0; k < NXP; k++) {
+        const int cnt = ps.elayer[k] < 0 ? 0 : (ps.eside[k] < 2 ? C.nc : C.nr);
+        const float ge = ps.ge0[k] * (float)scale;
+        float D = cnt * ge + ps.gamb[k];
+        for (int o = 0; o < NXP; o++) D += ps.link[k][o];
+        at(N + k, N + k) += D;
+        for (int o = 0; o < NXP; o++) at(N + k, N + o) -= ps.link[k][o];
+        if (ps.elayer[k] >= 0) {
+          const int layer = ps.elayer[k], side = ps.eside[k];
+          const int len = side < 2 ? C.nc : C.nr;
+          const long long base = (long long)layer * pl +
+                                 (side == 0 ? 0 : side == 1 ? (long long)(C.nr - 1) * C.nc : side == 2 ? 0 : C.nc - 1);
+          const long long stp = side < 2 ? 1 : C.nc;
+          for (int qq = 0; qq < len; qq++) at(N + k, base + qq * stp) -= ge;
+        }
+      }
+      for (long long r = 0; r < n; r++) at(r, n + r) = 1.0;
+      bool ok = true;
+      for (long long c = 0; c < n && ok; c++) {
+        long long piv = c;
+        for (long long r = c + 1; r < n; r++)
+          if (fabs(at(r, c)) > fabs(at(piv, c))) piv = r;
+        if (at(piv, c) == 0.0) {
+          ok = false;
+          break;
+        }
+        if (piv != c)
+          for (long long q2 = 0; q2 < 2 * n; q2++) std::swap(at(c, q2), at(piv, q2));
+        const double inv = 1.0 / at(c, c);
+        for (long long q2 = 0; q2 < 2 * n; q2++) at(c, q2) *= inv;
+        for (long long r = 0; r < n; r++)
+          if (r != c && at(r, c) != 0.0) {
+            const double fct = at(r, c);
+            for (long long q2 = c; q2 < 2 * n; q2++) at(r, q2) -= fct * at(c, q2);
+          }
+      }
+      if (ok) {
+        std::vector<double> inv((size_t)n * n);
+        for (long long r = 0; r < n; r++)
+          for (long long c = 0; c < n; c++) inv[(size_t)r * n + c] = at(r, n + c);
+        HSB_CUDA(cudaMalloc(&w->cinv, sizeof(double) * n * n));
+        HSB_CUDA(cudaMemcpy(w->cinv, inv.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice));
+        w->cn = (int)n;
+      }
+    }
+  }
   return HSB_OK;
 }
 
@@ -834,7 +951,8 @@ static void vcycle(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f)
   const MgLevel &L = w->lv[l];
   mg_zero<<<nb(L.n), MGT, 0, m->stream>>>(x, L.n);
   if (l == w->nlev - 1) {
-    mg_coarse_solve<<<1, 1024, 0, m->stream>>>(dev_level(m, L, l), w->d_ps, x, f, 8);
+    if (w->cn > 0) mg_coarse_direct<<<1, 1024, 0, m->stream>>>(w->cinv, w->cn, x, f);
+    else mg_coarse_solve<<<1, 1024, 0, m->stream>>>(dev_level(m, L, l), w->d_ps, x, f, 8);
     return;
   }
   const MgLevelDev d = dev_level(m, L, l);
