@@ -91,7 +91,11 @@ __device__ __forceinline__ int edge_node(int layer, int side, int spidx, int hsi
   return -1;
 }
 
-// y = A x on level L (cells only; package rows handled by pack_apply)
+// y = A x on level L (cells only; package rows handled by mg_apply_pack),
+// written in difference form, gAmb x + sum g (x - x_nbr): the system is
+// nearly singular (the overall temperature level is tied to ambient only
+// through weak convection), and diag*x - sum g*x_nbr would cancel most FP32
+// digits of smooth vectors
 __global__ void mg_apply_cells(MgLevelDev L, const float *__restrict__ x, float *__restrict__ y,
                                const float *__restrict__ f, int mode) {
   // mode 0: y = A x ; mode 1: y = f - A x
@@ -100,28 +104,31 @@ __global__ void mg_apply_cells(MgLevelDev L, const float *__restrict__ x, float 
   const int n = (int)(c / L.plane);
   const long long r = c - n * L.plane;
   const int i = (int)(r / L.nc), j = (int)(r - (long long)i * L.nc);
-  float s = L.diag[c] * x[c];
-  if (j < L.nc - 1) s -= L.gE[c] * x[c + 1];
-  if (j > 0) s -= L.gE[c - 1] * x[c - 1];
-  if (i < L.nr - 1) s -= L.gS[c] * x[c + L.nc];
-  if (i > 0) s -= L.gS[c - L.nc] * x[c - L.nc];
-  if (n < L.nl - 1) s -= L.gB[c] * x[c + L.plane];
-  if (n > 0) s -= L.gB[c - L.plane] * x[c - L.plane];
+  const float xc = x[c];
+  float s = L.gAmbL[n] * xc;
+  if (j < L.nc - 1) s += L.gE[c] * (xc - x[c + 1]);
+  if (j > 0) s += L.gE[c - 1] * (xc - x[c - 1]);
+  if (i < L.nr - 1) s += L.gS[c] * (xc - x[c + L.nc]);
+  if (i > 0) s += L.gS[c - L.nc] * (xc - x[c - L.nc]);
+  if (n < L.nl - 1) s += L.gB[c] * (xc - x[c + L.plane]);
+  if (n > 0) s += L.gB[c - L.plane] * (xc - x[c - L.plane]);
   const float *xp = x + L.ncell;
   if (n == L.spidx || n == L.hsidx) {
-    if (i == 0) s -= L.gEdgeNS[n] * xp[edge_node(n, 0, L.spidx, L.hsidx)];
-    if (i == L.nr - 1) s -= L.gEdgeNS[n] * xp[edge_node(n, 1, L.spidx, L.hsidx)];
-    if (j == 0) s -= L.gEdgeEW[n] * xp[edge_node(n, 2, L.spidx, L.hsidx)];
-    if (j == L.nc - 1) s -= L.gEdgeEW[n] * xp[edge_node(n, 3, L.spidx, L.hsidx)];
+    if (i == 0) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 0, L.spidx, L.hsidx)]);
+    if (i == L.nr - 1) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 1, L.spidx, L.hsidx)]);
+    if (j == 0) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 2, L.spidx, L.hsidx)]);
+    if (j == L.nc - 1) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 3, L.spidx, L.hsidx)]);
   }
   y[c] = mode ? f[c] - s : s;
 }
 
-// package rows: one CTA; sums of the attached edges by warps
+// package rows (one CTA), difference form: ge sum_edge (x_k - x_c) +
+// gamb x_k + sum link (x_k - x_o)
 __global__ void mg_apply_pack(MgLevelDev L, const PackSys *__restrict__ ps, const float *__restrict__ x,
                               float *__restrict__ y, const float *__restrict__ f, int mode) {
   __shared__ float esum[NXP];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const float *xp = x + L.ncell;
   for (int k = w; k < NXP; k += blockDim.x >> 5) {
     float s = 0.f;
     const int layer = ps->elayer[k], side = ps->eside[k];
@@ -130,7 +137,8 @@ __global__ void mg_apply_pack(MgLevelDev L, const PackSys *__restrict__ ps, cons
       const long long base = (long long)layer * L.plane +
                              (side == 0 ? 0 : side == 1 ? (long long)(L.nr - 1) * L.nc : side == 2 ? 0 : L.nc - 1);
       const long long st = side < 2 ? 1 : L.nc;
-      for (int q = lane; q < len; q += 32) s += x[base + q * st];
+      const float xk = xp[k];
+      for (int q = lane; q < len; q += 32) s += xk - x[base + q * st];
       for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     }
     if (lane == 0) esum[k] = s;
@@ -138,13 +146,9 @@ __global__ void mg_apply_pack(MgLevelDev L, const PackSys *__restrict__ ps, cons
   __syncthreads();
   if (threadIdx.x < NXP) {
     const int k = threadIdx.x;
-    const float *xp = x + L.ncell;
-    const int cnt = ps->elayer[k] < 0 ? 0 : (ps->eside[k] < 2 ? L.nc : L.nr);
     const float ge = ps->ge0[k] * L.scale;
-    float D = cnt * ge + ps->gamb[k];
-    for (int o = 0; o < NXP; o++) D += ps->link[k][o];
-    float s = D * xp[k] - ge * esum[k];
-    for (int o = 0; o < NXP; o++) s -= ps->link[k][o] * xp[o];
+    float s = ge * esum[k] + ps->gamb[k] * xp[k];
+    for (int o = 0; o < NXP; o++) s += ps->link[k][o] * (xp[k] - xp[o]);
     y[L.ncell + k] = mode ? f[L.ncell + k] - s : s;
   }
 }

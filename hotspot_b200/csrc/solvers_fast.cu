@@ -50,6 +50,7 @@ struct BcLevelDev {
   int nl, nr, nc;
   long long plane, ncell;
   const float *cN, *cS, *cW, *cE, *cA, *cB, *dg;   // A[c, neighbour] and A[c, c]
+  const float *rs;                                 // row sums without the package edges
   const float *LF, *UB;                            // plane LU factors (plane storage)
   float geNS[BC_MAX_NL], geEW[BC_MAX_NL];          // cell <-> package edge conductance per layer
   float escNS;                                     // N/S package rows: edge conductance scale 2^k
@@ -59,7 +60,7 @@ struct BcLevelDev {
 struct BcLevel {
   int nc;
   long long plane, ncell, n;
-  float *cN, *cS, *cW, *cE, *cA, *cB, *dg;
+  float *cN, *cS, *cW, *cE, *cA, *cB, *dg, *rs;
   float *LF, *UB;              // plane LU factors (plane storage)
   float *x, *f, *r;
   float *pr, *py;              // plane right-hand sides and forward-pass values (plane storage)
@@ -72,7 +73,7 @@ struct BcWork {
   BcPack pk;
   BcPack *d_pk;
   double geNS0[BC_MAX_NL], geEW0[BC_MAX_NL];
-  double *c64;                 // 7 x ncell: cN cS cW cE cA cB dg (FP64, level 0)
+  double *c64;                 // 8 x ncell: cN cS cW cE cA cB dg rs (FP64, level 0)
   double *b64, *r64;           // right-hand side, residual (vlen)
   double *band;                // FP64 band scratch of the factorisation
   // BiCGStab vectors (level 0, FP32, n = ncell + 12)
@@ -152,6 +153,14 @@ __global__ void bc_build64(const StencilArgs S, const double *__restrict__ pgrid
   c64[4 * N + c] = n > 0 ? -gA : 0.0;
   c64[5 * N + c] = n < S.nl - 1 ? -gB : 0.0;
   c64[6 * N + c] = dg;
+  // row sum without the package edges: the coefficient of x itself in the
+  // difference form rs x + sum(-c)(x - x_nbr) + ge (x - x_pk)
+  double edges = 0.0;
+  if (L.kind == LK_SPREADER || L.kind == LK_SINK)
+    edges = (i == 0 ? geNS[n] : 0.0) + (i == S.nr - 1 ? geNS[n] : 0.0) + (j == 0 ? geEW[n] : 0.0) +
+            (j == S.nc - 1 ? geEW[n] : 0.0);
+  c64[7 * N + c] = dg + c64[0 * N + c] + c64[1 * N + c] + c64[2 * N + c] + c64[3 * N + c] + c64[4 * N + c] +
+                   c64[5 * N + c] - edges;
   b64[c] = b;
 }
 
@@ -234,7 +243,7 @@ __global__ void bc_pack_residual64(const StencilArgs S, const BcPack *__restrict
 // ---------------------------------------------------------------------------
 // coarse cell (n, i, J) from the fine cells (n, i, 2J) and (n, i, 2J+1)
 __global__ void bc_coarsen(BcLevelDev F, float *cN, float *cS, float *cW, float *cE, float *cA, float *cB,
-                           float *dg, int cnc) {
+                           float *dg, float *rs, int cnc) {
   const long long cpl = (long long)F.nr * cnc;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= cpl * F.nl) return;
@@ -250,6 +259,7 @@ __global__ void bc_coarsen(BcLevelDev F, float *cN, float *cS, float *cW, float 
   cW[t] = 0.5f * wg;
   cE[t] = 0.5f * eg;
   dg[t] = F.dg[a] + F.dg[b] + F.cE[a] + F.cW[b] + 0.5f * wg + 0.5f * eg;
+  rs[t] = F.rs[a] + F.rs[b];   // the pair's row sums (the halving keeps them)
 }
 
 // Plane storage: plane j sits in slot (j & 1) * half + (j >> 1), half =
@@ -583,7 +593,10 @@ __global__ void bc_pack_solve(BcLevelDev L, const BcPack *__restrict__ pk, float
   }
 }
 
-// y = A x (mode 0) or y = f - A x (mode 1), cells
+// y = A x (mode 0) or y = f - A x (mode 1), cells, in difference form
+// rs x + sum(-c)(x - x_nbr) + ge (x - x_pk): the system is nearly singular
+// and the plain form diag*x + sum c*x_nbr would cancel the FP32 digits of
+// smooth vectors
 __global__ void bc_apply_cells(BcLevelDev L, const float *__restrict__ x, float *__restrict__ y,
                                const float *__restrict__ f, int mode) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -591,38 +604,49 @@ __global__ void bc_apply_cells(BcLevelDev L, const float *__restrict__ x, float 
   const int n = (int)(c / L.plane);
   const long long r = c - n * L.plane;
   const int i = (int)(r / L.nc), j = (int)(r - (long long)i * L.nc);
-  float s = L.dg[c] * x[c];
-  if (i > 0) s += L.cN[c] * x[c - L.nc];
-  if (i < L.nr - 1) s += L.cS[c] * x[c + L.nc];
-  if (j > 0) s += L.cW[c] * x[c - 1];
-  if (j < L.nc - 1) s += L.cE[c] * x[c + 1];
-  if (n > 0) s += L.cA[c] * x[c - L.plane];
-  if (n < L.nl - 1) s += L.cB[c] * x[c + L.plane];
+  const float xc = x[c];
+  float s = L.rs[c] * xc;
+  if (i > 0) s -= L.cN[c] * (xc - x[c - L.nc]);
+  if (i < L.nr - 1) s -= L.cS[c] * (xc - x[c + L.nc]);
+  if (j > 0) s -= L.cW[c] * (xc - x[c - 1]);
+  if (j < L.nc - 1) s -= L.cE[c] * (xc - x[c + 1]);
+  if (n > 0) s -= L.cA[c] * (xc - x[c - L.plane]);
+  if (n < L.nl - 1) s -= L.cB[c] * (xc - x[c + L.plane]);
   if (n == L.spidx || n == L.hsidx) {
     const float *xp = x + L.ncell;
-    if (i == 0) s -= L.geNS[n] * xp[bc_edge_node(n, 0, L.spidx, L.hsidx)];
-    if (i == L.nr - 1) s -= L.geNS[n] * xp[bc_edge_node(n, 1, L.spidx, L.hsidx)];
-    if (j == 0) s -= L.geEW[n] * xp[bc_edge_node(n, 2, L.spidx, L.hsidx)];
-    if (j == L.nc - 1) s -= L.geEW[n] * xp[bc_edge_node(n, 3, L.spidx, L.hsidx)];
+    if (i == 0) s += L.geNS[n] * (xc - xp[bc_edge_node(n, 0, L.spidx, L.hsidx)]);
+    if (i == L.nr - 1) s += L.geNS[n] * (xc - xp[bc_edge_node(n, 1, L.spidx, L.hsidx)]);
+    if (j == 0) s += L.geEW[n] * (xc - xp[bc_edge_node(n, 2, L.spidx, L.hsidx)]);
+    if (j == L.nc - 1) s += L.geEW[n] * (xc - xp[bc_edge_node(n, 3, L.spidx, L.hsidx)]);
   }
   y[c] = mode ? f[c] - s : s;
 }
 
-// same, package rows (one CTA)
+// same, package rows (one CTA), difference form
 __global__ void bc_apply_pack(BcLevelDev L, const BcPack *__restrict__ pk, const float *__restrict__ x,
                               float *__restrict__ y, const float *__restrict__ f, int mode) {
   __shared__ float esum[BNX];
-  bc_edge_sums(L, pk, x, esum);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const float *xp = x + L.ncell;
+  for (int k = w; k < BNX; k += blockDim.x >> 5) {
+    float s = 0.f;
+    const int layer = pk->elayer[k], side = pk->eside[k];
+    if (layer >= 0) {
+      const int len = side < 2 ? L.nc : L.nr;
+      const long long base = (long long)layer * L.plane +
+                             (side == 0 ? 0 : side == 1 ? (long long)(L.nr - 1) * L.nc : side == 2 ? 0 : L.nc - 1);
+      const long long st = side < 2 ? 1 : L.nc;
+      const float xk = xp[k];
+      for (int q = lane; q < len; q += 32) s += xk - x[base + q * st];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    if (lane == 0) esum[k] = s;
+  }
   __syncthreads();
   if (threadIdx.x < BNX) {
     const int k = threadIdx.x;
-    const float *xp = x + L.ncell;
-    const int cnt = pk->elayer[k] < 0 ? 0 : (pk->eside[k] < 2 ? L.nc : L.nr);
-    const float ge = bc_pack_ge(L, pk, k);
-    float D = cnt * ge + (float)pk->gamb[k];
-    for (int o = 0; o < BNX; o++) D += (float)pk->link[k][o];
-    float s = D * xp[k] - ge * esum[k];
-    for (int o = 0; o < BNX; o++) s -= (float)pk->link[k][o] * xp[o];
+    float s = bc_pack_ge(L, pk, k) * esum[k] + (float)pk->gamb[k] * xp[k];
+    for (int o = 0; o < BNX; o++) s += (float)pk->link[k][o] * (xp[k] - xp[o]);
     y[L.ncell + k] = mode ? f[L.ncell + k] - s : s;
   }
 }
@@ -818,6 +842,7 @@ static BcLevelDev bc_dev(const hsb_dev_model *m, const BcWork *w, int k) {
   d.nl = m->nl; d.nr = m->nr; d.nc = L.nc;
   d.plane = L.plane; d.ncell = L.ncell;
   d.cN = L.cN; d.cS = L.cS; d.cW = L.cW; d.cE = L.cE; d.cA = L.cA; d.cB = L.cB; d.dg = L.dg;
+  d.rs = L.rs;
   d.LF = L.LF; d.UB = L.UB;
   d.pinv = L.pinv;
   const double sc = (double)(1ll << k);
@@ -838,7 +863,7 @@ static void free_bc(void *p) {
   BcWork *w = (BcWork *)p;
   if (!w) return;
   for (auto &L : w->lv) {
-    float *b[] = {L.cN, L.cS, L.cW, L.cE, L.cA, L.cB, L.dg, L.LF, L.UB, L.x, L.f, L.r, L.pr, L.py, L.pinv};
+    float *b[] = {L.cN, L.cS, L.cW, L.cE, L.cA, L.cB, L.dg, L.rs, L.LF, L.UB, L.x, L.f, L.r, L.pr, L.py, L.pinv};
     for (float *q : b)
       if (q) cudaFree(q);
   }
@@ -873,7 +898,7 @@ static int bc_setup(hsb_dev_model *m, BcWork **out) {
   };
   size_t band_max = 0;
   for (auto &L : w->lv) {
-    float **arr[] = {&L.cN, &L.cS, &L.cW, &L.cE, &L.cA, &L.cB, &L.dg};
+    float **arr[] = {&L.cN, &L.cS, &L.cW, &L.cE, &L.cA, &L.cB, &L.dg, &L.rs};
     for (float **a : arr)
       if (cudaMalloc(a, sizeof(float) * L.ncell) != cudaSuccess) return fail(set_error(HSB_E_NOMEM, "BiCGStab levels"));
     const size_t nqa = (size_t)L.ncell;   // planes x nq
@@ -888,7 +913,7 @@ static int bc_setup(hsb_dev_model *m, BcWork **out) {
     if (bm > band_max) band_max = bm;
   }
   const long long n0 = m->vlen;
-  if (cudaMalloc(&w->d_pk, sizeof(BcPack)) != cudaSuccess || cudaMalloc(&w->c64, sizeof(double) * 7 * m->ncell) != cudaSuccess ||
+  if (cudaMalloc(&w->d_pk, sizeof(BcPack)) != cudaSuccess || cudaMalloc(&w->c64, sizeof(double) * 8 * m->ncell) != cudaSuccess ||
       cudaMalloc(&w->b64, sizeof(double) * n0) != cudaSuccess || cudaMalloc(&w->r64, sizeof(double) * n0) != cudaSuccess ||
       cudaMalloc(&w->band, sizeof(double) * band_max) != cudaSuccess)
     return fail(set_error(HSB_E_NOMEM, "BiCGStab operator"));
@@ -999,11 +1024,12 @@ static int bc_build(hsb_dev_model *m, BcWork *w) {
   bc_build64<<<bnb(m->vlen), BCT, 0, m->stream>>>(S, m->pgrid, d_ge, d_ge + BC_MAX_NL, w->c64, w->b64, d_gamb);
   // FP32 level 0 and the coarse levels
   BcLevel &L0 = w->lv[0];
-  float *dst[7] = {L0.cN, L0.cS, L0.cW, L0.cE, L0.cA, L0.cB, L0.dg};
-  for (int a = 0; a < 7; a++) bc_to32<<<bnb(m->ncell), BCT, 0, m->stream>>>(w->c64 + (size_t)a * m->ncell, dst[a], m->ncell);
+  float *dst[8] = {L0.cN, L0.cS, L0.cW, L0.cE, L0.cA, L0.cB, L0.dg, L0.rs};
+  for (int a = 0; a < 8; a++) bc_to32<<<bnb(m->ncell), BCT, 0, m->stream>>>(w->c64 + (size_t)a * m->ncell, dst[a], m->ncell);
   for (int k = 1; k < w->nlev; k++) {
     BcLevel &C = w->lv[k];
-    bc_coarsen<<<bnb(C.ncell), BCT, 0, m->stream>>>(bc_dev(m, w, k - 1), C.cN, C.cS, C.cW, C.cE, C.cA, C.cB, C.dg, C.nc);
+    bc_coarsen<<<bnb(C.ncell), BCT, 0, m->stream>>>(bc_dev(m, w, k - 1), C.cN, C.cS, C.cW, C.cE, C.cA, C.cB, C.dg,
+                                                    C.rs, C.nc);
   }
   for (int k = 0; k < w->nlev; k++) {
     BcLevel &L = w->lv[k];
