@@ -242,6 +242,8 @@ _SIGS = {
     "hsb_server_destroy": (None, [C.c_void_p]),
     "hsb_server_add_model": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_longlong]),
     "hsb_server_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "hsb_server_set_priority": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "hsb_dev_set_priority": (C.c_int, [C.c_void_p, C.c_int]),
     "hsb_batch_tuning": (C.c_int, [C.c_void_p, _D, C.c_int]),
 }
 

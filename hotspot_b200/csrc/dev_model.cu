@@ -591,6 +591,18 @@ int hsb_dev_steady(hsb_dev_model *m, const double *block_power, double *block_te
   return HSB_OK;
 }
 
+int hsb_dev_set_priority(hsb_dev_model *m, int high) {
+  if (!m) return set_error(HSB_E_ARG, "null model");
+  int least = 0, greatest = 0;
+  HSB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  cudaStream_t s;
+  HSB_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, high ? greatest : least));
+  HSB_CUDA(cudaStreamSynchronize(m->stream));   // nothing of the model is left in flight
+  cudaStreamDestroy(m->stream);
+  m->stream = s;
+  return HSB_OK;
+}
+
 int hsb_dev_get_state(hsb_dev_model *m, int which, double *out) {
   if (!m || !out) return set_error(HSB_E_ARG, "null argument");
   HSB_CUDA(cudaMemcpyAsync(out, which ? m->ys : m->y, sizeof(double) * m->vlen,

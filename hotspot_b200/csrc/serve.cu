@@ -14,7 +14,10 @@
 // the model's declared workspace plus the reserve; later requests of that
 // model allocate nothing.  Among admissible requests the one with the least
 // estimated work (cells x passes) goes first, so short requests are not
-// held behind long ones; ties go to the earlier arrival.
+// held behind long ones; ties go to the earlier arrival.  Models of the high
+// priority class (hsb_server_set_priority) are dispatched before all others
+// and run on high-priority streams, so their kernels are scheduled ahead of
+// the other requests' on the device too.
 //
 // Each request's result depends only on its model and inputs: the kernels
 // are deterministic and models share no mutable device state, so a result
@@ -39,6 +42,7 @@ struct hsb_server {
     long long workspace;
     bool warm = false;   // workspace allocated by an earlier request
     bool busy = false;
+    int high = 0;        // priority class
   };
   std::vector<Model> models;
 };
@@ -69,6 +73,14 @@ int hsb_server_add_model(hsb_server *s, hsb_dev_model *m, int form, double stead
   e.workspace = workspace_bytes;
   s->models.push_back(e);
   return (int)s->models.size() - 1;
+}
+
+int hsb_server_set_priority(hsb_server *s, int model, int high) {
+  if (!s || model < 0 || model >= (int)s->models.size()) return set_error(HSB_E_ARG, "unknown model");
+  const int rc = hsb_dev_set_priority(s->models[model].m, high);
+  if (rc) return rc;
+  s->models[model].high = high ? 1 : 0;
+  return HSB_OK;
 }
 
 // one request, synchronously, on the calling thread
@@ -128,8 +140,17 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
           }
           if ((long long)free_b < M.workspace + s->reserve) continue;
         }
-        if (best < 0 || cost(r) < cost(reqs[best]) ||
-            (cost(r) == cost(reqs[best]) && r.arrival < reqs[best].arrival))
+        // high-priority models first, then the least work, then the earliest arrival
+        if (best < 0) {
+          best = k;
+          continue;
+        }
+        const int hb = s->models[reqs[best].model].high, hr = M.high;
+        if (hr != hb) {
+          if (hr > hb) best = k;
+          continue;
+        }
+        if (cost(r) < cost(reqs[best]) || (cost(r) == cost(reqs[best]) && r.arrival < reqs[best].arrival))
           best = k;
       }
       if (best < 0 && running == 0 && next_arrival >= 1e300) {

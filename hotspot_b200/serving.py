@@ -68,6 +68,10 @@ class Server:
         self.models.append(model)
         return idx
 
+    def set_priority(self, model: int, high: bool = True):
+        """Dispatch this model's requests first and run them on a high-priority stream."""
+        _check(lib().hsb_server_set_priority(self.ptr, int(model), int(bool(high))))
+
     def run(self, requests: list[Request]):
         n = len(requests)
         arr = (_abi.Request * n)()
@@ -117,17 +121,23 @@ class Mix:
 def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.0, duration: float = 1.0,
                 steady_frac: float = 0.7, transient_steps: int = 500, dt: float = 3.333e-6,
                 steady_sides=(64, 128, 256, 512, 1024), transient_sides=(64, 128, 256),
-                max_layers: int = 8, model_factory=None) -> Mix:
+                max_layers: int = 8, model_factory=None, high_priority_cells: int = 0,
+                reuse: Mix | None = None) -> Mix:
     """Seeded Poisson arrivals at `rate` req/s for `duration` s.  Steady
     requests: side drawn log-uniformly from `steady_sides`, 1..max_layers
     chip layers; transients: `transient_steps` intervals of `dt` on
     `transient_sides`.  One resident model per (kind, side, layers) class,
     registered on `server`; every request carries its own power map
     (U(0.5, 20) W per block, AR(1) over a transient) and transients their
-    initial block temperatures, so results do not depend on history."""
+    initial block temperatures, so results do not depend on history.
+    Steady classes of at most `high_priority_cells` cells get the high
+    priority class.  `reuse`: the resident models of an earlier mix on the
+    same server serve the classes they cover."""
     from . import model as hm
     rng = np.random.default_rng(seed)
     mix = Mix(requests=[])
+    if reuse is not None:
+        mix.classes, mix.models = reuse.classes, reuse.models
     t = 0.0
     model_factory = model_factory or hm.from_scenario
     scen = {}
@@ -148,6 +158,8 @@ def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.
             mix.models.append(m)
             scen[key] = sc
             mix.classes[key] = server.add_model(m, FORM_FAST, 1e-5)
+            if steady and m.n_cells <= high_priority_cells:
+                server.set_priority(mix.classes[key], True)
         mi = mix.classes[key]
         m = server.models[mi]
         nblk = sum(m.layer_units[l] for l in range(m.n_layers) if m.layer_power[l])

@@ -221,6 +221,13 @@ int  hsb_server_add_model(hsb_server *s, hsb_dev_model *m, int form, double stea
                           long long workspace_bytes);
 /* serve n requests (released at their arrival times); returns when all are done */
 int  hsb_server_run(hsb_server *s, hsb_request *reqs, int n);
+/* priority class of a registered model: its requests are dispatched before
+ * normal ones and its kernels run on a high-priority stream (high = 1) */
+int  hsb_server_set_priority(hsb_server *s, int model, int high);
+
+/* run the model's work on a high-priority (high = 1) or normal stream; call
+ * with no work of the model in flight */
+int hsb_dev_set_priority(hsb_dev_model *m, int high);
 
 /* which: 0 = transient state (last_trans), 1 = steady state (last_steady);
  * n = nl*nr*nc + n_extra doubles */

@@ -42,6 +42,7 @@ def test_alone_equals_mixed(workdir):
     srv = Server(workers=4)
     for m in models:
         srv.add_model(m, _abi.FORM_FAST, 1e-6)
+    srv.set_priority(0, True)        # a high-priority class: its own stream priority, dispatched first
     mixed = _requests(srv, scs, models, np.random.default_rng(91), 24, 4000.0)
     # alone: the same requests one at a time
     alone = [Request(r.model, r.kind, r.power, 0.0, r.temp_in, r.steps, r.dt, r.tag) for r in mixed]

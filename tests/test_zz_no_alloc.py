@@ -6,8 +6,9 @@ cudaMalloc's implicit synchronisation) get one more C entry point that runs
 the fast transient form with its temporaries in a static device array.
 This test calls it through the C-ABI on a state and power vectors held in
 device memory, twice in a row, and checks each result against the regular
-entry point (the fast form of compute_temp on the same model inputs) within
-the parity tolerance used by the GPU tests.  It lives in its own file so a
+entry point (compute_temp with the stage-by-stage fast form, the arithmetic
+the allocation-free entry point runs) within the parity tolerance used by the
+GPU tests.  It lives in its own file so a
 run that stops at the first failure has run every other test first; it
 passes alone in a fresh process and after the other tests.
 """
@@ -16,7 +17,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from hotspot_b200 import FORM_FAST, _abi
+from hotspot_b200 import FORM_FAST_STAGES, _abi
 from hotspot_b200 import model as hm
 from hotspot_b200 import workloads as W
 from oracle.restatement import OracleModel
@@ -31,9 +32,9 @@ def test_noalloc_matches_regular_entry(workdir):
     sc = W.scenario_chip2d(workdir, seed=31, grid=64, steps=3)
     L = _abi.lib()
 
-    # regular entry point: fast form through compute_temp
+    # regular entry point: the stage-by-stage fast form through compute_temp
     a = hm.from_scenario(sc)
-    a.set_solver(FORM_FAST)
+    a.set_solver(FORM_FAST_STAGES)
     temp = a.vector(a.config.init_temp)
     p0 = a.power_vector(sc.block_power[0])
     a.compute_temp(p0.copy(), temp, 0.0)          # zero-length interval: state = b2g(temp)
