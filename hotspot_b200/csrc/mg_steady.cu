@@ -30,6 +30,9 @@ namespace hsb {
 
 #define MGT 256
 #define NXP 12
+#ifndef MG_INNER
+#define MG_INNER 4   // PCG iterations per FP64 refinement pass
+#endif
 
 struct PackSys {               // the 12 package nodes' equations
   float D[NXP];                // diagonal (edge cells + links + ambient) at level 0
@@ -1005,7 +1008,7 @@ int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
   const MgLevelDev d0 = dev_level(m, L0, 0);
   double *sc = w->red;   // [0] rz, [1] pq, [2] rz_new, [3] max|e| bits, [4] max|r| bits
   unsigned long long *maxbits = (unsigned long long *)(w->red + 4);
-  const int inner = 6;
+  const int inner = MG_INNER;
   // one refinement pass: r = b - G T (FP64), `inner` PCG iterations on
   // G e = r (FP32), T += e, |e|_2^2 to the host; the same kernel sequence
   // every time, so it is captured once as a CUDA graph and replayed

@@ -654,7 +654,10 @@ static int batch_schedule(hsb_batch *b) {
   std::vector<int> g(b->n, 1);
   double w_small = 0.0, sum_g = 0.0;
   for (int c = 0; c < b->n; c++) {
-    int q = (int)(wk[c] / share * b->split);
+    // a chip worth more than one fair share gets enough CTAs that none of
+    // them carries more than a share (rounded up, not down)
+    const double ratio = wk[c] / share * b->split;
+    int q = ratio > 1.0 ? (int)ceil(ratio) : 1;
     if (q > b->h_chips[c].ntiles) q = b->h_chips[c].ntiles;
     if (q >= 2) {
       g[c] = q;
@@ -898,7 +901,7 @@ int hsb_batch_autotune(hsb_batch *b, int enable) {
   }
   b->cands.clear();
   const int cps[2] = {2, 1};
-  const double split[3] = {1.0, 1.5, 0.75};
+  const double split[3] = {1.0, 1.5, 2.0};
   const int ring[2] = {0, 2};
   for (int a : cps)
     for (double sp : split)
