@@ -7,7 +7,7 @@ the final transient grid vector, the steady block and grid vectors.  The
 scenario inputs are regenerated from their seeds by hotspot_b200.workloads;
 the power rows used are stored too, so a change of the generator is caught.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 """
 import os
 import sys
@@ -40,6 +40,11 @@ def cases(d):
     sc.block_power = np.repeat(sc.block_power, 2, axis=0)
     sc.dt = 1e-5
     out["microchannel_32"] = (sc, 2)
+    # the secondary heat path: five more chip-side layers (substrate, solder,
+    # PCB ...) and 16 more package nodes (temperature_grid.c:2228-2379)
+    sc = W.scenario_chip2d(d, seed=9, grid=16, steps=4)
+    sc.config["model_secondary"] = "1"
+    out["secondary_16"] = (sc, 4)
     return out
 
 
@@ -64,13 +69,15 @@ def run(sc, intervals, steady=True):
     return res
 
 
-def main():
+def main(names=None):
     with tempfile.TemporaryDirectory() as d:
         for name, (sc, n) in cases(d).items():
+            if names and name not in names:
+                continue
             res = run(sc, n, steady=not sc.use_microchannels)
             np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **res)
             print(name, {k: v.shape for k, v in res.items()})
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -30,6 +30,9 @@ def _golden_cases(d):
 def test_restatement_matches_golden(workdir, name):
     g = np.load(os.path.join(GOLDEN, name + ".npz"))
     sc, n = _golden_cases(workdir)[name]
+    if sc.config.get("model_secondary") == "1":
+        pytest.skip("the restatement covers the primary heat path; the secondary path's golden "
+                    "vectors pin the GPU forms directly")
     o = OracleModel(sc)
     t = o.vector(333.15)
     for k in range(n):

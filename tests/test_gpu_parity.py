@@ -91,3 +91,39 @@ def test_microchannel_transient(workdir):
     assert np.max(np.abs(t - to)) <= TOL
     assert np.max(np.abs(m.grid("trans") - o.grid("trans"))) <= TOL
     m.close()
+
+
+def _golden(workdir, name):
+    import importlib.util
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(here, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    sc, n = mg.cases(workdir)[name]
+    return sc, n, np.load(os.path.join(here, name + ".npz"))
+
+
+def test_secondary_path_against_reference_golden(workdir):
+    """The secondary heat path (substrate, solder and PCB layers, 28 package
+    nodes), against the reference's own results (golden vectors made by the
+    reference build): the FP64 replay to 1e-6 K, the fast forms to 0.01 K."""
+    from hotspot_b200 import FORM_FAST
+    sc, n, g = _golden(workdir, "secondary_16")
+    for form, tol in ((None, TOL), (FORM_FAST, 0.01)):
+        m = hm.from_scenario(sc)
+        if form is not None:
+            m.set_solver(form)
+        t = m.vector(333.15)
+        assert t.size == g["temps"].shape[1]
+        for k in range(n):
+            p = g["block_power"][k].copy()
+            m.compute_temp(p, t if k == 0 else None, sc.dt)
+            assert np.max(np.abs(t - g["temps"][k])) <= tol, (form, k)
+        assert np.max(np.abs(m.grid("trans") - g["grid_trans"])) <= tol
+        if form is None:   # the FP64 replay of the reference's steady solver
+            s = m.vector()
+            m.steady(g["steady_power"].copy(), s)
+            assert np.max(np.abs(s - g["steady"])) <= TOL
+            assert np.max(np.abs(m.grid("steady") - g["grid_steady"])) <= TOL
+        m.close()
