@@ -556,7 +556,9 @@ def run_ours(args):
 
     peak, peak_kind = measured_peak()
     alg_bytes_launch = ALG_BYTES_FP32 * ncell * steps_total / K
-    achieved = alg_bytes_launch / ((ker_ms / K) / 1e3) / 1e9
+    # the kernel's own events; if the library could not time it, the whole interval
+    kernel_timed = ker_ms > 0
+    achieved = alg_bytes_launch / (((ker_ms if kernel_timed else dev_ms) / K) / 1e3) / 1e9
     traffic = profiled_traffic("rk4_krylov_kernel_stack256.md")
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": K,
@@ -576,7 +578,8 @@ def run_ours(args):
                      "alg_bytes_per_launch": alg_bytes_launch,
                      "note": "one launch = one sampling interval; 108 B per cell-step (FP32 stages, FP64 "
                              "state); the 393k-cell state fits the 126 MB L2, so the kernel is latency-bound, "
-                             "not HBM-bound"},
+                             "not HBM-bound" + ("" if kernel_timed else "; kernel events unavailable: duration = "
+                                                "the whole interval's device time")},
         "gpu_launches": launches,
         "trace": dict(trace, note="K intervals through hsb_dev_transient_trace: one persistent launch, device "
                                   "time including the copy of the K block-power rows"),

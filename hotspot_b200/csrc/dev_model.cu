@@ -85,10 +85,9 @@ __global__ void b2g_kernel(const int *__restrict__ ptr, const int *__restrict__ 
 }
 
 // grid -> block (xlate_temp_g2b, temperature_grid.c:1932-2015)
-__global__ void g2b_kernel(const int *__restrict__ map, const double *__restrict__ g,
-                           double *__restrict__ b, int nblk, int nx, int nr, int nc,
-                           long long ncell, int mode) {
-  int u = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void g2b_one(const int *__restrict__ map, const double *__restrict__ g,
+                                        double *__restrict__ b, int nblk, int nx, int nr, int nc, long long ncell,
+                                        int mode, int u) {
   if (u < nblk) {
     const int n = map[5 * u], i1 = map[5 * u + 1], i2 = map[5 * u + 2];
     const int j1 = map[5 * u + 3], j2 = map[5 * u + 4];
@@ -116,6 +115,20 @@ __global__ void g2b_kernel(const int *__restrict__ map, const double *__restrict
   }
 }
 
+__global__ void g2b_kernel(const int *__restrict__ map, const double *__restrict__ g,
+                           double *__restrict__ b, int nblk, int nx, int nr, int nc,
+                           long long ncell, int mode) {
+  g2b_one(map, g, b, nblk, nx, nr, nc, ncell, mode, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// the same on whichever of g0 / g1 the device word *which selects
+__global__ void g2b_select_kernel(const int *__restrict__ map, const double *__restrict__ g0,
+                                  const double *__restrict__ g1, const long long *__restrict__ which,
+                                  double *__restrict__ b, int nblk, int nx, int nr, int nc, long long ncell,
+                                  int mode) {
+  g2b_one(map, *which ? g1 : g0, b, nblk, nx, nr, nc, ncell, mode, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 int b2g(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type) {
   return b2g_on(m, blk_dev, grid_dev, type, m->stream);
 }
@@ -132,6 +145,14 @@ int b2g_on(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type, 
 
 int g2b(hsb_dev_model *m, const double *grid_dev, double *blk_dev) {
   return g2b_on(m, grid_dev, blk_dev, m->stream);
+}
+
+int g2b_select(hsb_dev_model *m, const double *g0, const double *g1, const long long *which, double *blk_dev) {
+  const int n = m->total_n_blocks + m->nx, T = 128;
+  g2b_select_kernel<<<(n + T - 1) / T, T, 0, m->stream>>>(m->g2b, g0, g1, which, blk_dev, m->total_n_blocks,
+                                                          m->nx, m->nr, m->nc, m->ncell, m->map_mode);
+  HSB_CUDA(cudaGetLastError());
+  return HSB_OK;
 }
 
 int g2b_on(hsb_dev_model *m, const double *grid_dev, double *blk_dev, cudaStream_t s) {
@@ -231,6 +252,10 @@ static void free_model(hsb_dev_model *m) {
   if (m->gs_status) cudaFree(m->gs_status);
   if (m->h_err) cudaFreeHost(m->h_err);
   if (m->h_blk) cudaFreeHost(m->h_blk);
+  for (auto &g : m->ivg)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (m->ev[0]) cudaEventDestroy(m->ev[0]);
+  if (m->ev[1]) cudaEventDestroy(m->ev[1]);
   if (m->h_gs) cudaFreeHost(m->h_gs);
   if (m->h_gsd) cudaFreeHost(m->h_gsd);
   if (m->levels) {
@@ -283,6 +308,10 @@ int hsb_dev_create(hsb_dev_model **out, const hsb_grid_desc *d) {
   {
     cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { rc = cuda_check(e, "cudaStreamCreate"); goto fail; }
+    if ((e = cudaEventCreate(&m->ev[0])) != cudaSuccess || (e = cudaEventCreate(&m->ev[1])) != cudaSuccess) {
+      rc = cuda_check(e, "cudaEventCreate");
+      goto fail;
+    }
   }
   {
     const size_t vb = sizeof(double) * (size_t)m->vlen;
@@ -446,6 +475,92 @@ int hsb_dev_set_maps(hsb_dev_model *m, const int *b2g_ptr, const int *b2g_blk,
   return HSB_OK;
 }
 
+// The fast form's interval replayed from a CUDA graph: the block powers
+// from pinned staging, the Krylov kernel (which maps them to the grid
+// itself), its counters to the host, g2b of the state buffer the kernel
+// ended in and the block temperatures back to staging -- one launch and one
+// wait per interval.  Returns 1, having done nothing, when the sequence
+// cannot be captured; the caller then launches step by step.
+static int fast_interval_graphed(hsb_dev_model *m, const double *block_power, double T, double *block_temp_out,
+                                 hsb_stats *st) {
+  const size_t nb = (size_t)m->total_n_blocks + m->nx;
+  void *work = nullptr;
+  const void *fn = nullptr;
+  int rc;
+  if ((rc = rk4_fast_ready(m, &work, &fn))) return rc;
+  const int want = block_temp_out != nullptr;
+  hsb_dev_model::IvGraph *g = nullptr;
+  for (auto &e : m->ivg)
+    if (e.exec && e.y == m->y && e.T == T && e.out == want && e.version == m->coef_version && e.fn == fn &&
+        e.mode == m->map_mode)
+      g = &e;
+  if (!g) {
+    g = &m->ivg[m->ivg_next];
+    m->ivg_next = (m->ivg_next + 1) % 4;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    g->exec = nullptr;
+    hsb_stats scratch;
+    memset(&scratch, 0, sizeof(scratch));
+    if (cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      m->ivg_off = 1;
+      return 1;
+    }
+    bool ok = cudaMemcpyAsync(m->blk_in, m->h_blk, sizeof(double) * nb, cudaMemcpyHostToDevice, m->stream) ==
+              cudaSuccess;
+    void *w2 = nullptr;
+    ok = ok && rk4_fast_interval_begin(m, T, &scratch, &w2, m->blk_in) == HSB_OK;
+    if (ok && want) {
+      double *second;
+      const long long *which;
+      fast_state_buffers(m, w2, &second, &which);
+      ok = g2b_select(m, m->y, second, which, m->blk_out) == HSB_OK &&
+           cudaMemcpyAsync(m->h_blk + nb, m->blk_out, sizeof(double) * nb, cudaMemcpyDeviceToHost, m->stream) ==
+               cudaSuccess;
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(m->stream, &graph);
+    if (!ok || ce != cudaSuccess || !graph || cudaGraphInstantiate(&g->exec, graph, 0) != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      g->exec = nullptr;
+      cudaGetLastError();
+      m->ivg_off = 1;
+      return 1;
+    }
+    cudaGraphDestroy(graph);
+    g->y = m->y;
+    g->T = T;
+    g->out = want;
+    g->version = m->coef_version;
+    g->fn = fn;
+    g->mode = m->map_mode;
+  }
+  memcpy(m->h_blk, block_power, sizeof(double) * nb);
+  HSB_CUDA(cudaEventRecord(m->ev[0], m->stream));
+  HSB_CUDA(cudaGraphLaunch(g->exec, m->stream));
+  HSB_CUDA(cudaEventRecord(m->ev[1], m->stream));
+  HSB_CUDA(cudaStreamSynchronize(m->stream));
+  st->launches += 1 + want;
+  int fell_back = 0;
+  if ((rc = rk4_fast_interval_end(m, work, T, st, &fell_back))) return rc;
+  if (fell_back) {   // the stage form finished the interval in place of the kernel
+    if (want) {
+      if ((rc = g2b(m, m->y, m->blk_out))) return rc;
+      st->launches += 1;
+      HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                               m->stream));
+    }
+    HSB_CUDA(cudaEventRecord(m->ev[1], m->stream));
+    HSB_CUDA(cudaStreamSynchronize(m->stream));
+  } else if (want) {
+    memcpy(block_temp_out, m->h_blk + nb, sizeof(double) * nb);
+  }
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, m->ev[0], m->ev[1]) == cudaSuccess) st->device_ms += ms;
+  else cudaGetLastError();
+  return HSB_OK;
+}
+
 int hsb_dev_transient(hsb_dev_model *m, const double *block_power, const double *block_temp_in,
                       double time_elapsed, double *block_temp_out, const hsb_solver_opts *o,
                       hsb_stats *st) {
@@ -454,11 +569,15 @@ int hsb_dev_transient(hsb_dev_model *m, const double *block_power, const double 
   const size_t nb = (size_t)m->total_n_blocks + m->nx;
   hsb_stats local;
   if (!st) st = &local;
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0, m->stream);
   int rc;
+  const int form = o ? o->form : HSB_FORM_PARITY;
+  // after the first interval (which sets up the workspace) the fast form
+  // replays its interval from a graph
+  if (form == HSB_FORM_FAST && !block_temp_in && m->fast && !m->ivg_off) {
+    rc = fast_interval_graphed(m, block_power, time_elapsed, block_temp_out, st);
+    if (rc != 1) return rc;
+  }
+  cudaEventRecord(m->ev[0], m->stream);
   HSB_CUDA(cudaMemcpyAsync(m->blk_in, block_power, sizeof(double) * nb, cudaMemcpyHostToDevice,
                            m->stream));
   if ((rc = b2g(m, m->blk_in, m->pgrid, HSB_V_POWER))) return rc;
@@ -469,24 +588,50 @@ int hsb_dev_transient(hsb_dev_model *m, const double *block_power, const double 
     if ((rc = b2g(m, m->blk_in + nb, m->y, HSB_V_TEMP))) return rc;
     st->launches += 1;
   }
-  const int form = o ? o->form : HSB_FORM_PARITY;
-  rc = form == HSB_FORM_FAST          ? rk4_fast_interval(m, time_elapsed, st)
-       : form == HSB_FORM_FAST_STAGES ? rk4_fast_stages_interval(m, time_elapsed, st)
+  if (form == HSB_FORM_FAST) {
+    // the Krylov launch, then the block temperatures read from whichever
+    // state buffer the kernel ended in (chosen on the device), one wait
+    void *work = nullptr;
+    if ((rc = rk4_fast_interval_begin(m, time_elapsed, st, &work, nullptr))) return rc;
+    if (block_temp_out) {
+      double *second;
+      const long long *which;
+      fast_state_buffers(m, work, &second, &which);
+      if ((rc = g2b_select(m, m->y, second, which, m->blk_out))) return rc;
+      st->launches += 1;
+      HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                               m->stream));
+    }
+    cudaEventRecord(m->ev[1], m->stream);
+    HSB_CUDA(cudaStreamSynchronize(m->stream));
+    int fell_back = 0;
+    if ((rc = rk4_fast_interval_end(m, work, time_elapsed, st, &fell_back))) return rc;
+    if (fell_back) {   // the stage form finished the interval: its state
+      if (block_temp_out) {
+        if ((rc = g2b(m, m->y, m->blk_out))) return rc;
+        st->launches += 1;
+        HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                                 m->stream));
+      }
+      cudaEventRecord(m->ev[1], m->stream);
+      HSB_CUDA(cudaStreamSynchronize(m->stream));
+    }
+  } else {
+    rc = form == HSB_FORM_FAST_STAGES ? rk4_fast_stages_interval(m, time_elapsed, st)
                                       : rk4_exact_interval(m, time_elapsed, st);
-  if (rc) return rc;
-  if (block_temp_out) {
-    if ((rc = g2b(m, m->y, m->blk_out))) return rc;
-    st->launches += 1;
-    HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb,
-                             cudaMemcpyDeviceToHost, m->stream));
+    if (rc) return rc;
+    if (block_temp_out) {
+      if ((rc = g2b(m, m->y, m->blk_out))) return rc;
+      st->launches += 1;
+      HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb,
+                               cudaMemcpyDeviceToHost, m->stream));
+    }
+    cudaEventRecord(m->ev[1], m->stream);
+    HSB_CUDA(cudaStreamSynchronize(m->stream));
   }
-  cudaEventRecord(e1, m->stream);
-  HSB_CUDA(cudaStreamSynchronize(m->stream));
   float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
-  st->device_ms += ms;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (cudaEventElapsedTime(&ms, m->ev[0], m->ev[1]) == cudaSuccess) st->device_ms += ms;
+  else cudaGetLastError();
   return HSB_OK;
 }
 
@@ -506,10 +651,7 @@ int hsb_dev_transient_trace(hsb_dev_model *m, const double *block_powers, int K,
     }
     return HSB_OK;
   }
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0, m->stream);
+  cudaEventRecord(m->ev[0], m->stream);
   int rc;
   // the block powers of all intervals, in a device buffer kept with the model
   if (m->trace_cap < (long long)(K * nb)) {
@@ -531,13 +673,11 @@ int hsb_dev_transient_trace(hsb_dev_model *m, const double *block_powers, int K,
     st->launches += 1;
     HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb, cudaMemcpyDeviceToHost, m->stream));
   }
-  cudaEventRecord(e1, m->stream);
+  cudaEventRecord(m->ev[1], m->stream);
   HSB_CUDA(cudaStreamSynchronize(m->stream));
   float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
-  st->device_ms += ms;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (cudaEventElapsedTime(&ms, m->ev[0], m->ev[1]) == cudaSuccess) st->device_ms += ms;
+  else cudaGetLastError();
   return HSB_OK;
 }
 
@@ -550,10 +690,7 @@ int hsb_dev_steady(hsb_dev_model *m, const double *block_power, double *block_te
   if (!st) st = &local;
   hsb_solver_opts def = {HSB_FORM_PARITY, HSB_STEADY_AUTO, 0.0, 0};
   if (!o) o = &def;
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0, m->stream);
+  cudaEventRecord(m->ev[0], m->stream);
   int rc;
   HSB_CUDA(cudaMemcpyAsync(m->blk_in, block_power, sizeof(double) * nb, cudaMemcpyHostToDevice,
                            m->stream));
@@ -581,13 +718,11 @@ int hsb_dev_steady(hsb_dev_model *m, const double *block_power, double *block_te
     HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb,
                              cudaMemcpyDeviceToHost, m->stream));
   }
-  cudaEventRecord(e1, m->stream);
+  cudaEventRecord(m->ev[1], m->stream);
   HSB_CUDA(cudaStreamSynchronize(m->stream));
   float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
-  st->device_ms += ms;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (cudaEventElapsedTime(&ms, m->ev[0], m->ev[1]) == cudaSuccess) st->device_ms += ms;
+  else cudaGetLastError();
   return HSB_OK;
 }
 

@@ -94,7 +94,19 @@ struct hsb_dev_model {
   double *blk_in, *blk_out;      // device block vectors (total_n_blocks + nx)
   double *trace_buf;             // block powers of a multi-interval call (trace_cap doubles)
   long long trace_cap;
-  double *h_blk;                 // pinned staging (2 * (total_n_blocks + nx))
+  double *h_blk;                 // pinned staging: [0, nb) block powers in, [nb, 2 nb) block temperatures out
+  cudaEvent_t ev[2];             // call timing events
+  // the fast-form interval as CUDA graphs, one per (state buffer in the
+  // state role, step, output request, coefficient version, kernel, g2b mode)
+  struct IvGraph {
+    const double *y;
+    double T;
+    int out, version, mode;
+    const void *fn;
+    cudaGraphExec_t exec;
+  } ivg[4];
+  int ivg_next;
+  int ivg_off;                   // capture refused once: launch by launch from then on
 
   // multigrid levels for the exact nested-iteration replay
   int n_levels;
@@ -113,6 +125,10 @@ struct hsb_dev_model {
   void (*mg_free)(void *);
   void *krylov;
   void (*krylov_free)(void *);
+  // called by the steady solvers between refinement passes (a scheduler
+  // may hold a background request there); null: never
+  void (*yield_fn)(void *);
+  void *yield_ctx;
 };
 
 namespace hsb {
@@ -137,6 +153,14 @@ int gs_exact_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
 // fast-form solvers
 int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
 int rk4_fast_stages_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
+// one interval of the fast form in two halves (rk4_fast.cu)
+int rk4_fast_interval_begin(hsb_dev_model *m, double time_elapsed, hsb_stats *st, void **work,
+                            const double *bpow_dev);
+int rk4_fast_interval_end(hsb_dev_model *m, void *work, double time_elapsed, hsb_stats *st, int *fell_back);
+int rk4_fast_ready(hsb_dev_model *m, void **work, const void **kernel);
+void fast_state_buffers(hsb_dev_model *m, void *work, double **second, const long long **which);
+// g2b of whichever of two grid vectors *which selects (read on the device)
+int g2b_select(hsb_dev_model *m, const double *g0, const double *g1, const long long *which, double *blk_dev);
 // K consecutive intervals of the fast form from K block-power vectors in device memory
 int rk4_fast_trace(hsb_dev_model *m, const double *bpow_dev, int K, double time_elapsed, hsb_stats *st);
 

@@ -82,6 +82,9 @@ struct FastWork {
   long long nstride;
   CUtensorMap kmap_y, kmap_y2, kmap_yi, kmap_y2i, kmap_pf, kmap_N, kmap_Ni;   // kmap_N(i): all vectors, 4-D
   const double *kmap_ybuf, *kmap_y2buf;           // the state buffers kmap_y / kmap_y2 describe
+  const void *kfn;                // Krylov kernel variant kgrid was computed for
+  int kgrid;                      // its co-resident grid
+  cudaEvent_t kev[2];             // kernel timing events
 };
 
 // Layers are processed in fixed-size chunks, so that a chunk's per-cell
@@ -324,5 +327,10 @@ int kry_prepare(hsb_dev_model *m, FastWork *w);
 // *t_done, continue with step size *h_next)
 int rk4_krylov_trace(hsb_dev_model *m, FastWork *w, const double *bpow, int K, double T, hsb_stats *st, int *done,
                      double *t_done, double *h_next);
+// the two halves of a launch: enqueue (kernel + counters to the host, no
+// wait) and complete (after the stream reached the counters)
+int rk4_krylov_enqueue(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, const double *bpow, int K);
+int rk4_krylov_complete(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next,
+                        int *done);
 
 }  // namespace hsb

@@ -585,6 +585,8 @@ static void free_fast(void *p) {
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (w->h_cnt) cudaFreeHost(w->h_cnt);
+  if (w->kev[0]) cudaEventDestroy(w->kev[0]);
+  if (w->kev[1]) cudaEventDestroy(w->kev[1]);
   delete w;
 }
 
@@ -757,6 +759,55 @@ int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
   return HSB_OK;
 }
 
+// one interval in two halves, so the caller can queue work that reads the
+// result (g2b with the state buffer chosen on the device) before waiting;
+// bpow_dev: the block powers, mapped to the grid in the kernel (null: the
+// grid power is in pgrid already)
+int rk4_fast_interval_begin(hsb_dev_model *m, double time_elapsed, hsb_stats *st, void **work,
+                            const double *bpow_dev) {
+  FastWork *w;
+  int rc;
+  if ((rc = fast_prepare(m, &w))) return rc;
+  *work = w;
+  return rk4_krylov_enqueue(m, w, time_elapsed, st, bpow_dev, bpow_dev ? 1 : 0);
+}
+
+int rk4_fast_interval_end(hsb_dev_model *m, void *work, double time_elapsed, hsb_stats *st, int *fell_back) {
+  FastWork *w = (FastWork *)work;
+  int rc, done = 0;
+  double t_done = time_elapsed, h_next = 0.0;
+  *fell_back = 0;
+  if ((rc = rk4_krylov_complete(m, w, time_elapsed, st, &t_done, &h_next, &done))) return rc;
+  if (t_done < time_elapsed) {
+    st->fallbacks += 1;
+    *fell_back = 1;
+    if ((rc = rk4_stage_run(m, w, time_elapsed - t_done, h_next, st))) return rc;
+  }
+  st->sim_time += time_elapsed;
+  return HSB_OK;
+}
+
+// the host-side preparation of the Krylov form (workspace, tensor maps,
+// co-resident grid) without launching anything
+int rk4_fast_ready(hsb_dev_model *m, void **work, const void **kernel) {
+  FastWork *w;
+  int rc;
+  if ((rc = fast_prepare(m, &w))) return rc;
+  if ((rc = kry_prepare(m, w))) return rc;
+  *work = w;
+  *kernel = w->kfn;
+  return HSB_OK;
+}
+
+// the second state buffer of the fast forms and the device word saying
+// which of the two buffers holds the state after the last launch
+void fast_state_buffers(hsb_dev_model *m, void *work, double **second, const long long **which) {
+  (void)m;
+  FastWork *w = (FastWork *)work;
+  *second = w->ytemp;
+  *which = w->cnt + 6;
+}
+
 // K intervals in as few launches as possible: one Krylov-form launch runs
 // them back to back; an interval whose rejection budget runs out is finished
 // by the stage form (from its own grid power) and the launches resume after it
@@ -779,9 +830,8 @@ int rk4_fast_trace(hsb_dev_model *m, const double *bpow_dev, int K, double time_
     if ((rc = rk4_stage_run(m, w, time_elapsed - t_done, h_next, st))) return rc;
     i0 = k + 1;
   }
-  // later single-interval calls find the last interval's grid power in place
-  if ((rc = b2g(m, bpow_dev + (long long)(K - 1) * nb, m->pgrid, HSB_V_POWER))) return rc;
-  st->launches += 1;
+  // the last interval's grid power is in pgrid: the kernel wrote it, or the
+  // b2g before the stage form did
   st->sim_time += time_elapsed * K;
   return HSB_OK;
 }

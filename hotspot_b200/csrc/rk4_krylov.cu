@@ -50,7 +50,7 @@ struct KryArgs {
   const PackF *pk;
   const float *gN, *gS, *gW, *gE, *gA, *gB, *invC;
   const float *aN, *aS, *aW, *aE, *aO;
-  const double *pgrid;
+  double *pgrid;                   // FP64 grid power (read when K = 0, written for the last interval when K > 0)
   float *pf;
   double *y, *y2;                  // the two state buffers (which holds the state alternates)
   float *N;
@@ -437,10 +437,13 @@ __device__ __forceinline__ void kpower(const KryArgs &A, int iv) {
     return;
   }
   const double *b = A.bpow + (long long)iv * A.nbv;
+  const bool last = iv == A.K - 1;   // later calls (and a stage-form fallback) find this power in pgrid
   for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
     double val = 0.0;
     for (int e = A.b2g_ptr[q]; e < A.b2g_ptr[q + 1]; e++) val += A.b2g_occ[e] * b[A.b2g_blk[e]] / A.b2g_area[e];
-    A.pf[q] = (float)(val * A.cell_area);
+    val *= A.cell_area;
+    A.pf[q] = (float)val;
+    if (last) A.pgrid[q] = val;
   }
 }
 
@@ -613,6 +616,16 @@ int kry_prepare(hsb_dev_model *m, FastWork *w) {
     if ((rc = make_map4(&w->kmap_N, w->N, m, KW, HR, KRY_DMAX + 1, w->nstride))) return rc;
     if ((rc = make_map4(&w->kmap_Ni, w->N, m, TJ, TI, KRY_DMAX + 1, w->nstride))) return rc;
   }
+  if (w->kmap_ybuf == w->ytemp && w->kmap_y2buf == m->y) {   // the buffers swapped roles: swap their maps
+    CUtensorMap t = w->kmap_y;
+    w->kmap_y = w->kmap_y2;
+    w->kmap_y2 = t;
+    t = w->kmap_yi;
+    w->kmap_yi = w->kmap_y2i;
+    w->kmap_y2i = t;
+    w->kmap_ybuf = m->y;
+    w->kmap_y2buf = w->ytemp;
+  }
   if (w->kmap_ybuf != m->y) {
     if ((rc = make_map(&w->kmap_y, m->y, true, m, DW, HR))) return rc;
     if ((rc = make_map(&w->kmap_yi, m->y, true, m, TJ, TI))) return rc;
@@ -622,6 +635,15 @@ int kry_prepare(hsb_dev_model *m, FastWork *w) {
     if ((rc = make_map(&w->kmap_y2, w->ytemp, true, m, DW, HR))) return rc;
     if ((rc = make_map(&w->kmap_y2i, w->ytemp, true, m, TJ, TI))) return rc;
     w->kmap_y2buf = w->ytemp;
+  }
+  const void *fn = kry_kernel_for(m->field, m->uchan_mask != 0);
+  if (w->kfn != fn) {   // co-resident grid of this kernel variant, once
+    if ((rc = coop_grid(m, fn, kry_smem(m->nl), &w->kgrid))) return rc;
+    w->kfn = fn;
+  }
+  if (!w->kev[0]) {
+    HSB_CUDA(cudaEventCreate(&w->kev[0]));
+    HSB_CUDA(cudaEventCreate(&w->kev[1]));
   }
   return HSB_OK;
 }
@@ -639,8 +661,8 @@ int rk4_krylov_trace(hsb_dev_model *m, FastWork *w, const double *bpow, int K, d
   return krylov_launch(m, w, T, st, t_done, h_next, bpow, K, done);
 }
 
-static int krylov_launch(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next,
-                         const double *bpow, int K, int *done) {
+// the launch and the copy of its counters to the host, without waiting
+int rk4_krylov_enqueue(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, const double *bpow, int K) {
   int rc;
   if ((rc = kry_prepare(m, w))) return rc;
   KryArgs A;
@@ -681,27 +703,41 @@ static int krylov_launch(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st,
   A.b2g_occ = m->b2g_occ;
   A.b2g_area = m->b2g_area;
   A.cell_area = m->cell_area;
-  const void *fn = kry_kernel_for(m->field, m->uchan_mask != 0);
-  int grid = 0;
-  if ((rc = coop_grid(m, fn, kry_smem(m->nl), &grid))) return rc;
+  const void *fn = w->kfn;
   HSB_CUDA(cudaMemsetAsync(w->cnt, 0, sizeof(long long) * 8, m->stream));
   void *args[] = {&A};
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0, m->stream);
-  HSB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(FT_THREADS), args, kry_smem(m->nl), m->stream));
-  cudaEventRecord(e1, m->stream);
+  // a cooperative launch through the attribute form, which stream capture
+  // records as a cooperative kernel node
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(w->kgrid);
+  cfg.blockDim = dim3(FT_THREADS);
+  cfg.dynamicSmemBytes = kry_smem(m->nl);
+  cfg.stream = m->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  // external records: under stream capture they become event-record nodes,
+  // so a replayed graph still times the kernel
+  HSB_CUDA(cudaEventRecordWithFlags(w->kev[0], m->stream, cudaEventRecordExternal));
+  HSB_CUDA(cudaLaunchKernelExC(&cfg, fn, args));
+  HSB_CUDA(cudaEventRecordWithFlags(w->kev[1], m->stream, cudaEventRecordExternal));
   HSB_CUDA(cudaMemcpyAsync(w->h_cnt, w->cnt, sizeof(long long) * 8, cudaMemcpyDeviceToHost, m->stream));
-  HSB_CUDA(cudaStreamSynchronize(m->stream));
+  st->launches += 1;
+  return HSB_OK;
+}
+
+// after the stream has reached the launch's counters: statistics, the swap of
+// the state buffers, and the outcome (*t_done < T: rejection budget ran out)
+int rk4_krylov_complete(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next,
+                        int *done) {
   {
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    st->kernel_ms += ms;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    if (cudaEventElapsedTime(&ms, w->kev[0], w->kev[1]) == cudaSuccess) st->kernel_ms += ms;
+    else cudaGetLastError();
   }
-  st->launches += 1;
   if (w->h_cnt[6]) {   // the state ended in the second buffer
     double *tmp = m->y;
     m->y = w->ytemp;
@@ -722,6 +758,14 @@ static int krylov_launch(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st,
     *h_next = tout[1];
   }
   return HSB_OK;
+}
+
+static int krylov_launch(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next,
+                         const double *bpow, int K, int *done) {
+  int rc;
+  if ((rc = rk4_krylov_enqueue(m, w, T, st, bpow, K))) return rc;
+  HSB_CUDA(cudaStreamSynchronize(m->stream));
+  return rk4_krylov_complete(m, w, T, st, t_done, h_next, done);
 }
 
 }  // namespace hsb
