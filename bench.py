@@ -344,10 +344,10 @@ def leg_serving(args):
     d = tempfile.mkdtemp(prefix="hsb_srv_")
     srv = Server(workers=8)
     t0 = time.perf_counter()
-    hp = 256 * 256 * 10          # steady classes up to 256x256 with 8 chip layers: high priority
-    mix = serving_mix(d, srv, seed=4, rate=2000.0, duration=args.serving_seconds, high_priority_cells=hp)
+    hp = [(256, 4)]              # the latency-SLO class (256x256, 4 chip layers, steady): high priority
+    mix = serving_mix(d, srv, seed=4, rate=2000.0, duration=args.serving_seconds, high_priority_classes=hp)
     calm = serving_mix(d, srv, seed=5, rate=args.serving_calm_rate, duration=args.serving_calm_seconds,
-                       high_priority_cells=hp, reuse=mix)
+                       high_priority_classes=hp, reuse=mix)
     # every resident model serves one request before the clock starts
     warm = []
     for _, mi in mix.classes.items():
@@ -376,8 +376,9 @@ def leg_serving(args):
     srv.run(calm.requests)
     sustainable = report(calm.requests, args.serving_calm_rate, args.serving_calm_seconds)
     res = {"workload": "Poisson arrivals: 70% steady (sides 64..1024, 1..8 chip layers), 30% 500-interval "
-                       "transients (sides 64..256); one resident model per class; steady classes up to "
-                       "256x256x8 chip layers in the high-priority class",
+                       "transients (sides 64..256); one resident model per class; the 256x256x4-layer steady "
+                       "class (the latency SLO) in the high-priority class, with 2 reserved workers; other "
+                       "requests pause between transient chunks and steady refinement passes while it runs",
            "models": len(mix.models), "workers": 8, "offered_2000_req_per_s": loaded,
            "sustainable_rate": sustainable, "setup_s": setup_s}
     srv.close()

@@ -1065,6 +1065,7 @@ int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
     st->refinements += 1;
     st->cycles += inner;
     if (emax < tol) break;
+    if (m->yield_fn) m->yield_fn(m->yield_ctx);
   }
   // final FP64 residual for the record
   HSB_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), m->stream));

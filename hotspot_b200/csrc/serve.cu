@@ -14,10 +14,18 @@
 // the model's declared workspace plus the reserve; later requests of that
 // model allocate nothing.  Among admissible requests the one with the least
 // estimated work (cells x passes) goes first, so short requests are not
-// held behind long ones; ties go to the earlier arrival.  Models of the high
-// priority class (hsb_server_set_priority) are dispatched before all others
-// and run on high-priority streams, so their kernels are scheduled ahead of
-// the other requests' on the device too.
+// held behind long ones; ties go to the earlier arrival.
+//
+// Priority classes (hsb_server_set_priority): requests of high-priority
+// models are dispatched before all others, run on high-priority streams (the
+// device schedules their thread blocks ahead of pending ones of other
+// streams), and have HIGH_SLOTS worker threads of their own, so they never
+// wait for a worker.  In a run that holds high-priority requests, while any
+// of them runs, the other requests pause at their next yield point: between
+// transient chunks (a background transient then runs its intervals in
+// chunks of about CHUNK_CELL_INTERVALS cell-intervals, so one launch holds
+// the device for about a millisecond) and between the refinement passes of
+// steady solves.
 //
 // Each request's result depends only on its model and inputs: the kernels
 // are deterministic and models share no mutable device state, so a result
@@ -32,6 +40,12 @@
 #include <vector>
 
 #include "dev_model.cuh"
+
+// worker threads reserved for high-priority requests
+#define HIGH_SLOTS 2
+// cell-intervals per launch of a background transient while a priority class runs
+#define CHUNK_CELL_INTERVALS (1LL << 21)
+#define CHUNK_MAX_INTERVALS 64
 
 struct hsb_server {
   int workers = 1;
@@ -83,18 +97,50 @@ int hsb_server_set_priority(hsb_server *s, int model, int high) {
   return HSB_OK;
 }
 
-// one request, synchronously, on the calling thread
-static int run_request(hsb_server::Model &M, hsb_request *r) {
+// the pause of background requests while high-priority ones run
+struct Gate {
+  std::mutex *mu;
+  std::condition_variable *cv;
+  const int *high_running;
+};
+
+static void gate_wait(void *ctx) {
+  Gate *g = (Gate *)ctx;
+  std::unique_lock<std::mutex> lk(*g->mu);
+  while (*g->high_running > 0) g->cv->wait_for(lk, std::chrono::milliseconds(10));
+}
+
+// one request, synchronously, on the calling thread; gate: null, or the
+// pause a background request takes between chunks and refinement passes
+static int run_request(hsb_server::Model &M, hsb_request *r, Gate *gate) {
   hsb_dev_model *m = M.m;
   const size_t nb = (size_t)m->total_n_blocks + m->nx;
   hsb_stats st;
   memset(&st, 0, sizeof(st));
   if (cudaSetDevice(m->device) != cudaSuccess) return set_error(HSB_E_CUDA, "cudaSetDevice");
-  if (r->kind == HSB_REQ_STEADY) return hsb_dev_steady(m, r->power, r->out, &M.opts, &st);
+  if (r->kind == HSB_REQ_STEADY) {
+    m->yield_fn = gate ? gate_wait : nullptr;
+    m->yield_ctx = gate;
+    const int rc = hsb_dev_steady(m, r->power, r->out, &M.opts, &st);
+    m->yield_fn = nullptr;
+    m->yield_ctx = nullptr;
+    return rc;
+  }
   if (r->kind != HSB_REQ_TRANSIENT || r->steps < 1) return set_error(HSB_E_ARG, "bad request kind or step count");
-  (void)nb;
-  // all intervals of the request in one call (one persistent launch in the fast form)
-  return hsb_dev_transient_trace(m, r->power, r->steps, r->temp_in, r->dt, r->out, &M.opts, &st);
+  if (!gate)   // all intervals in one call (one persistent launch in the fast form)
+    return hsb_dev_transient_trace(m, r->power, r->steps, r->temp_in, r->dt, r->out, &M.opts, &st);
+  long long K = CHUNK_CELL_INTERVALS / (m->ncell > 0 ? m->ncell : 1);
+  if (K < 1) K = 1;
+  if (K > CHUNK_MAX_INTERVALS) K = CHUNK_MAX_INTERVALS;
+  for (int k0 = 0; k0 < r->steps; k0 += (int)K) {
+    const int k = (int)std::min<long long>(K, r->steps - k0);
+    const bool last = k0 + k >= r->steps;
+    const int rc = hsb_dev_transient_trace(m, r->power + (size_t)k0 * nb, k, k0 == 0 ? r->temp_in : nullptr, r->dt,
+                                           last ? r->out : nullptr, &M.opts, &st);
+    if (rc) return rc;
+    if (!last) gate_wait(gate);
+  }
+  return HSB_OK;
 }
 
 int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
@@ -105,7 +151,10 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
   std::mutex mu;
   std::condition_variable cv;
   std::vector<int> state(n, 0);   // 0 pending, 1 running, 2 done
-  int done = 0, running = 0;
+  int done = 0, running = 0, running_high = 0, running_low = 0;
+  bool any_high = false;   // a high-priority request is in this run
+  for (int k = 0; k < n; k++) any_high = any_high || s->models[reqs[k].model].high;
+  Gate gate{&mu, &cv, &running_high};
   std::string first_error;        // message of the first failed request
   using clk = std::chrono::steady_clock;
   const auto t0 = clk::now();
@@ -132,6 +181,7 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
         }
         hsb_server::Model &M = s->models[r.model];
         if (M.busy) continue;
+        if (!M.high && running_low >= s->workers) continue;   // the other threads are kept for high priority
         if (!M.warm) {   // first use: admission by free device memory
           if (!mem_known) {
             cudaSetDevice(M.m->device);
@@ -177,12 +227,15 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
       hsb_server::Model &M = s->models[r.model];
       state[best] = 1;
       running++;
+      const bool high = M.high != 0;
+      (high ? running_high : running_low)++;
       M.busy = true;
       r.start = t;
       r.worker = wid;
       lk.unlock();
-      const int rc = run_request(M, &r);
+      const int rc = run_request(M, &r, (any_high && !high) ? &gate : nullptr);
       lk.lock();
+      (high ? running_high : running_low)--;
       r.finish = now();
       r.status = rc;
       if (rc != HSB_OK && first_error.empty()) first_error = hsb_dev_last_error();
@@ -195,7 +248,8 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
     }
   };
   std::vector<std::thread> pool;
-  for (int w = 0; w < s->workers; w++) pool.emplace_back(worker, w);
+  const int threads = s->workers + (any_high ? HIGH_SLOTS : 0);
+  for (int w = 0; w < threads; w++) pool.emplace_back(worker, w);
   for (auto &th : pool) th.join();
   int failed = 0;
   for (int k = 0; k < n; k++)

@@ -1229,6 +1229,7 @@ int bicgstab_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
     st->cycles += BC_INNER;
     if (!(emax == emax)) return set_error(HSB_E_NOCONV, "BiCGStab steady solve broke down (NaN correction)");
     if (emax < tol) break;
+    if (m->yield_fn) m->yield_fn(m->yield_ctx);
   }
   // final FP64 residual for the record
   HSB_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), m->stream));

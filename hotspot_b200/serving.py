@@ -122,7 +122,7 @@ def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.
                 steady_frac: float = 0.7, transient_steps: int = 500, dt: float = 3.333e-6,
                 steady_sides=(64, 128, 256, 512, 1024), transient_sides=(64, 128, 256),
                 max_layers: int = 8, model_factory=None, high_priority_cells: int = 0,
-                reuse: Mix | None = None) -> Mix:
+                high_priority_classes=(), reuse: Mix | None = None) -> Mix:
     """Seeded Poisson arrivals at `rate` req/s for `duration` s.  Steady
     requests: side drawn log-uniformly from `steady_sides`, 1..max_layers
     chip layers; transients: `transient_steps` intervals of `dt` on
@@ -130,9 +130,10 @@ def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.
     registered on `server`; every request carries its own power map
     (U(0.5, 20) W per block, AR(1) over a transient) and transients their
     initial block temperatures, so results do not depend on history.
-    Steady classes of at most `high_priority_cells` cells get the high
-    priority class.  `reuse`: the resident models of an earlier mix on the
-    same server serve the classes they cover."""
+    Steady classes of at most `high_priority_cells` cells, and the steady
+    classes named in `high_priority_classes` as (side, chip layers), get the
+    high priority class.  `reuse`: the resident models of an earlier mix on
+    the same server serve the classes they cover."""
     from . import model as hm
     rng = np.random.default_rng(seed)
     mix = Mix(requests=[])
@@ -158,7 +159,7 @@ def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.
             mix.models.append(m)
             scen[key] = sc
             mix.classes[key] = server.add_model(m, FORM_FAST, 1e-5)
-            if steady and m.n_cells <= high_priority_cells:
+            if steady and (m.n_cells <= high_priority_cells or (side, layers) in set(high_priority_classes)):
                 server.set_priority(mix.classes[key], True)
         mi = mix.classes[key]
         m = server.models[mi]

@@ -26,9 +26,10 @@ def _requests(server, scs, models, rng, n, rate):
             reqs.append(Request(mi, _abi.REQ_STEADY, m.power_vector(rng.uniform(0.5, 20.0, nblk)), t,
                                 tag=f"steady{mi}"))
         else:
-            trace = W.ar1_power(rng, rng.uniform(0.5, 20.0, nblk), 12)
-            p = np.stack([m.power_vector(trace[s]) for s in range(12)])
-            reqs.append(Request(mi, _abi.REQ_TRANSIENT, p, t, temp_in=m.vector(m.config.init_temp), steps=12,
+            # 70 intervals: more than one launch chunk of a background transient
+            trace = W.ar1_power(rng, rng.uniform(0.5, 20.0, nblk), 70)
+            p = np.stack([m.power_vector(trace[s]) for s in range(70)])
+            reqs.append(Request(mi, _abi.REQ_TRANSIENT, p, t, temp_in=m.vector(m.config.init_temp), steps=70,
                                 dt=3.333e-6, tag="transient"))
     return reqs
 
@@ -42,7 +43,10 @@ def test_alone_equals_mixed(workdir):
     srv = Server(workers=4)
     for m in models:
         srv.add_model(m, _abi.FORM_FAST, 1e-6)
-    srv.set_priority(0, True)        # a high-priority class: its own stream priority, dispatched first
+    # a high-priority class: its own stream priority and workers, dispatched
+    # first; in the mixed run the other requests pause between chunks while it
+    # runs, alone (no high-priority request in the run) they run unchunked
+    srv.set_priority(0, True)
     mixed = _requests(srv, scs, models, np.random.default_rng(91), 24, 4000.0)
     # alone: the same requests one at a time
     alone = [Request(r.model, r.kind, r.power, 0.0, r.temp_in, r.steps, r.dt, r.tag) for r in mixed]
