@@ -719,11 +719,15 @@ int rk4_krylov_enqueue(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, c
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  // external records: under stream capture they become event-record nodes,
-  // so a replayed graph still times the kernel
-  HSB_CUDA(cudaEventRecordWithFlags(w->kev[0], m->stream, cudaEventRecordExternal));
+  // under stream capture the records are external ones, which become
+  // event-record nodes, so a replayed graph still times the kernel (the
+  // external flag is refused outside a capture)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  HSB_CUDA(cudaStreamIsCapturing(m->stream, &cap));
+  const unsigned rec = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+  HSB_CUDA(cudaEventRecordWithFlags(w->kev[0], m->stream, rec));
   HSB_CUDA(cudaLaunchKernelExC(&cfg, fn, args));
-  HSB_CUDA(cudaEventRecordWithFlags(w->kev[1], m->stream, cudaEventRecordExternal));
+  HSB_CUDA(cudaEventRecordWithFlags(w->kev[1], m->stream, rec));
   HSB_CUDA(cudaMemcpyAsync(w->h_cnt, w->cnt, sizeof(long long) * 8, cudaMemcpyDeviceToHost, m->stream));
   st->launches += 1;
   return HSB_OK;
