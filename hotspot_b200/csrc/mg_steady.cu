@@ -456,22 +456,21 @@ __global__ void mg_zero(float *x, long long n) {
 // ---------------------------------------------------------------------------
 // The coarse end of the V-cycle in one CTA.  Below some size every level
 // kernel is a few microseconds of launch and memory latency for very little
-// work; levels fuse .. nlev-1 (planes of at most 32 x 32 columns) instead run
-// here, with their x, f and r in shared memory, in exactly the order of the
+// work; levels fuse .. nlev-1 (planes of at most 16 x 16 columns) instead run
+// here, with their x, f, r and coefficients in shared memory, in the order of the
 // kernel-by-kernel cycle: zero x, two pre-smoothing sweeps (red z-lines,
 // black z-lines, package nodes), r = f - A x, restriction, the coarser
 // level, prolongation, two post-smoothing sweeps (package, black, red); the
-// coarsest level by its dense FP64 inverse.  Coefficients stay in global
-// memory (read-only, L1-resident after the first sweep).
+// coarsest level by its dense FP64 inverse (read from global memory).
 // ---------------------------------------------------------------------------
 #define MG_FUSE_MAXLEV 8
 #define MG_FUSE_THREADS 512
-#define MG_FUSE_SMEM (160 * 1024)
-#define MG_FUSE_PLANE 1024
+#define MG_FUSE_SMEM (200 * 1024)
+#define MG_FUSE_PLANE 256
 
 struct FusedArgs {
   MgLevelDev L[MG_FUSE_MAXLEV];
-  int off[MG_FUSE_MAXLEV];   // float offset of level k's x in shared memory; f, r follow (n_k each)
+  int off[MG_FUSE_MAXLEV];   // float offset of level k's block in shared memory (fused_block_floats)
   int nf;                    // fused levels; the last is the coarsest
   const PackSys *ps;
   const double *cinv;        // coarsest level inverse (cn x cn)
@@ -480,18 +479,61 @@ struct FusedArgs {
   float *x_out;              // its solution (global)
 };
 
+// a fused level's block of shared memory, in floats: x, f, r (n each), then
+// its coefficients gE, gS, gB, diag (ncell each), the package inverse
+// (NXP x NXP) and the per-layer ambient and edge conductances (3 x nl)
+__host__ __device__ inline long long fused_block_floats(long long ncell, int nl) {
+  const long long n = ncell + NXP;
+  return (3 * n + 4 * ncell + NXP * NXP + 3 * nl + 3) / 4 * 4;
+}
+
 template <int MAXL>
 __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_constant__ FusedArgs A) {
   extern __shared__ __align__(16) float smf[];
   __shared__ float esum[NXP], prhs[NXP];
+  __shared__ MgLevelDev SL[MG_FUSE_MAXLEV];   // the levels with their coefficients in shared memory
+  __shared__ PackSys sps;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int w = tid >> 5, lane = tid & 31, nw = nt >> 5;
-  const PackSys *ps = A.ps;
+  const PackSys *ps = &sps;
 
+  // stage every read-only table in shared memory: each phase below is then a
+  // few shared-memory round trips instead of global-memory ones
+  for (int q = tid; q < (int)(sizeof(PackSys) / 4); q += nt) ((int *)&sps)[q] = ((const int *)A.ps)[q];
+  for (int k = 0; k < A.nf; k++) {
+    const MgLevelDev &G = A.L[k];
+    const long long n = G.ncell + NXP, nc = G.ncell;
+    float *blk = smf + A.off[k];
+    float *gE = blk + 3 * n, *gS = gE + nc, *gB = gS + nc, *dg = gB + nc, *pinv = dg + nc;
+    float *amb = pinv + NXP * NXP, *ens = amb + G.nl, *eew = ens + G.nl;
+    for (long long q = tid; q < nc; q += nt) {
+      gE[q] = G.gE[q];
+      gS[q] = G.gS[q];
+      gB[q] = G.gB[q];
+      dg[q] = G.diag[q];
+    }
+    for (int q = tid; q < NXP * NXP; q += nt) pinv[q] = G.pinv[q];
+    for (int q = tid; q < G.nl; q += nt) {
+      amb[q] = G.gAmbL[q];
+      ens[q] = G.gEdgeNS[q];
+      eew[q] = G.gEdgeEW[q];
+    }
+    if (tid == 0) {
+      MgLevelDev L = G;
+      L.gE = gE; L.gS = gS; L.gB = gB; L.diag = dg; L.pinv = pinv;
+      L.gAmbL = amb; L.gEdgeNS = ens; L.gEdgeEW = eew;
+      SL[k] = L;
+    }
+  }
+  __syncthreads();
+
+  // the z-lines of one colour (non-coarsest levels have an even column count)
   auto zl = [&](const MgLevelDev &L, float *x, const float *f, int color) {
-    for (long long col = tid; col < L.plane; col += nt) {
-      const int i = (int)(col / L.nc), j = (int)(col - (long long)i * L.nc);
-      if (((i + j) & 1) == color) zline_colT<MAXL>(L, x, f, col);
+    const int half = L.nc >> 1;
+    for (long long k = tid; k < (L.plane >> 1); k += nt) {
+      const int i = (int)(k / half), jj = (int)(k - (long long)i * half);
+      const int j = 2 * jj + ((i + color) & 1);
+      zline_colT<MAXL>(L, x, f, (long long)i * L.nc + j);
     }
     __syncthreads();
   };
@@ -623,13 +665,13 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
 
   const int nf = A.nf;
   {
-    const long long n0 = A.L[0].ncell + NXP;
+    const long long n0 = SL[0].ncell + NXP;
     float *f0 = smf + A.off[0] + n0;
     for (long long q = tid; q < n0; q += nt) f0[q] = A.f_in[q];
   }
   __syncthreads();
   for (int k = 0; k < nf - 1; k++) {
-    const MgLevelDev &L = A.L[k];
+    const MgLevelDev &L = SL[k];
     const long long n = L.ncell + NXP;
     float *x = smf + A.off[k], *f = x + n, *r = f + n;
     for (long long q = tid; q < n; q += nt) x[q] = 0.f;
@@ -640,11 +682,11 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
       pk(L, x, f);
     }
     resid(L, x, f, r);
-    const MgLevelDev &C = A.L[k + 1];
+    const MgLevelDev &C = SL[k + 1];
     restrict_to(L, r, C, smf + A.off[k + 1] + (C.ncell + NXP));
   }
   {   // coarsest: x = A^-1 f, one warp per row
-    const MgLevelDev &C = A.L[nf - 1];
+    const MgLevelDev &C = SL[nf - 1];
     const long long n = C.ncell + NXP;
     float *x = smf + A.off[nf - 1], *f = x + n;
     for (int r = w; r < A.cn; r += nw) {
@@ -657,7 +699,7 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
     __syncthreads();
   }
   for (int k = nf - 2; k >= 0; k--) {
-    const MgLevelDev &L = A.L[k], &C = A.L[k + 1];
+    const MgLevelDev &L = SL[k], &C = SL[k + 1];
     const long long n = L.ncell + NXP;
     float *x = smf + A.off[k], *f = x + n;
     prolong(C, smf + A.off[k + 1], L, x);
@@ -668,7 +710,7 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
     }
   }
   {
-    const long long n0 = A.L[0].ncell + NXP;
+    const long long n0 = SL[0].ncell + NXP;
     const float *x0 = smf + A.off[0];
     for (long long q = tid; q < n0; q += nt) A.x_out[q] = x0[q];
   }
@@ -1226,15 +1268,15 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
   }
   // the coarse levels that fuse into one single-CTA kernel: from the first
   // level of at most MG_FUSE_PLANE columns whose levels down to the coarsest
-  // fit MG_FUSE_SMEM of shared memory (x, f, r each); needs the exact
-  // coarsest inverse and at most 16 layers
+  // fit MG_FUSE_SMEM of shared memory (vectors and coefficients); needs the
+  // exact coarsest inverse and at most 16 layers
   w->fuse = -1;
   w->fuse_smem = 0;
   if (w->cn > 0 && m->nl <= 16) {
     for (int l = 0; l < w->nlev; l++) {
       if (w->lv[l].plane > MG_FUSE_PLANE || w->nlev - l > MG_FUSE_MAXLEV) continue;
       size_t bytes = 0;
-      for (int k = l; k < w->nlev; k++) bytes += 3 * sizeof(float) * (size_t)(w->lv[k].ncell + NXP);
+      for (int k = l; k < w->nlev; k++) bytes += sizeof(float) * (size_t)fused_block_floats(w->lv[k].ncell, m->nl);
       if (bytes > MG_FUSE_SMEM) continue;
       const void *fn = m->nl <= 8 ? (const void *)mg_cycle_fused<8> : (const void *)mg_cycle_fused<16>;
       int rc;
@@ -1276,11 +1318,11 @@ static void vcycle(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f)
     FusedArgs A;
     memset(&A, 0, sizeof(A));
     A.nf = w->nlev - l;
-    int off = 0;
+    long long off = 0;
     for (int k = 0; k < A.nf; k++) {
       A.L[k] = dev_level(m, w->lv[l + k], l + k);
-      A.off[k] = off;
-      off += 3 * (int)(w->lv[l + k].ncell + NXP);
+      A.off[k] = (int)off;
+      off += fused_block_floats(w->lv[l + k].ncell, m->nl);
     }
     A.ps = w->d_ps;
     A.cinv = w->cinv;

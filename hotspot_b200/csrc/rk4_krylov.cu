@@ -124,6 +124,10 @@ struct KCtl {
 };
 
 // the attempt's polynomials (one thread): D = ytemp - y, F1 = f(t1), E = ytemp - t2
+// the h = 1 first-attempt coefficients (E1, D1, F11), once computed
+__device__ Coef g_first[3];
+__device__ int g_first_ready;
+
 __device__ __forceinline__ void plan_attempt(KShared &sh, double h, int dcomp) {
   kry_plan(sh.E, sh.D, sh.F1, sh.K, sh.ps, h, dcomp);
 }
@@ -475,17 +479,33 @@ __global__ void __launch_bounds__(FT_THREADS, 2) rk4_krylov_kernel(const __grid_
   kpower(A, 0);
   if (threadIdx.x < nx) sh.yp[threadIdx.x] = A.y[S.ncell + threadIdx.x];
   if (blockIdx.x == 0 && threadIdx.x == 0) { A.err[0] = 0ull; A.err[1] = 0ull; }
-  grid.sync();
-
-  // first-attempt coefficients for h = 1 (they scale with h)
+  // first-attempt coefficients for h = 1 (they scale with h); they depend on
+  // nothing but the method, so the first launch in the process computes them
+  // (one thread, tens of microseconds of FP64 scalar work) and later
+  // launches read them back
   if (threadIdx.x == 0) {
     for (int q = 0; q < PMAX; q++) sh.ps[q] = 1.0;
     c_one(sh.K);
-    plan_attempt(sh, 1.0, 0);
-    c_copy(sh.E1, sh.E);
-    c_copy(sh.D1, sh.D);
-    c_copy(sh.F11, sh.F1);
+    if (*(volatile int *)&g_first_ready) {
+      __threadfence();
+      c_copy(sh.E1, g_first[0]);
+      c_copy(sh.D1, g_first[1]);
+      c_copy(sh.F11, g_first[2]);
+    } else {
+      plan_attempt(sh, 1.0, 0);
+      c_copy(sh.E1, sh.E);
+      c_copy(sh.D1, sh.D);
+      c_copy(sh.F11, sh.F1);
+      if (blockIdx.x == 0) {
+        c_copy(g_first[0], sh.E1);
+        c_copy(g_first[1], sh.D1);
+        c_copy(g_first[2], sh.F11);
+        __threadfence();
+        atomicExch(&g_first_ready, 1);
+      }
+    }
   }
+  grid.sync();
   KCtl c;
   c.pkind = -1;
   c.sp = 0;
