@@ -86,6 +86,10 @@ struct MgWork {
   // (mg_cycle_fused); -1: every level kernel by kernel
   int fuse;
   size_t fuse_smem;
+  // the package step folded into z-line launches: per-CTA edge-sum shares
+  // and the ticket that finds the last CTA
+  float *pk_part;
+  unsigned *pk_ticket;
 };
 
 // ---------------------------------------------------------------------------
@@ -103,9 +107,18 @@ __device__ __forceinline__ int edge_node(int layer, int side, int spidx, int hsi
 // nearly singular (the overall temperature level is tied to ambient only
 // through weak convection), and diag*x - sum g*x_nbr would cancel most FP32
 // digits of smooth vectors
+__device__ void apply_pack_rows(const MgLevelDev &L, const PackSys *__restrict__ ps, const float *__restrict__ x,
+                                float *__restrict__ y, const float *__restrict__ f, int mode);
+
+// ps != null: the grid has one more CTA, which applies the package rows
+// (mg_apply_pack's work, in the same launch)
 __global__ void mg_apply_cells(MgLevelDev L, const float *__restrict__ x, float *__restrict__ y,
-                               const float *__restrict__ f, int mode) {
+                               const float *__restrict__ f, int mode, const PackSys *__restrict__ ps) {
   // mode 0: y = A x ; mode 1: y = f - A x
+  if (ps && blockIdx.x == gridDim.x - 1) {
+    apply_pack_rows(L, ps, x, y, f, mode);
+    return;
+  }
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.ncell) return;
   const int n = (int)(c / L.plane);
@@ -133,6 +146,11 @@ __global__ void mg_apply_cells(MgLevelDev L, const float *__restrict__ x, float 
 // gamb x_k + sum link (x_k - x_o)
 __global__ void mg_apply_pack(MgLevelDev L, const PackSys *__restrict__ ps, const float *__restrict__ x,
                               float *__restrict__ y, const float *__restrict__ f, int mode) {
+  apply_pack_rows(L, ps, x, y, f, mode);
+}
+
+__device__ void apply_pack_rows(const MgLevelDev &L, const PackSys *__restrict__ ps, const float *__restrict__ x,
+                                float *__restrict__ y, const float *__restrict__ f, int mode) {
   __shared__ float esum[NXP];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const float *xp = x + L.ncell;
@@ -206,25 +224,33 @@ __device__ __forceinline__ void zline_col(const MgLevelDev &L, float *__restrict
 // costs one memory round trip instead of one per layer.  x and f may be
 // global or shared memory.
 template <int MAXL>
-__device__ __forceinline__ void zline_colT(const MgLevelDev &L, float *x, const float *f, long long col) {
-  const int i = (int)(col / L.nc), j = (int)(col - (long long)i * L.nc);
+__device__ __forceinline__ void zline_colT(const MgLevelDev &L, float *x, const float *f, int col) {
+  const int nc = L.nc, nr = L.nr;
+  const int i = col / nc, j = col - i * nc;
   const int nl = L.nl;
   const float *xp = x + L.ncell;
+  // neighbour columns clamped to this one at the boundary, where the face
+  // conductance is zero: every load is unconditional and can be in flight
+  // at once; a zero weight adds exactly nothing
+  const int dE = j < nc - 1 ? 1 : 0, dW = j > 0 ? 1 : 0;
+  const int dS = i < nr - 1 ? nc : 0, dN = i > 0 ? nc : 0;
   float rhs[MAXL], gb[MAXL], bd[MAXL];
 #pragma unroll
   for (int n = 0; n < MAXL; n++) {
     if (n < nl) {
       const long long c = (long long)n * L.plane + col;
+      const float wE = dE ? L.gE[c] : 0.f, wW = dW ? L.gE[c - dW] : 0.f;
+      const float wS = dS ? L.gS[c] : 0.f, wN = dN ? L.gS[c - dN] : 0.f;
       float r = f[c];
-      if (j < L.nc - 1) r += L.gE[c] * x[c + 1];
-      if (j > 0) r += L.gE[c - 1] * x[c - 1];
-      if (i < L.nr - 1) r += L.gS[c] * x[c + L.nc];
-      if (i > 0) r += L.gS[c - L.nc] * x[c - L.nc];
+      r += wE * x[c + dE];
+      r += wW * x[c - dW];
+      r += wS * x[c + dS];
+      r += wN * x[c - dN];
       if (n == L.spidx || n == L.hsidx) {
         if (i == 0) r += L.gEdgeNS[n] * xp[edge_node(n, 0, L.spidx, L.hsidx)];
-        if (i == L.nr - 1) r += L.gEdgeNS[n] * xp[edge_node(n, 1, L.spidx, L.hsidx)];
+        if (i == nr - 1) r += L.gEdgeNS[n] * xp[edge_node(n, 1, L.spidx, L.hsidx)];
         if (j == 0) r += L.gEdgeEW[n] * xp[edge_node(n, 2, L.spidx, L.hsidx)];
-        if (j == L.nc - 1) r += L.gEdgeEW[n] * xp[edge_node(n, 3, L.spidx, L.hsidx)];
+        if (j == nc - 1) r += L.gEdgeEW[n] * xp[edge_node(n, 3, L.spidx, L.hsidx)];
       }
       rhs[n] = r;
       gb[n] = n < nl - 1 ? L.gB[c] : 0.f;
@@ -257,13 +283,68 @@ __device__ __forceinline__ void zline_colT(const MgLevelDev &L, float *x, const 
   }
 }
 
-template <int MAXL>
-__global__ void mg_zline_t(MgLevelDev L, float *__restrict__ x, const float *__restrict__ f, int color) {
-  long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= L.plane) return;
-  const int i = (int)(col / L.nc), j = (int)(col - (long long)i * L.nc);
-  if (((i + j) & 1) != color) return;
-  zline_colT<MAXL>(L, x, f, col);
+// One colour of z-lines.  PK: the package nodes are solved at the end of
+// the same launch (the smoother's package step, mg_pack_solve's work): every
+// CTA writes its share of the 12 edge sums, and the last CTA to finish --
+// found by a ticket counter, no waiting -- adds the shares in CTA order and
+// applies the package inverse.  Columns are < 2^31 (checked at set-up).
+template <int MAXL, bool PK>
+__global__ void __launch_bounds__(MGT) mg_zline_t(MgLevelDev L, float *__restrict__ x, const float *__restrict__ f,
+                                                  int color, const PackSys *__restrict__ ps, float *__restrict__ part,
+                                                  unsigned *__restrict__ ticket) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in = col < L.plane;
+  int i = 0, j = 0;
+  if (in) {
+    i = col / L.nc;
+    j = col - i * L.nc;
+    if (((i + j) & 1) == color) zline_colT<MAXL>(L, x, f, col);
+  }
+  if (!PK) return;
+  __shared__ float red[MGT / 32][NXP];
+  __shared__ float esum[NXP], prhs[NXP];
+  __shared__ int last;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  // this CTA's share of the edge sums: each thread its own column (which it
+  // just wrote, or the previous half sweep did)
+  for (int k = 0; k < NXP; k++) {
+    const int layer = ps->elayer[k], side = ps->eside[k];
+    float v = 0.f;
+    if (in && layer >= 0) {
+      const bool on = side == 0 ? i == 0 : side == 1 ? i == L.nr - 1 : side == 2 ? j == 0 : j == L.nc - 1;
+      if (on) v = x[(long long)layer * L.plane + col];
+    }
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[w][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NXP) {
+    float sm = 0.f;
+    for (int q = 0; q < nw; q++) sm += red[q][threadIdx.x];
+    part[(long long)blockIdx.x * NXP + threadIdx.x] = sm;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int k = w; k < NXP; k += nw) {
+    float sm = 0.f;
+    for (int b = lane; b < (int)gridDim.x; b += 32) sm += __ldcg(part + (long long)b * NXP + k);
+    for (int o = 16; o > 0; o >>= 1) sm += __shfl_down_sync(0xffffffffu, sm, o);
+    if (lane == 0) esum[k] = sm;
+  }
+  __syncthreads();
+  if (threadIdx.x < NXP) prhs[threadIdx.x] = f[L.ncell + threadIdx.x] + ps->ge0[threadIdx.x] * L.scale * esum[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x < NXP) {
+    float v = 0.f;
+#pragma unroll
+    for (int o = 0; o < NXP; o++) v += L.pinv[threadIdx.x * NXP + o] * prhs[o];
+    x[L.ncell + threadIdx.x] = v;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
 }
 
 // red-black z-line Gauss-Seidel half sweep on level L: solve A x = f
@@ -529,11 +610,11 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
 
   // the z-lines of one colour (non-coarsest levels have an even column count)
   auto zl = [&](const MgLevelDev &L, float *x, const float *f, int color) {
-    const int half = L.nc >> 1;
-    for (long long k = tid; k < (L.plane >> 1); k += nt) {
-      const int i = (int)(k / half), jj = (int)(k - (long long)i * half);
+    const int half = L.nc >> 1, ncol = (int)(L.plane >> 1);
+    for (int k = tid; k < ncol; k += nt) {
+      const int i = k / half, jj = k - i * half;
       const int j = 2 * jj + ((i + color) & 1);
-      zline_colT<MAXL>(L, x, f, (long long)i * L.nc + j);
+      zline_colT<MAXL>(L, x, f, i * L.nc + j);
     }
     __syncthreads();
   };
@@ -566,10 +647,11 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
   // r = f - A x (mg_apply_cells and mg_apply_pack, mode 1)
   auto resid = [&](const MgLevelDev &L, const float *x, const float *f, float *r) {
     const float *xp = x + L.ncell;
-    for (long long c = tid; c < L.ncell; c += nt) {
-      const int n = (int)(c / L.plane);
-      const long long q = c - n * L.plane;
-      const int i = (int)(q / L.nc), j = (int)(q - (long long)i * L.nc);
+    const int plane = (int)L.plane, ncl = (int)L.ncell;
+    for (int c = tid; c < ncl; c += nt) {
+      const int n = c / plane;
+      const int q = c - n * plane;
+      const int i = q / L.nc, j = q - i * L.nc;
       const float xc = x[c];
       float s = L.gAmbL[n] * xc;
       if (j < L.nc - 1) s += L.gE[c] * (xc - x[c + 1]);
@@ -613,12 +695,12 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
   // coarse f = P^T r (mg_restrict_f)
   auto restrict_to = [&](const MgLevelDev &F, const float *rf, const MgLevelDev &C, float *fc) {
     const int cnr = C.nr, cnc = C.nc, fnr = F.nr, fnc = F.nc;
-    const long long cpl = C.plane, fpl = F.plane;
-    for (long long t = tid; t < C.ncell + NXP; t += nt) {
-      if (t < C.ncell) {
-        const int n = (int)(t / cpl);
-        const long long q = t - n * cpl;
-        const int i = (int)(q / cnc), j = (int)(q - (long long)i * cnc);
+    const int cpl = (int)C.plane, fpl = (int)F.plane, cncell = (int)C.ncell;
+    for (int t = tid; t < cncell + NXP; t += nt) {
+      if (t < cncell) {
+        const int n = t / cpl;
+        const int q = t - n * cpl;
+        const int i = q / cnc, j = q - i * cnc;
         const float *src = rf + n * fpl;
         float acc = 0.f;
         for (int fi = 2 * i - 1; fi <= 2 * i + 2; fi++) {
@@ -635,7 +717,7 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
         }
         fc[t] = acc;
       } else {
-        fc[t] = rf[F.ncell + (t - C.ncell)];
+        fc[t] = rf[F.ncell + (t - cncell)];
       }
     }
     __syncthreads();
@@ -643,12 +725,12 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
   // fine x += P xc (mg_prolong_add)
   auto prolong = [&](const MgLevelDev &C, const float *xc, const MgLevelDev &F, float *xf) {
     const int cnr = C.nr, cnc = C.nc, fnc = F.nc;
-    const long long cpl = C.plane, fpl = F.plane;
-    for (long long t = tid; t < F.ncell + NXP; t += nt) {
-      if (t < F.ncell) {
-        const int n = (int)(t / fpl);
-        const long long q = t - n * fpl;
-        const int fi = (int)(q / fnc), fj = (int)(q - (long long)fi * fnc);
+    const int cpl = (int)C.plane, fpl = (int)F.plane, fncell = (int)F.ncell;
+    for (int t = tid; t < fncell + NXP; t += nt) {
+      if (t < fncell) {
+        const int n = t / fpl;
+        const int q = t - n * fpl;
+        const int fi = q / fnc, fj = q - fi * fnc;
         const int ci = fi >> 1, cj = fj >> 1;
         int ci2 = ci + ((fi & 1) ? 1 : -1), cj2 = cj + ((fj & 1) ? 1 : -1);
         ci2 = ci2 < 0 ? 0 : ci2 >= cnr ? cnr - 1 : ci2;
@@ -657,7 +739,7 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
         xf[t] += 0.5625f * c[(long long)ci * cnc + cj] + 0.1875f * c[(long long)ci2 * cnc + cj] +
                  0.1875f * c[(long long)ci * cnc + cj2] + 0.0625f * c[(long long)ci2 * cnc + cj2];
       } else {
-        xf[t] += xc[C.ncell + (t - F.ncell)];
+        xf[t] += xc[C.ncell + (t - fncell)];
       }
     }
     __syncthreads();
@@ -1029,6 +1111,10 @@ static int mg_setup(hsb_dev_model *m, MgWork **out) {
   HSB_CUDA(cudaMalloc(&w->rr, sizeof(float) * n0));
   HSB_CUDA(cudaMalloc(&w->red, sizeof(double) * 4096));
   HSB_CUDA(cudaMalloc(&w->d_ps, sizeof(PackSys)));
+  if (w->lv[0].plane >= (1LL << 31) - MGT) return set_error(HSB_E_ARG, "multigrid: more than 2^31 columns per layer");
+  HSB_CUDA(cudaMalloc(&w->pk_part, sizeof(float) * NXP * nb(w->lv[0].plane)));
+  HSB_CUDA(cudaMalloc(&w->pk_ticket, sizeof(unsigned)));
+  HSB_CUDA(cudaMemset(w->pk_ticket, 0, sizeof(unsigned)));
   HSB_CUDA(cudaMallocHost(&w->h_red, sizeof(double) * 8));
   *out = w;
   return HSB_OK;
@@ -1043,7 +1129,7 @@ static void free_mg(void *p) {
       if (q) cudaFree(q);
   }
   void *b2[] = {w->gE64, w->gS64, w->gB64, w->gAmb64, w->gEdgeNS64, w->gEdgeEW64, w->r64, w->b64,
-                w->p, w->q, w->z, w->e, w->rr, w->red, w->d_ps, w->cinv};
+                w->p, w->q, w->z, w->e, w->rr, w->red, w->d_ps, w->cinv, w->pk_part, w->pk_ticket};
   for (void *q : b2)
     if (q) cudaFree(q);
   if (w->h_red) cudaFreeHost(w->h_red);
@@ -1289,24 +1375,36 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
   return HSB_OK;
 }
 
-static void zline(hsb_dev_model *m, const MgLevel &L, const MgLevelDev &d, float *x, const float *f, int color) {
-  if (m->nl <= 8) mg_zline_t<8><<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, color);
-  else if (m->nl <= 16) mg_zline_t<16><<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, color);
-  else mg_zline<<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, color);
+// one colour of z-lines; pk: followed by the package step (in the same
+// launch where the layer count allows, else as its own kernel)
+static void zline(hsb_dev_model *m, MgWork *w, const MgLevel &L, const MgLevelDev &d, float *x, const float *f,
+                  int color, bool pk) {
+  const unsigned g = nb(L.plane);
+  if (m->nl <= 8) {
+    if (pk) mg_zline_t<8, true><<<g, MGT, 0, m->stream>>>(d, x, f, color, w->d_ps, w->pk_part, w->pk_ticket);
+    else mg_zline_t<8, false><<<g, MGT, 0, m->stream>>>(d, x, f, color, nullptr, nullptr, nullptr);
+  } else if (m->nl <= 16) {
+    if (pk) mg_zline_t<16, true><<<g, MGT, 0, m->stream>>>(d, x, f, color, w->d_ps, w->pk_part, w->pk_ticket);
+    else mg_zline_t<16, false><<<g, MGT, 0, m->stream>>>(d, x, f, color, nullptr, nullptr, nullptr);
+  } else {
+    mg_zline<<<g, MGT, 0, m->stream>>>(d, x, f, color);
+    if (pk) mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
+  }
 }
 
 static void smooth(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f, int pre, int sweeps) {
   const MgLevel &L = w->lv[l];
   const MgLevelDev d = dev_level(m, L, l);
   for (int s = 0; s < sweeps; s++) {
+    // a sweep is red, black, package (pre) or package, black, red (post);
+    // a package step that follows a z-line launch runs inside it
     if (pre) {
-      zline(m, L, d, x, f, 0);
-      zline(m, L, d, x, f, 1);
-      mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
+      zline(m, w, L, d, x, f, 0, false);
+      zline(m, w, L, d, x, f, 1, true);
     } else {
-      mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
-      zline(m, L, d, x, f, 1);
-      zline(m, L, d, x, f, 0);
+      if (s == 0) mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
+      zline(m, w, L, d, x, f, 1, false);
+      zline(m, w, L, d, x, f, 0, s + 1 < sweeps);
     }
   }
 }
@@ -1341,8 +1439,7 @@ static void vcycle(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f)
   }
   const MgLevelDev d = dev_level(m, L, l);
   smooth(m, w, l, x, f, 1, 2);
-  mg_apply_cells<<<nb(L.ncell), MGT, 0, m->stream>>>(d, x, L.r, f, 1);
-  mg_apply_pack<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, L.r, f, 1);
+  mg_apply_cells<<<nb(L.ncell) + 1, MGT, 0, m->stream>>>(d, x, L.r, f, 1, w->d_ps);
   MgLevel &C = w->lv[l + 1];
   mg_restrict_f<<<nb(C.n), MGT, 0, m->stream>>>(L.r, C.f, m->nl, C.nr, C.nc, m->nx);
   vcycle(m, w, l + 1, C.x, C.f);
@@ -1400,8 +1497,7 @@ int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
       dot(m, w, w->rr, w->z, n0, sc + 2);
       pcg_update_p<<<nb(n0), MGT, 0, m->stream>>>(w->p, w->z, sc, n0, it == 0);
       shift_scalars<<<1, 1, 0, m->stream>>>(sc);
-      mg_apply_cells<<<nb(L0.ncell), MGT, 0, m->stream>>>(d0, w->p, w->q, nullptr, 0);
-      mg_apply_pack<<<1, 384, 0, m->stream>>>(d0, w->d_ps, w->p, w->q, nullptr, 0);
+      mg_apply_cells<<<nb(L0.ncell) + 1, MGT, 0, m->stream>>>(d0, w->p, w->q, nullptr, 0, w->d_ps);
       dot(m, w, w->p, w->q, n0, sc + 1);
       pcg_update_xr<<<nb(n0), MGT, 0, m->stream>>>(w->e, w->rr, w->p, w->q, sc, n0);
     }
