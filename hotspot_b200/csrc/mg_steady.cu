@@ -30,6 +30,9 @@ namespace hsb {
 
 #define MGT 256
 #define NXP 12
+#ifndef MG_SWEEPS
+#define MG_SWEEPS 2  // smoothing sweeps before and after each coarse-grid correction
+#endif
 #ifndef MG_INNER
 #define MG_INNER 4   // PCG iterations per FP64 refinement pass
 #endif
@@ -86,10 +89,6 @@ struct MgWork {
   // (mg_cycle_fused); -1: every level kernel by kernel
   int fuse;
   size_t fuse_smem;
-  // the package step folded into z-line launches: per-CTA edge-sum shares
-  // and the ticket that finds the last CTA
-  float *pk_part;
-  unsigned *pk_ticket;
 };
 
 // ---------------------------------------------------------------------------
@@ -223,11 +222,11 @@ __device__ __forceinline__ void zline_col(const MgLevelDev &L, float *__restrict
 // before the elimination starts (the arrays live in registers), so a column
 // costs one memory round trip instead of one per layer.  x and f may be
 // global or shared memory.
-template <int MAXL>
+template <int MAXL, bool EXACT = false>
 __device__ __forceinline__ void zline_colT(const MgLevelDev &L, float *x, const float *f, int col) {
   const int nc = L.nc, nr = L.nr;
   const int i = col / nc, j = col - i * nc;
-  const int nl = L.nl;
+  const int nl = EXACT ? MAXL : L.nl;   // EXACT: the layer count is MAXL, every layer test is static
   const float *xp = x + L.ncell;
   // neighbour columns clamped to this one at the boundary, where the face
   // conductance is zero: every load is unconditional and can be in flight
@@ -283,68 +282,15 @@ __device__ __forceinline__ void zline_colT(const MgLevelDev &L, float *x, const 
   }
 }
 
-// One colour of z-lines.  PK: the package nodes are solved at the end of
-// the same launch (the smoother's package step, mg_pack_solve's work): every
-// CTA writes its share of the 12 edge sums, and the last CTA to finish --
-// found by a ticket counter, no waiting -- adds the shares in CTA order and
-// applies the package inverse.  Columns are < 2^31 (checked at set-up).
-template <int MAXL, bool PK>
+// one colour of z-lines for models of exactly NL layers (columns < 2^31,
+// checked at set-up)
+template <int NL>
 __global__ void __launch_bounds__(MGT) mg_zline_t(MgLevelDev L, float *__restrict__ x, const float *__restrict__ f,
-                                                  int color, const PackSys *__restrict__ ps, float *__restrict__ part,
-                                                  unsigned *__restrict__ ticket) {
+                                                  int color) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool in = col < L.plane;
-  int i = 0, j = 0;
-  if (in) {
-    i = col / L.nc;
-    j = col - i * L.nc;
-    if (((i + j) & 1) == color) zline_colT<MAXL>(L, x, f, col);
-  }
-  if (!PK) return;
-  __shared__ float red[MGT / 32][NXP];
-  __shared__ float esum[NXP], prhs[NXP];
-  __shared__ int last;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  // this CTA's share of the edge sums: each thread its own column (which it
-  // just wrote, or the previous half sweep did)
-  for (int k = 0; k < NXP; k++) {
-    const int layer = ps->elayer[k], side = ps->eside[k];
-    float v = 0.f;
-    if (in && layer >= 0) {
-      const bool on = side == 0 ? i == 0 : side == 1 ? i == L.nr - 1 : side == 2 ? j == 0 : j == L.nc - 1;
-      if (on) v = x[(long long)layer * L.plane + col];
-    }
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) red[w][k] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x < NXP) {
-    float sm = 0.f;
-    for (int q = 0; q < nw; q++) sm += red[q][threadIdx.x];
-    part[(long long)blockIdx.x * NXP + threadIdx.x] = sm;
-  }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  for (int k = w; k < NXP; k += nw) {
-    float sm = 0.f;
-    for (int b = lane; b < (int)gridDim.x; b += 32) sm += __ldcg(part + (long long)b * NXP + k);
-    for (int o = 16; o > 0; o >>= 1) sm += __shfl_down_sync(0xffffffffu, sm, o);
-    if (lane == 0) esum[k] = sm;
-  }
-  __syncthreads();
-  if (threadIdx.x < NXP) prhs[threadIdx.x] = f[L.ncell + threadIdx.x] + ps->ge0[threadIdx.x] * L.scale * esum[threadIdx.x];
-  __syncthreads();
-  if (threadIdx.x < NXP) {
-    float v = 0.f;
-#pragma unroll
-    for (int o = 0; o < NXP; o++) v += L.pinv[threadIdx.x * NXP + o] * prhs[o];
-    x[L.ncell + threadIdx.x] = v;
-  }
-  if (threadIdx.x == 0) *ticket = 0u;
+  if (col >= L.plane) return;
+  const int i = col / L.nc, j = col - i * L.nc;
+  if (((i + j) & 1) == color) zline_colT<NL, true>(L, x, f, col);
 }
 
 // red-black z-line Gauss-Seidel half sweep on level L: solve A x = f
@@ -445,19 +391,35 @@ __global__ void __launch_bounds__(1024) mg_coarse_solve(MgLevelDev L, const Pack
 // exact solve of the coarsest level, x = A^-1 f, with its dense FP64 inverse
 // (one CTA; the level has at most MG_COARSE_MAX unknowns)
 #define MG_COARSE_MAX 2048
+// x = inv f for the rows of warp w: four rows at a time, so that each lane
+// has the loads of four rows in flight; per row the lane-strided partial
+// sums and the shuffle tree are those of a one-row-per-warp loop
+template <typename FV>
+__device__ __forceinline__ void coarse_rows(const double *__restrict__ inv, int n, const FV *fv, float *x, int w,
+                                            int nw, int lane) {
+  for (int r0 = 4 * w; r0 < n; r0 += 4 * nw) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int c = lane; c < n; c += 32) {
+      const double v = (double)fv[c];
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (r0 + q < n) acc[q] += inv[(long long)(r0 + q) * n + c] * v;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      double sacc = acc[q];
+      for (int o = 16; o > 0; o >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, o);
+      if (lane == 0 && r0 + q < n) x[r0 + q] = (float)sacc;
+    }
+  }
+}
 __global__ void __launch_bounds__(1024) mg_coarse_direct(const double *__restrict__ inv, int n,
                                                          float *__restrict__ x, const float *__restrict__ f) {
   __shared__ double fs[MG_COARSE_MAX];
   for (int k = threadIdx.x; k < n; k += blockDim.x) fs[k] = (double)f[k];
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int r = w; r < n; r += nw) {   // one warp per row, coalesced along the row
-    double s = 0.0;
-    const double *row = inv + (long long)r * n;
-    for (int c = lane; c < n; c += 32) s += row[c] * fs[c];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) x[r] = (float)s;
-  }
+  coarse_rows(inv, n, fs, x, w, nw, lane);
 }
 
 // Transfers: cell-centred bilinear prolongation (each fine cell takes 9/16 of
@@ -539,9 +501,9 @@ __global__ void mg_zero(float *x, long long n) {
 // kernel is a few microseconds of launch and memory latency for very little
 // work; levels fuse .. nlev-1 (planes of at most 16 x 16 columns) instead run
 // here, with their x, f, r and coefficients in shared memory, in the order of the
-// kernel-by-kernel cycle: zero x, two pre-smoothing sweeps (red z-lines,
+// kernel-by-kernel cycle: zero x, MG_SWEEPS pre-smoothing sweeps (red z-lines,
 // black z-lines, package nodes), r = f - A x, restriction, the coarser
-// level, prolongation, two post-smoothing sweeps (package, black, red); the
+// level, prolongation, MG_SWEEPS post-smoothing sweeps (package, black, red); the
 // coarsest level by its dense FP64 inverse (read from global memory).
 // ---------------------------------------------------------------------------
 #define MG_FUSE_MAXLEV 8
@@ -758,7 +720,7 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
     float *x = smf + A.off[k], *f = x + n, *r = f + n;
     for (long long q = tid; q < n; q += nt) x[q] = 0.f;
     __syncthreads();
-    for (int sw = 0; sw < 2; sw++) {
+    for (int sw = 0; sw < MG_SWEEPS; sw++) {
       zl(L, x, f, 0);
       zl(L, x, f, 1);
       pk(L, x, f);
@@ -771,13 +733,7 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
     const MgLevelDev &C = SL[nf - 1];
     const long long n = C.ncell + NXP;
     float *x = smf + A.off[nf - 1], *f = x + n;
-    for (int r = w; r < A.cn; r += nw) {
-      double sacc = 0.0;
-      const double *row = A.cinv + (long long)r * A.cn;
-      for (int c = lane; c < A.cn; c += 32) sacc += row[c] * (double)f[c];
-      for (int o = 16; o > 0; o >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, o);
-      if (lane == 0) x[r] = (float)sacc;
-    }
+    coarse_rows(A.cinv, A.cn, f, x, w, nw, lane);
     __syncthreads();
   }
   for (int k = nf - 2; k >= 0; k--) {
@@ -785,7 +741,7 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
     const long long n = L.ncell + NXP;
     float *x = smf + A.off[k], *f = x + n;
     prolong(C, smf + A.off[k + 1], L, x);
-    for (int sw = 0; sw < 2; sw++) {
+    for (int sw = 0; sw < MG_SWEEPS; sw++) {
       pk(L, x, f);
       zl(L, x, f, 1);
       zl(L, x, f, 0);
@@ -1112,9 +1068,7 @@ static int mg_setup(hsb_dev_model *m, MgWork **out) {
   HSB_CUDA(cudaMalloc(&w->red, sizeof(double) * 4096));
   HSB_CUDA(cudaMalloc(&w->d_ps, sizeof(PackSys)));
   if (w->lv[0].plane >= (1LL << 31) - MGT) return set_error(HSB_E_ARG, "multigrid: more than 2^31 columns per layer");
-  HSB_CUDA(cudaMalloc(&w->pk_part, sizeof(float) * NXP * nb(w->lv[0].plane)));
-  HSB_CUDA(cudaMalloc(&w->pk_ticket, sizeof(unsigned)));
-  HSB_CUDA(cudaMemset(w->pk_ticket, 0, sizeof(unsigned)));
+
   HSB_CUDA(cudaMallocHost(&w->h_red, sizeof(double) * 8));
   *out = w;
   return HSB_OK;
@@ -1129,7 +1083,7 @@ static void free_mg(void *p) {
       if (q) cudaFree(q);
   }
   void *b2[] = {w->gE64, w->gS64, w->gB64, w->gAmb64, w->gEdgeNS64, w->gEdgeEW64, w->r64, w->b64,
-                w->p, w->q, w->z, w->e, w->rr, w->red, w->d_ps, w->cinv, w->pk_part, w->pk_ticket};
+                w->p, w->q, w->z, w->e, w->rr, w->red, w->d_ps, w->cinv};
   for (void *q : b2)
     if (q) cudaFree(q);
   if (w->h_red) cudaFreeHost(w->h_red);
@@ -1375,20 +1329,32 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
   return HSB_OK;
 }
 
-// one colour of z-lines; pk: followed by the package step (in the same
-// launch where the layer count allows, else as its own kernel)
-static void zline(hsb_dev_model *m, MgWork *w, const MgLevel &L, const MgLevelDev &d, float *x, const float *f,
-                  int color, bool pk) {
-  const unsigned g = nb(L.plane);
-  if (m->nl <= 8) {
-    if (pk) mg_zline_t<8, true><<<g, MGT, 0, m->stream>>>(d, x, f, color, w->d_ps, w->pk_part, w->pk_ticket);
-    else mg_zline_t<8, false><<<g, MGT, 0, m->stream>>>(d, x, f, color, nullptr, nullptr, nullptr);
-  } else if (m->nl <= 16) {
-    if (pk) mg_zline_t<16, true><<<g, MGT, 0, m->stream>>>(d, x, f, color, w->d_ps, w->pk_part, w->pk_ticket);
-    else mg_zline_t<16, false><<<g, MGT, 0, m->stream>>>(d, x, f, color, nullptr, nullptr, nullptr);
-  } else {
-    mg_zline<<<g, MGT, 0, m->stream>>>(d, x, f, color);
-    if (pk) mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
+template <int NL>
+static void zline_n(hsb_dev_model *m, const MgLevel &L, const MgLevelDev &d, float *x, const float *f, int color) {
+  mg_zline_t<NL><<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, color);
+}
+
+// one colour of z-lines: the kernel compiled for the model's layer count
+// (up to 16), else the generic one
+static void zline(hsb_dev_model *m, const MgLevel &L, const MgLevelDev &d, float *x, const float *f, int color) {
+  switch (m->nl) {
+    case 1: zline_n<1>(m, L, d, x, f, color); break;
+    case 2: zline_n<2>(m, L, d, x, f, color); break;
+    case 3: zline_n<3>(m, L, d, x, f, color); break;
+    case 4: zline_n<4>(m, L, d, x, f, color); break;
+    case 5: zline_n<5>(m, L, d, x, f, color); break;
+    case 6: zline_n<6>(m, L, d, x, f, color); break;
+    case 7: zline_n<7>(m, L, d, x, f, color); break;
+    case 8: zline_n<8>(m, L, d, x, f, color); break;
+    case 9: zline_n<9>(m, L, d, x, f, color); break;
+    case 10: zline_n<10>(m, L, d, x, f, color); break;
+    case 11: zline_n<11>(m, L, d, x, f, color); break;
+    case 12: zline_n<12>(m, L, d, x, f, color); break;
+    case 13: zline_n<13>(m, L, d, x, f, color); break;
+    case 14: zline_n<14>(m, L, d, x, f, color); break;
+    case 15: zline_n<15>(m, L, d, x, f, color); break;
+    case 16: zline_n<16>(m, L, d, x, f, color); break;
+    default: mg_zline<<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, color);
   }
 }
 
@@ -1396,15 +1362,14 @@ static void smooth(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f,
   const MgLevel &L = w->lv[l];
   const MgLevelDev d = dev_level(m, L, l);
   for (int s = 0; s < sweeps; s++) {
-    // a sweep is red, black, package (pre) or package, black, red (post);
-    // a package step that follows a z-line launch runs inside it
     if (pre) {
-      zline(m, w, L, d, x, f, 0, false);
-      zline(m, w, L, d, x, f, 1, true);
+      zline(m, L, d, x, f, 0);
+      zline(m, L, d, x, f, 1);
+      mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
     } else {
-      if (s == 0) mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
-      zline(m, w, L, d, x, f, 1, false);
-      zline(m, w, L, d, x, f, 0, s + 1 < sweeps);
+      mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
+      zline(m, L, d, x, f, 1);
+      zline(m, L, d, x, f, 0);
     }
   }
 }
@@ -1438,13 +1403,13 @@ static void vcycle(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f)
     return;
   }
   const MgLevelDev d = dev_level(m, L, l);
-  smooth(m, w, l, x, f, 1, 2);
+  smooth(m, w, l, x, f, 1, MG_SWEEPS);
   mg_apply_cells<<<nb(L.ncell) + 1, MGT, 0, m->stream>>>(d, x, L.r, f, 1, w->d_ps);
   MgLevel &C = w->lv[l + 1];
   mg_restrict_f<<<nb(C.n), MGT, 0, m->stream>>>(L.r, C.f, m->nl, C.nr, C.nc, m->nx);
   vcycle(m, w, l + 1, C.x, C.f);
   mg_prolong_add<<<nb(L.n), MGT, 0, m->stream>>>(C.x, x, m->nl, C.nr, C.nc, m->nx);
-  smooth(m, w, l, x, f, 0, 2);
+  smooth(m, w, l, x, f, 0, MG_SWEEPS);
 }
 
 static int dot(hsb_dev_model *m, MgWork *w, const float *a, const float *b, long long n, double *out) {
