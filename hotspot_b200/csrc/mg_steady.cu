@@ -31,11 +31,13 @@ namespace hsb {
 #define MGT 256
 #define NXP 12
 #ifndef MG_SWEEPS
-#define MG_SWEEPS 2  // smoothing sweeps before and after each coarse-grid correction
+#define MG_SWEEPS 1  // smoothing sweeps before and after each coarse-grid correction
 #endif
 #ifndef MG_INNER
-#define MG_INNER 4   // PCG iterations per FP64 refinement pass
+#define MG_INNER 6   // PCG iterations per FP64 refinement pass
 #endif
+// background solves of at least this many cells yield between PCG iterations
+#define MG_YIELD_SPLIT_CELLS (1LL << 19)
 
 struct PackSys {               // the 12 package nodes' equations
   float D[NXP];                // diagonal (edge cells + links + ambient) at level 0
@@ -81,6 +83,11 @@ struct MgWork {
   cudaGraphExec_t pass_exec;
   const double *pass_T;
   int pass_version;
+  // the same pass in pieces (head + first iteration, one further iteration,
+  // tail), for solves that yield between iterations
+  cudaGraphExec_t piece_exec[3];
+  const double *piece_T;
+  int piece_version;
   // exact solve of the coarsest level: its dense FP64 inverse (cn x cn), or
   // none when the level is too large (then smoothing sweeps stand in)
   double *cinv;
@@ -1088,6 +1095,8 @@ static void free_mg(void *p) {
     if (q) cudaFree(q);
   if (w->h_red) cudaFreeHost(w->h_red);
   if (w->pass_exec) cudaGraphExecDestroy(w->pass_exec);
+  for (auto &e : w->piece_exec)
+    if (e) cudaGraphExecDestroy(e);
   delete w;
 }
 
@@ -1451,44 +1460,73 @@ int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
   // one refinement pass: r = b - G T (FP64), `inner` PCG iterations on
   // G e = r (FP32), T += e, |e|_2^2 to the host; the same kernel sequence
   // every time, so it is captured once as a CUDA graph and replayed
-  auto pass = [&]() {
+  auto head = [&]() {
     cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), m->stream);
     fine_residual64<<<nb(m->ncell), MGT, 0, m->stream>>>(S, w->gE64, w->gS64, w->gB64, gambL, w->gEdgeNS64,
                                                          w->gEdgeEW64, T, w->b64, w->r64, w->rr, maxbits);
     pack_residual64<<<1, 384, 0, m->stream>>>(S, w->d_ps, ge_p, link64, gamb_p, T, w->b64, w->r64, w->rr, maxbits);
     mg_zero<<<nb(n0), MGT, 0, m->stream>>>(w->e, n0);
-    for (int it = 0; it < inner; it++) {
-      vcycle(m, w, 0, w->z, w->rr);
-      dot(m, w, w->rr, w->z, n0, sc + 2);
-      pcg_update_p<<<nb(n0), MGT, 0, m->stream>>>(w->p, w->z, sc, n0, it == 0);
-      shift_scalars<<<1, 1, 0, m->stream>>>(sc);
-      mg_apply_cells<<<nb(L0.ncell) + 1, MGT, 0, m->stream>>>(d0, w->p, w->q, nullptr, 0, w->d_ps);
-      dot(m, w, w->p, w->q, n0, sc + 1);
-      pcg_update_xr<<<nb(n0), MGT, 0, m->stream>>>(w->e, w->rr, w->p, w->q, sc, n0);
-    }
+  };
+  auto iteration = [&](int it) {
+    vcycle(m, w, 0, w->z, w->rr);
+    dot(m, w, w->rr, w->z, n0, sc + 2);
+    pcg_update_p<<<nb(n0), MGT, 0, m->stream>>>(w->p, w->z, sc, n0, it == 0);
+    shift_scalars<<<1, 1, 0, m->stream>>>(sc);
+    mg_apply_cells<<<nb(L0.ncell) + 1, MGT, 0, m->stream>>>(d0, w->p, w->q, nullptr, 0, w->d_ps);
+    dot(m, w, w->p, w->q, n0, sc + 1);
+    pcg_update_xr<<<nb(n0), MGT, 0, m->stream>>>(w->e, w->rr, w->p, w->q, sc, n0);
+  };
+  auto tail = [&]() {
     // the max norm of this correction (K) decides convergence
     cudaMemsetAsync(sc + 3, 0, sizeof(double), m->stream);
     add_correction<<<nb(n0), MGT, 0, m->stream>>>(T, w->e, n0, (unsigned long long *)(sc + 3));
     cudaMemcpyAsync(w->h_red, sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, m->stream);
   };
-  if (!w->pass_exec || w->pass_T != T || w->pass_version != m->coef_version) {
-    if (w->pass_exec) {
-      cudaGraphExecDestroy(w->pass_exec);
-      w->pass_exec = nullptr;
+  auto capture = [&](auto &&fn, cudaGraphExec_t *out, const char *what) -> int {
+    if (*out) {
+      cudaGraphExecDestroy(*out);
+      *out = nullptr;
     }
     cudaGraph_t g;
     HSB_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
-    pass();
+    fn();
     const cudaError_t ce = cudaStreamEndCapture(m->stream, &g);
-    if (ce != cudaSuccess) return cuda_check(ce, "capturing the multigrid refinement pass");
-    const cudaError_t ie = cudaGraphInstantiate(&w->pass_exec, g, 0);
+    if (ce != cudaSuccess) return cuda_check(ce, what);
+    const cudaError_t ie = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) {
-      w->pass_exec = nullptr;
-      return cuda_check(ie, "instantiating the multigrid refinement pass");
+      *out = nullptr;
+      return cuda_check(ie, what);
     }
+    return HSB_OK;
+  };
+  // a background request (one a scheduler may hold, m->yield_fn) on a large
+  // model runs each pass iteration by iteration and offers to yield between
+  // them, so that it holds the device for one iteration at most after a
+  // priority request arrives; otherwise one graph per pass
+  const bool pieces = m->yield_fn && m->ncell >= MG_YIELD_SPLIT_CELLS && inner > 1;
+  if (!pieces && (!w->pass_exec || w->pass_T != T || w->pass_version != m->coef_version)) {
+    if ((rc = capture([&]() {
+                        head();
+                        for (int it = 0; it < inner; it++) iteration(it);
+                        tail();
+                      },
+                      &w->pass_exec, "capturing the multigrid refinement pass")))
+      return rc;
     w->pass_T = T;
     w->pass_version = m->coef_version;
+  }
+  if (pieces && (!w->piece_exec[0] || w->piece_T != T || w->piece_version != m->coef_version)) {
+    if ((rc = capture([&]() {
+                        head();
+                        iteration(0);
+                      },
+                      &w->piece_exec[0], "capturing the multigrid pass head")) ||
+        (rc = capture([&]() { iteration(1); }, &w->piece_exec[1], "capturing a multigrid pass iteration")) ||
+        (rc = capture([&]() { tail(); }, &w->piece_exec[2], "capturing the multigrid pass tail")))
+      return rc;
+    w->piece_T = T;
+    w->piece_version = m->coef_version;
   }
   // Stopping: the last correction is below tol, or the passes contract so
   // fast that the next correction -- the error left in T, estimated as
@@ -1499,7 +1537,17 @@ int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
   double rmax = 0.0, emax = 1e300, eprev = 0.0;
   bool converged = false;
   for (refine = 0; refine < max_ref; refine++) {
-    HSB_CUDA(cudaGraphLaunch(w->pass_exec, m->stream));
+    if (pieces) {
+      HSB_CUDA(cudaGraphLaunch(w->piece_exec[0], m->stream));
+      for (int it = 1; it < inner; it++) {
+        HSB_CUDA(cudaStreamSynchronize(m->stream));
+        m->yield_fn(m->yield_ctx);
+        HSB_CUDA(cudaGraphLaunch(w->piece_exec[1], m->stream));
+      }
+      HSB_CUDA(cudaGraphLaunch(w->piece_exec[2], m->stream));
+    } else {
+      HSB_CUDA(cudaGraphLaunch(w->pass_exec, m->stream));
+    }
     HSB_CUDA(cudaStreamSynchronize(m->stream));
     {
       unsigned long long bits;

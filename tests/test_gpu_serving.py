@@ -37,7 +37,9 @@ def _requests(server, scs, models, rng, n, rate):
 def test_alone_equals_mixed(workdir):
     rng = np.random.default_rng(90)
     scs = [W.scenario_random_chip(workdir, rng, "a", side=64, chip_layers=2, steps=0),
-           W.scenario_random_chip(workdir, rng, "b", side=128, chip_layers=3, steps=0),
+           # 256x256x8 = 2^19 cells: a background steady solve this large runs
+           # its passes iteration by iteration in the mixed run
+           W.scenario_random_chip(workdir, rng, "b", side=256, chip_layers=6, steps=0),
            W.scenario_random_chip(workdir, rng, "c", side=64, chip_layers=4, steps=0)]
     models = [hm.from_scenario(sc) for sc in scs]
     srv = Server(workers=4)
