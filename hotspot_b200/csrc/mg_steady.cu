@@ -37,7 +37,7 @@ namespace hsb {
 #define MG_INNER 6   // PCG iterations per FP64 refinement pass
 #endif
 // background solves of at least this many cells yield between PCG iterations
-#define MG_YIELD_SPLIT_CELLS (1LL << 19)
+#define MG_YIELD_SPLIT_CELLS (1LL << 18)
 
 struct PackSys {               // the 12 package nodes' equations
   float D[NXP];                // diagonal (edge cells + links + ambient) at level 0

@@ -24,8 +24,11 @@
 // of them runs, the other requests pause at their next yield point: between
 // transient chunks (a background transient then runs its intervals in
 // chunks of about CHUNK_CELL_INTERVALS cell-intervals, so one launch holds
-// the device for about a millisecond) and between the refinement passes of
-// steady solves.
+// the device for under a millisecond), between the refinement passes of
+// steady solves and, on large models, between their PCG iterations.  A
+// priority request starts once the background requests in flight have all
+// reached a yield point (at most DRAIN_MS later), so it runs on a drained
+// device instead of interleaving with their kernels.
 //
 // Each request's result depends only on its model and inputs: the kernels
 // are deterministic and models share no mutable device state, so a result
@@ -44,7 +47,9 @@
 // worker threads reserved for high-priority requests
 #define HIGH_SLOTS 2
 // cell-intervals per launch of a background transient while a priority class runs
-#define CHUNK_CELL_INTERVALS (1LL << 21)
+#define CHUNK_CELL_INTERVALS (1LL << 20)
+// longest wait of a priority request for background work to reach a yield point
+#define DRAIN_MS 4.0
 #define CHUNK_MAX_INTERVALS 64
 
 struct hsb_server {
@@ -102,12 +107,17 @@ struct Gate {
   std::mutex *mu;
   std::condition_variable *cv;
   const int *high_running;
+  int *paused_low;               // background requests waiting here
 };
 
 static void gate_wait(void *ctx) {
   Gate *g = (Gate *)ctx;
   std::unique_lock<std::mutex> lk(*g->mu);
+  if (*g->high_running == 0) return;
+  ++*g->paused_low;
+  g->cv->notify_all();           // a priority request may be waiting for the device to drain
   while (*g->high_running > 0) g->cv->wait_for(lk, std::chrono::milliseconds(10));
+  --*g->paused_low;
 }
 
 // one request, synchronously, on the calling thread; gate: null, or the
@@ -151,10 +161,10 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
   std::mutex mu;
   std::condition_variable cv;
   std::vector<int> state(n, 0);   // 0 pending, 1 running, 2 done
-  int done = 0, running = 0, running_high = 0, running_low = 0;
+  int done = 0, running = 0, running_high = 0, running_low = 0, paused_low = 0;
   bool any_high = false;   // a high-priority request is in this run
   for (int k = 0; k < n; k++) any_high = any_high || s->models[reqs[k].model].high;
-  Gate gate{&mu, &cv, &running_high};
+  Gate gate{&mu, &cv, &running_high, &paused_low};
   std::string first_error;        // message of the first failed request
   using clk = std::chrono::steady_clock;
   const auto t0 = clk::now();
@@ -232,6 +242,13 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
       M.busy = true;
       r.start = t;
       r.worker = wid;
+      if (high) {
+        // let the background work already on the device drain: every
+        // running background request reaches its next yield point within
+        // one chunk or iteration (bounded wait, DRAIN_MS at most)
+        const auto until = clk::now() + std::chrono::microseconds((long long)(DRAIN_MS * 1000));
+        while (paused_low < running_low && clk::now() < until) cv.wait_until(lk, until);
+      }
       lk.unlock();
       const int rc = run_request(M, &r, (any_high && !high) ? &gate : nullptr);
       lk.lock();
