@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="transient intervals of the fast form only (the case profiled with ncu)")
     ap.add_argument("--headline-only", action="store_true", help="skip the batched / microchannel / serving legs")
-    ap.add_argument("--profile-case", choices=["batch", "microchannel"], default=None,
+    ap.add_argument("--profile-case", choices=["batch", "microchannel", "steady"], default=None,
                     help="small cases of the other kernels, for ncu captures (a few GB at most)")
     ap.add_argument("--batch-chips", type=int, default=512)
     ap.add_argument("--batch-intervals", type=int, default=10)
@@ -609,8 +609,9 @@ def run_ours(args):
 
 
 def profile_case(args):
-    """Small cases of the batched transient and of the BiCGStab solver, sized
-    for ncu (inputs above the L2 size, a few GB on the device at most)."""
+    """Small cases of the batched transient, the MG steady solve of the
+    serving latency class and the BiCGStab solver, sized for ncu (a few GB on
+    the device at most)."""
     from hotspot_b200 import FORM_FAST, STEADY_BICGSTAB
     from hotspot_b200 import model as hm
     from hotspot_b200 import workloads as W
@@ -636,6 +637,19 @@ def profile_case(args):
             out.append({"kernel_ms": st["kernel_ms"], "rk4_steps": st["rk4_steps"]})
         print(json.dumps({"profile_case": "batch", "cells": int(sum(m.n_cells for m in models)), "intervals": out}))
         bt.close()
+    elif args.profile_case == "steady":
+        # the serving latency class: one 256x256 chip with 4 chip layers, MG-PCG to 1e-5 K
+        sc = W.scenario_random_chip(d, np.random.default_rng([0, 256, 4, 1]), "p", side=256, chip_layers=4, steps=0)
+        m = hm.from_scenario(sc)
+        m.set_solver(FORM_FAST, steady_tol=1e-5)
+        nblk = sum(m.layer_units[l] for l in range(m.n_layers) if m.layer_power[l])
+        p = m.power_vector(np.random.default_rng(1).uniform(0.5, 20.0, nblk))
+        s = m.vector()
+        m.steady(p.copy(), s)
+        st = m.stats()
+        print(json.dumps({"profile_case": "steady", "cells": m.n_cells, "device_ms": st["device_ms"],
+                          "refinements": st["refinements"], "cycles": st["cycles"]}))
+        m.close()
     else:
         sc = W.scenario_microchannel(d, seed=3, grid=128, die=128 * 20e-6, blocks=8)
         m = hm.from_scenario(sc)
