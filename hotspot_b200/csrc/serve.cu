@@ -192,6 +192,7 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
         hsb_server::Model &M = s->models[r.model];
         if (M.busy) continue;
         if (!M.high && running_low >= s->workers) continue;   // the other threads are kept for high priority
+        if (!M.high && running_high > 0) continue;             // no new background work while a priority request runs
         if (!M.warm) {   // first use: admission by free device memory
           if (!mem_known) {
             cudaSetDevice(M.m->device);
