@@ -270,9 +270,9 @@ __device__ __forceinline__ void zline_colT(const MgLevelDev &L, float *x, const 
     if (n < nl) {
       const float a = n > 0 ? -gb[n - 1] : 0.f;   // sub-diagonal
       const float cc = -gb[n];                     // super-diagonal (0 on the last layer)
-      const float den = bd[n] - a * prev_c;
-      const float cn = cc / den;
-      const float dn = (rhs[n] - a * prev_d) / den;
+      const float inv = 1.f / (bd[n] - a * prev_c);
+      const float cn = cc * inv;
+      const float dn = (rhs[n] - a * prev_d) * inv;
       cp[n] = cn;
       dp[n] = dn;
       prev_c = cn;
@@ -537,6 +537,159 @@ __host__ __device__ inline long long fused_block_floats(long long ncell, int nl)
   return (3 * n + 4 * ncell + NXP * NXP + 3 * nl + 3) / 4 * 4;
 }
 
+// phases of the fused coarse cycle (one CTA; each ends with a block barrier),
+// kept out of line so the kernel's code stays small
+// the z-lines of one colour (non-coarsest levels have an even column count)
+template <int MAXL>
+__device__ __noinline__ void fz_zl(const MgLevelDev &L, float *x, const float *f, int color) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int half = L.nc >> 1, ncol = (int)(L.plane >> 1);
+  for (int k = tid; k < ncol; k += nt) {
+    const int i = k / half, jj = k - i * half;
+    const int j = 2 * jj + ((i + color) & 1);
+    zline_colT<MAXL>(L, x, f, i * L.nc + j);
+  }
+  __syncthreads();
+}
+
+// package nodes with the grid fixed (mg_pack_solve)
+__device__ __noinline__ void fz_pk(const MgLevelDev &L, const PackSys *ps, float *x, const float *f, float *esum,
+                                   float *prhs) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int w = tid >> 5, lane = tid & 31, nw = nt >> 5;
+  for (int k = w; k < NXP; k += nw) {
+    float sm = 0.f;
+    const int layer = ps->elayer[k], side = ps->eside[k];
+    if (layer >= 0) {
+      const int len = side < 2 ? L.nc : L.nr;
+      const long long base = (long long)layer * L.plane +
+                             (side == 0 ? 0 : side == 1 ? (long long)(L.nr - 1) * L.nc : side == 2 ? 0 : L.nc - 1);
+      const long long st = side < 2 ? 1 : L.nc;
+      for (int q = lane; q < len; q += 32) sm += x[base + q * st];
+      for (int o = 16; o > 0; o >>= 1) sm += __shfl_down_sync(0xffffffffu, sm, o);
+    }
+    if (lane == 0) esum[k] = sm;
+  }
+  __syncthreads();
+  if (tid < NXP) prhs[tid] = f[L.ncell + tid] + ps->ge0[tid] * L.scale * esum[tid];
+  __syncthreads();
+  if (tid < NXP) {
+    float v = 0.f;
+#pragma unroll
+    for (int o = 0; o < NXP; o++) v += L.pinv[tid * NXP + o] * prhs[o];
+    x[L.ncell + tid] = v;
+  }
+  __syncthreads();
+}
+
+// r = f - A x (mg_apply_cells and mg_apply_pack, mode 1)
+__device__ __noinline__ void fz_resid(const MgLevelDev &L, const PackSys *ps, const float *x, const float *f, float *r,
+                                      float *esum) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int w = tid >> 5, lane = tid & 31, nw = nt >> 5;
+  const float *xp = x + L.ncell;
+  const int plane = (int)L.plane, ncl = (int)L.ncell;
+  for (int c = tid; c < ncl; c += nt) {
+    const int n = c / plane;
+    const int q = c - n * plane;
+    const int i = q / L.nc, j = q - i * L.nc;
+    const float xc = x[c];
+    float s = L.gAmbL[n] * xc;
+    if (j < L.nc - 1) s += L.gE[c] * (xc - x[c + 1]);
+    if (j > 0) s += L.gE[c - 1] * (xc - x[c - 1]);
+    if (i < L.nr - 1) s += L.gS[c] * (xc - x[c + L.nc]);
+    if (i > 0) s += L.gS[c - L.nc] * (xc - x[c - L.nc]);
+    if (n < L.nl - 1) s += L.gB[c] * (xc - x[c + L.plane]);
+    if (n > 0) s += L.gB[c - L.plane] * (xc - x[c - L.plane]);
+    if (n == L.spidx || n == L.hsidx) {
+      if (i == 0) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 0, L.spidx, L.hsidx)]);
+      if (i == L.nr - 1) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 1, L.spidx, L.hsidx)]);
+      if (j == 0) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 2, L.spidx, L.hsidx)]);
+      if (j == L.nc - 1) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 3, L.spidx, L.hsidx)]);
+    }
+    r[c] = f[c] - s;
+  }
+  for (int k = w; k < NXP; k += nw) {
+    float sm = 0.f;
+    const int layer = ps->elayer[k], side = ps->eside[k];
+    if (layer >= 0) {
+      const int len = side < 2 ? L.nc : L.nr;
+      const long long base = (long long)layer * L.plane +
+                             (side == 0 ? 0 : side == 1 ? (long long)(L.nr - 1) * L.nc : side == 2 ? 0 : L.nc - 1);
+      const long long st = side < 2 ? 1 : L.nc;
+      const float xk = xp[k];
+      for (int q = lane; q < len; q += 32) sm += xk - x[base + q * st];
+      for (int o = 16; o > 0; o >>= 1) sm += __shfl_down_sync(0xffffffffu, sm, o);
+    }
+    if (lane == 0) esum[k] = sm;
+  }
+  __syncthreads();
+  if (tid < NXP) {
+    const int k = tid;
+    const float ge = ps->ge0[k] * L.scale;
+    float s = ge * esum[k] + ps->gamb[k] * xp[k];
+    for (int o = 0; o < NXP; o++) s += ps->link[k][o] * (xp[k] - xp[o]);
+    r[L.ncell + k] = f[L.ncell + k] - s;
+  }
+  __syncthreads();
+}
+
+// coarse f = P^T r (mg_restrict_f)
+__device__ __noinline__ void fz_restrict(const MgLevelDev &F, const float *rf, const MgLevelDev &C, float *fc) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int cnr = C.nr, cnc = C.nc, fnr = F.nr, fnc = F.nc;
+  const int cpl = (int)C.plane, fpl = (int)F.plane, cncell = (int)C.ncell;
+  for (int t = tid; t < cncell + NXP; t += nt) {
+    if (t < cncell) {
+      const int n = t / cpl;
+      const int q = t - n * cpl;
+      const int i = q / cnc, j = q - i * cnc;
+      const float *src = rf + n * fpl;
+      float acc = 0.f;
+      for (int fi = 2 * i - 1; fi <= 2 * i + 2; fi++) {
+        if (fi < 0 || fi >= fnr) continue;
+        const float wi = bl_w(fi, i, cnr);
+        if (wi == 0.f) continue;
+        float row = 0.f;
+        for (int fj = 2 * j - 1; fj <= 2 * j + 2; fj++) {
+          if (fj < 0 || fj >= fnc) continue;
+          const float wj = bl_w(fj, j, cnc);
+          if (wj != 0.f) row += wj * src[(long long)fi * fnc + fj];
+        }
+        acc += wi * row;
+      }
+      fc[t] = acc;
+    } else {
+      fc[t] = rf[F.ncell + (t - cncell)];
+    }
+  }
+  __syncthreads();
+}
+
+// fine x += P xc (mg_prolong_add)
+__device__ __noinline__ void fz_prolong(const MgLevelDev &C, const float *xc, const MgLevelDev &F, float *xf) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int cnr = C.nr, cnc = C.nc, fnc = F.nc;
+  const int cpl = (int)C.plane, fpl = (int)F.plane, fncell = (int)F.ncell;
+  for (int t = tid; t < fncell + NXP; t += nt) {
+    if (t < fncell) {
+      const int n = t / fpl;
+      const int q = t - n * fpl;
+      const int fi = q / fnc, fj = q - fi * fnc;
+      const int ci = fi >> 1, cj = fj >> 1;
+      int ci2 = ci + ((fi & 1) ? 1 : -1), cj2 = cj + ((fj & 1) ? 1 : -1);
+      ci2 = ci2 < 0 ? 0 : ci2 >= cnr ? cnr - 1 : ci2;
+      cj2 = cj2 < 0 ? 0 : cj2 >= cnc ? cnc - 1 : cj2;
+      const float *c = xc + n * cpl;
+      xf[t] += 0.5625f * c[(long long)ci * cnc + cj] + 0.1875f * c[(long long)ci2 * cnc + cj] +
+               0.1875f * c[(long long)ci * cnc + cj2] + 0.0625f * c[(long long)ci2 * cnc + cj2];
+    } else {
+      xf[t] += xc[C.ncell + (t - fncell)];
+    }
+  }
+  __syncthreads();
+}
+
 template <int MAXL>
 __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_constant__ FusedArgs A) {
   extern __shared__ __align__(16) float smf[];
@@ -577,142 +730,6 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
   }
   __syncthreads();
 
-  // the z-lines of one colour (non-coarsest levels have an even column count)
-  auto zl = [&](const MgLevelDev &L, float *x, const float *f, int color) {
-    const int half = L.nc >> 1, ncol = (int)(L.plane >> 1);
-    for (int k = tid; k < ncol; k += nt) {
-      const int i = k / half, jj = k - i * half;
-      const int j = 2 * jj + ((i + color) & 1);
-      zline_colT<MAXL>(L, x, f, i * L.nc + j);
-    }
-    __syncthreads();
-  };
-  // package nodes with the grid fixed (mg_pack_solve)
-  auto pk = [&](const MgLevelDev &L, float *x, const float *f) {
-    for (int k = w; k < NXP; k += nw) {
-      float sm = 0.f;
-      const int layer = ps->elayer[k], side = ps->eside[k];
-      if (layer >= 0) {
-        const int len = side < 2 ? L.nc : L.nr;
-        const long long base = (long long)layer * L.plane +
-                               (side == 0 ? 0 : side == 1 ? (long long)(L.nr - 1) * L.nc : side == 2 ? 0 : L.nc - 1);
-        const long long st = side < 2 ? 1 : L.nc;
-        for (int q = lane; q < len; q += 32) sm += x[base + q * st];
-        for (int o = 16; o > 0; o >>= 1) sm += __shfl_down_sync(0xffffffffu, sm, o);
-      }
-      if (lane == 0) esum[k] = sm;
-    }
-    __syncthreads();
-    if (tid < NXP) prhs[tid] = f[L.ncell + tid] + ps->ge0[tid] * L.scale * esum[tid];
-    __syncthreads();
-    if (tid < NXP) {
-      float v = 0.f;
-#pragma unroll
-      for (int o = 0; o < NXP; o++) v += L.pinv[tid * NXP + o] * prhs[o];
-      x[L.ncell + tid] = v;
-    }
-    __syncthreads();
-  };
-  // r = f - A x (mg_apply_cells and mg_apply_pack, mode 1)
-  auto resid = [&](const MgLevelDev &L, const float *x, const float *f, float *r) {
-    const float *xp = x + L.ncell;
-    const int plane = (int)L.plane, ncl = (int)L.ncell;
-    for (int c = tid; c < ncl; c += nt) {
-      const int n = c / plane;
-      const int q = c - n * plane;
-      const int i = q / L.nc, j = q - i * L.nc;
-      const float xc = x[c];
-      float s = L.gAmbL[n] * xc;
-      if (j < L.nc - 1) s += L.gE[c] * (xc - x[c + 1]);
-      if (j > 0) s += L.gE[c - 1] * (xc - x[c - 1]);
-      if (i < L.nr - 1) s += L.gS[c] * (xc - x[c + L.nc]);
-      if (i > 0) s += L.gS[c - L.nc] * (xc - x[c - L.nc]);
-      if (n < L.nl - 1) s += L.gB[c] * (xc - x[c + L.plane]);
-      if (n > 0) s += L.gB[c - L.plane] * (xc - x[c - L.plane]);
-      if (n == L.spidx || n == L.hsidx) {
-        if (i == 0) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 0, L.spidx, L.hsidx)]);
-        if (i == L.nr - 1) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 1, L.spidx, L.hsidx)]);
-        if (j == 0) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 2, L.spidx, L.hsidx)]);
-        if (j == L.nc - 1) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 3, L.spidx, L.hsidx)]);
-      }
-      r[c] = f[c] - s;
-    }
-    for (int k = w; k < NXP; k += nw) {
-      float sm = 0.f;
-      const int layer = ps->elayer[k], side = ps->eside[k];
-      if (layer >= 0) {
-        const int len = side < 2 ? L.nc : L.nr;
-        const long long base = (long long)layer * L.plane +
-                               (side == 0 ? 0 : side == 1 ? (long long)(L.nr - 1) * L.nc : side == 2 ? 0 : L.nc - 1);
-        const long long st = side < 2 ? 1 : L.nc;
-        const float xk = xp[k];
-        for (int q = lane; q < len; q += 32) sm += xk - x[base + q * st];
-        for (int o = 16; o > 0; o >>= 1) sm += __shfl_down_sync(0xffffffffu, sm, o);
-      }
-      if (lane == 0) esum[k] = sm;
-    }
-    __syncthreads();
-    if (tid < NXP) {
-      const int k = tid;
-      const float ge = ps->ge0[k] * L.scale;
-      float s = ge * esum[k] + ps->gamb[k] * xp[k];
-      for (int o = 0; o < NXP; o++) s += ps->link[k][o] * (xp[k] - xp[o]);
-      r[L.ncell + k] = f[L.ncell + k] - s;
-    }
-    __syncthreads();
-  };
-  // coarse f = P^T r (mg_restrict_f)
-  auto restrict_to = [&](const MgLevelDev &F, const float *rf, const MgLevelDev &C, float *fc) {
-    const int cnr = C.nr, cnc = C.nc, fnr = F.nr, fnc = F.nc;
-    const int cpl = (int)C.plane, fpl = (int)F.plane, cncell = (int)C.ncell;
-    for (int t = tid; t < cncell + NXP; t += nt) {
-      if (t < cncell) {
-        const int n = t / cpl;
-        const int q = t - n * cpl;
-        const int i = q / cnc, j = q - i * cnc;
-        const float *src = rf + n * fpl;
-        float acc = 0.f;
-        for (int fi = 2 * i - 1; fi <= 2 * i + 2; fi++) {
-          if (fi < 0 || fi >= fnr) continue;
-          const float wi = bl_w(fi, i, cnr);
-          if (wi == 0.f) continue;
-          float row = 0.f;
-          for (int fj = 2 * j - 1; fj <= 2 * j + 2; fj++) {
-            if (fj < 0 || fj >= fnc) continue;
-            const float wj = bl_w(fj, j, cnc);
-            if (wj != 0.f) row += wj * src[(long long)fi * fnc + fj];
-          }
-          acc += wi * row;
-        }
-        fc[t] = acc;
-      } else {
-        fc[t] = rf[F.ncell + (t - cncell)];
-      }
-    }
-    __syncthreads();
-  };
-  // fine x += P xc (mg_prolong_add)
-  auto prolong = [&](const MgLevelDev &C, const float *xc, const MgLevelDev &F, float *xf) {
-    const int cnr = C.nr, cnc = C.nc, fnc = F.nc;
-    const int cpl = (int)C.plane, fpl = (int)F.plane, fncell = (int)F.ncell;
-    for (int t = tid; t < fncell + NXP; t += nt) {
-      if (t < fncell) {
-        const int n = t / fpl;
-        const int q = t - n * fpl;
-        const int fi = q / fnc, fj = q - fi * fnc;
-        const int ci = fi >> 1, cj = fj >> 1;
-        int ci2 = ci + ((fi & 1) ? 1 : -1), cj2 = cj + ((fj & 1) ? 1 : -1);
-        ci2 = ci2 < 0 ? 0 : ci2 >= cnr ? cnr - 1 : ci2;
-        cj2 = cj2 < 0 ? 0 : cj2 >= cnc ? cnc - 1 : cj2;
-        const float *c = xc + n * cpl;
-        xf[t] += 0.5625f * c[(long long)ci * cnc + cj] + 0.1875f * c[(long long)ci2 * cnc + cj] +
-                 0.1875f * c[(long long)ci * cnc + cj2] + 0.0625f * c[(long long)ci2 * cnc + cj2];
-      } else {
-        xf[t] += xc[C.ncell + (t - fncell)];
-      }
-    }
-    __syncthreads();
-  };
 
   const int nf = A.nf;
   {
@@ -728,13 +745,13 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
     for (long long q = tid; q < n; q += nt) x[q] = 0.f;
     __syncthreads();
     for (int sw = 0; sw < MG_SWEEPS; sw++) {
-      zl(L, x, f, 0);
-      zl(L, x, f, 1);
-      pk(L, x, f);
+      fz_zl<MAXL>(L, x, f, 0);
+      fz_zl<MAXL>(L, x, f, 1);
+      fz_pk(L, ps, x, f, esum, prhs);
     }
-    resid(L, x, f, r);
+    fz_resid(L, ps, x, f, r, esum);
     const MgLevelDev &C = SL[k + 1];
-    restrict_to(L, r, C, smf + A.off[k + 1] + (C.ncell + NXP));
+    fz_restrict(L, r, C, smf + A.off[k + 1] + (C.ncell + NXP));
   }
   {   // coarsest: x = A^-1 f, one warp per row
     const MgLevelDev &C = SL[nf - 1];
@@ -747,11 +764,11 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) mg_cycle_fused(const __grid_c
     const MgLevelDev &L = SL[k], &C = SL[k + 1];
     const long long n = L.ncell + NXP;
     float *x = smf + A.off[k], *f = x + n;
-    prolong(C, smf + A.off[k + 1], L, x);
+    fz_prolong(C, smf + A.off[k + 1], L, x);
     for (int sw = 0; sw < MG_SWEEPS; sw++) {
-      pk(L, x, f);
-      zl(L, x, f, 1);
-      zl(L, x, f, 0);
+      fz_pk(L, ps, x, f, esum, prhs);
+      fz_zl<MAXL>(L, x, f, 1);
+      fz_zl<MAXL>(L, x, f, 0);
     }
   }
   {
