@@ -96,6 +96,7 @@ struct MgWork {
   // (mg_cycle_fused); -1: every level kernel by kernel
   int fuse;
   size_t fuse_smem;
+  unsigned *dot_ticket;          // last-block counter of dot_one (returns to 0 after each launch)
 };
 
 // ---------------------------------------------------------------------------
@@ -229,7 +230,9 @@ __device__ __forceinline__ void zline_col(const MgLevelDev &L, float *__restrict
 // before the elimination starts (the arrays live in registers), so a column
 // costs one memory round trip instead of one per layer.  x and f may be
 // global or shared memory.
-template <int MAXL, bool EXACT = false>
+// ZERO: x is zero on entry (the first half sweep of a V-cycle level), so the
+// right-hand side is f alone -- the neighbour and package terms all vanish
+template <int MAXL, bool EXACT = false, bool ZERO = false>
 __device__ __forceinline__ void zline_colT(const MgLevelDev &L, float *x, const float *f, int col) {
   const int nc = L.nc, nr = L.nr;
   const int i = col / nc, j = col - i * nc;
@@ -245,14 +248,16 @@ __device__ __forceinline__ void zline_colT(const MgLevelDev &L, float *x, const 
   for (int n = 0; n < MAXL; n++) {
     if (n < nl) {
       const long long c = (long long)n * L.plane + col;
-      const float wE = dE ? L.gE[c] : 0.f, wW = dW ? L.gE[c - dW] : 0.f;
-      const float wS = dS ? L.gS[c] : 0.f, wN = dN ? L.gS[c - dN] : 0.f;
       float r = f[c];
-      r += wE * x[c + dE];
-      r += wW * x[c - dW];
-      r += wS * x[c + dS];
-      r += wN * x[c - dN];
-      if (n == L.spidx || n == L.hsidx) {
+      if (!ZERO) {
+        const float wE = dE ? L.gE[c] : 0.f, wW = dW ? L.gE[c - dW] : 0.f;
+        const float wS = dS ? L.gS[c] : 0.f, wN = dN ? L.gS[c - dN] : 0.f;
+        r += wE * x[c + dE];
+        r += wW * x[c - dW];
+        r += wS * x[c + dS];
+        r += wN * x[c - dN];
+      }
+      if (!ZERO && (n == L.spidx || n == L.hsidx)) {
         if (i == 0) r += L.gEdgeNS[n] * xp[edge_node(n, 0, L.spidx, L.hsidx)];
         if (i == nr - 1) r += L.gEdgeNS[n] * xp[edge_node(n, 1, L.spidx, L.hsidx)];
         if (j == 0) r += L.gEdgeEW[n] * xp[edge_node(n, 2, L.spidx, L.hsidx)];
@@ -291,13 +296,23 @@ __device__ __forceinline__ void zline_colT(const MgLevelDev &L, float *x, const 
 
 // one colour of z-lines for models of exactly NL layers (columns < 2^31,
 // checked at set-up)
+// first: x holds no defined values yet and counts as zero -- this colour is
+// solved from f alone and the other colour and the package nodes are set to
+// zero (what a zeroing pass followed by this half sweep gives)
 template <int NL>
 __global__ void __launch_bounds__(MGT) mg_zline_t(MgLevelDev L, float *__restrict__ x, const float *__restrict__ f,
-                                                  int color) {
+                                                  int color, int first) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= L.plane) return;
   const int i = col / L.nc, j = col - i * L.nc;
-  if (((i + j) & 1) == color) zline_colT<NL, true>(L, x, f, col);
+  if (first && blockIdx.x == 0 && threadIdx.x < NXP) x[L.ncell + threadIdx.x] = 0.f;
+  if (((i + j) & 1) == color) {
+    if (first) zline_colT<NL, true, true>(L, x, f, col);
+    else zline_colT<NL, true>(L, x, f, col);
+  } else if (first) {
+#pragma unroll
+    for (int n = 0; n < NL; n++) x[(long long)n * L.plane + col] = 0.f;
+  }
 }
 
 // red-black z-line Gauss-Seidel half sweep on level L: solve A x = f
@@ -894,9 +909,14 @@ __global__ void pack_residual64(const hsb::StencilArgs S, const PackSys *__restr
 // ---------------------------------------------------------------------------
 // PCG vector kernels (FP32 data, FP64 reductions in a fixed order)
 // ---------------------------------------------------------------------------
-__global__ void dot_partial(const float *__restrict__ a, const float *__restrict__ b, long long n,
-                            double *__restrict__ part) {
+// dot product in one launch: each block writes its partial, and the last
+// block to finish (ticket counter, no waiting) adds the partials in block
+// order; shift: the previous value of *out is first moved there (the PCG
+// keeps rz_old beside rz)
+__global__ void dot_one(const float *__restrict__ a, const float *__restrict__ b, long long n,
+                        double *__restrict__ part, unsigned *__restrict__ ticket, double *out, double *shift) {
   __shared__ double sm[MGT / 32];
+  __shared__ int last;
   double s = 0.0;
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
     s += (double)a[k] * (double)b[k];
@@ -907,27 +927,31 @@ __global__ void dot_partial(const float *__restrict__ a, const float *__restrict
     double t = 0.0;
     for (int w = 0; w < MGT / 32; w++) t += sm[w];
     part[blockIdx.x] = t;
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
   }
-}
-
-__global__ void dot_final(const double *__restrict__ part, int np, double *__restrict__ out) {
-  __shared__ double sm[32];
-  double s = 0.0;
-  for (int k = threadIdx.x; k < np; k += blockDim.x) s += part[k];
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  s = 0.0;
+  for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) s += __ldcg(part + k);
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  __syncthreads();
   if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
   __syncthreads();
   if (threadIdx.x == 0) {
     double t = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sm[w];
+    for (int w = 0; w < MGT / 32; w++) t += sm[w];
+    if (shift) *shift = *out;
     *out = t;
+    *ticket = 0u;
   }
 }
 
-// x += alpha p; r -= alpha q   with alpha = rz / pq
+// x += alpha p; r -= alpha q   with alpha = rz / pq  (sc[2] rz, sc[1] pq)
 __global__ void pcg_update_xr(float *__restrict__ x, float *__restrict__ r, const float *__restrict__ p,
                               const float *__restrict__ q, const double *__restrict__ sc, long long n) {
-  const double alpha = sc[0] / sc[1];
+  const double alpha = sc[2] / sc[1];
   const float a = (float)alpha;
   long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) {
@@ -942,11 +966,6 @@ __global__ void pcg_update_p(float *__restrict__ p, const float *__restrict__ z,
   const float beta = first ? 0.f : (float)(sc[2] / sc[0]);
   long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) p[k] = z[k] + beta * p[k];
-}
-
-__global__ void shift_scalars(double *sc) {
-  // sc[0] = rz (old) <- sc[2] (new)
-  sc[0] = sc[2];
 }
 
 // T += e; the max |e| (K) into *emax_bits (zeroed by the caller)
@@ -1091,6 +1110,8 @@ static int mg_setup(hsb_dev_model *m, MgWork **out) {
   HSB_CUDA(cudaMalloc(&w->rr, sizeof(float) * n0));
   HSB_CUDA(cudaMalloc(&w->red, sizeof(double) * 4096));
   HSB_CUDA(cudaMalloc(&w->d_ps, sizeof(PackSys)));
+  HSB_CUDA(cudaMalloc(&w->dot_ticket, sizeof(unsigned)));
+  HSB_CUDA(cudaMemset(w->dot_ticket, 0, sizeof(unsigned)));
   if (w->lv[0].plane >= (1LL << 31) - MGT) return set_error(HSB_E_ARG, "multigrid: more than 2^31 columns per layer");
 
   HSB_CUDA(cudaMallocHost(&w->h_red, sizeof(double) * 8));
@@ -1107,7 +1128,7 @@ static void free_mg(void *p) {
       if (q) cudaFree(q);
   }
   void *b2[] = {w->gE64, w->gS64, w->gB64, w->gAmb64, w->gEdgeNS64, w->gEdgeEW64, w->r64, w->b64,
-                w->p, w->q, w->z, w->e, w->rr, w->red, w->d_ps, w->cinv};
+                w->p, w->q, w->z, w->e, w->rr, w->red, w->d_ps, w->cinv, w->dot_ticket};
   for (void *q : b2)
     if (q) cudaFree(q);
   if (w->h_red) cudaFreeHost(w->h_red);
@@ -1356,40 +1377,45 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
 }
 
 template <int NL>
-static void zline_n(hsb_dev_model *m, const MgLevel &L, const MgLevelDev &d, float *x, const float *f, int color) {
-  mg_zline_t<NL><<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, color);
+static void zline_n(hsb_dev_model *m, const MgLevel &L, const MgLevelDev &d, float *x, const float *f, int color,
+                    int first) {
+  mg_zline_t<NL><<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, color, first);
 }
 
 // one colour of z-lines: the kernel compiled for the model's layer count
-// (up to 16), else the generic one
-static void zline(hsb_dev_model *m, const MgLevel &L, const MgLevelDev &d, float *x, const float *f, int color) {
+// (up to 16; first: x counts as zero, see mg_zline_t), else the generic one
+static void zline(hsb_dev_model *m, const MgLevel &L, const MgLevelDev &d, float *x, const float *f, int color,
+                  int first = 0) {
+  if (first && m->nl > 16) mg_zero<<<nb(L.n), MGT, 0, m->stream>>>(x, L.n);
   switch (m->nl) {
-    case 1: zline_n<1>(m, L, d, x, f, color); break;
-    case 2: zline_n<2>(m, L, d, x, f, color); break;
-    case 3: zline_n<3>(m, L, d, x, f, color); break;
-    case 4: zline_n<4>(m, L, d, x, f, color); break;
-    case 5: zline_n<5>(m, L, d, x, f, color); break;
-    case 6: zline_n<6>(m, L, d, x, f, color); break;
-    case 7: zline_n<7>(m, L, d, x, f, color); break;
-    case 8: zline_n<8>(m, L, d, x, f, color); break;
-    case 9: zline_n<9>(m, L, d, x, f, color); break;
-    case 10: zline_n<10>(m, L, d, x, f, color); break;
-    case 11: zline_n<11>(m, L, d, x, f, color); break;
-    case 12: zline_n<12>(m, L, d, x, f, color); break;
-    case 13: zline_n<13>(m, L, d, x, f, color); break;
-    case 14: zline_n<14>(m, L, d, x, f, color); break;
-    case 15: zline_n<15>(m, L, d, x, f, color); break;
-    case 16: zline_n<16>(m, L, d, x, f, color); break;
+    case 1: zline_n<1>(m, L, d, x, f, color, first); break;
+    case 2: zline_n<2>(m, L, d, x, f, color, first); break;
+    case 3: zline_n<3>(m, L, d, x, f, color, first); break;
+    case 4: zline_n<4>(m, L, d, x, f, color, first); break;
+    case 5: zline_n<5>(m, L, d, x, f, color, first); break;
+    case 6: zline_n<6>(m, L, d, x, f, color, first); break;
+    case 7: zline_n<7>(m, L, d, x, f, color, first); break;
+    case 8: zline_n<8>(m, L, d, x, f, color, first); break;
+    case 9: zline_n<9>(m, L, d, x, f, color, first); break;
+    case 10: zline_n<10>(m, L, d, x, f, color, first); break;
+    case 11: zline_n<11>(m, L, d, x, f, color, first); break;
+    case 12: zline_n<12>(m, L, d, x, f, color, first); break;
+    case 13: zline_n<13>(m, L, d, x, f, color, first); break;
+    case 14: zline_n<14>(m, L, d, x, f, color, first); break;
+    case 15: zline_n<15>(m, L, d, x, f, color, first); break;
+    case 16: zline_n<16>(m, L, d, x, f, color, first); break;
     default: mg_zline<<<nb(L.plane), MGT, 0, m->stream>>>(d, x, f, color);
   }
 }
 
-static void smooth(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f, int pre, int sweeps) {
+// first: x counts as zero on entry (the pre-smoothing of a V-cycle level)
+static void smooth(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f, int pre, int sweeps,
+                   int first = 0) {
   const MgLevel &L = w->lv[l];
   const MgLevelDev d = dev_level(m, L, l);
   for (int s = 0; s < sweeps; s++) {
     if (pre) {
-      zline(m, L, d, x, f, 0);
+      zline(m, L, d, x, f, 0, first && s == 0);
       zline(m, L, d, x, f, 1);
       mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
     } else {
@@ -1422,14 +1448,17 @@ static void vcycle(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f)
     else mg_cycle_fused<16><<<1, MG_FUSE_THREADS, w->fuse_smem, m->stream>>>(A);
     return;
   }
-  mg_zero<<<nb(L.n), MGT, 0, m->stream>>>(x, L.n);
   if (l == w->nlev - 1) {
-    if (w->cn > 0) mg_coarse_direct<<<1, 1024, 0, m->stream>>>(w->cinv, w->cn, x, f);
-    else mg_coarse_solve<<<1, 1024, 0, m->stream>>>(dev_level(m, L, l), w->d_ps, x, f, 8);
+    if (w->cn > 0) {
+      mg_coarse_direct<<<1, 1024, 0, m->stream>>>(w->cinv, w->cn, x, f);   // writes every entry
+    } else {
+      mg_zero<<<nb(L.n), MGT, 0, m->stream>>>(x, L.n);
+      mg_coarse_solve<<<1, 1024, 0, m->stream>>>(dev_level(m, L, l), w->d_ps, x, f, 8);
+    }
     return;
   }
   const MgLevelDev d = dev_level(m, L, l);
-  smooth(m, w, l, x, f, 1, MG_SWEEPS);
+  smooth(m, w, l, x, f, 1, MG_SWEEPS, 1);   // from x = 0: the first half sweep zeroes the rest
   mg_apply_cells<<<nb(L.ncell) + 1, MGT, 0, m->stream>>>(d, x, L.r, f, 1, w->d_ps);
   MgLevel &C = w->lv[l + 1];
   mg_restrict_f<<<nb(C.n), MGT, 0, m->stream>>>(L.r, C.f, m->nl, C.nr, C.nc, m->nx);
@@ -1438,10 +1467,10 @@ static void vcycle(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f)
   smooth(m, w, l, x, f, 0, MG_SWEEPS);
 }
 
-static int dot(hsb_dev_model *m, MgWork *w, const float *a, const float *b, long long n, double *out) {
+static int dot(hsb_dev_model *m, MgWork *w, const float *a, const float *b, long long n, double *out,
+               double *shift = nullptr) {
   const int np = 296;
-  dot_partial<<<np, MGT, 0, m->stream>>>(a, b, n, w->red + 16);
-  dot_final<<<1, 256, 0, m->stream>>>(w->red + 16, np, out);
+  dot_one<<<np, MGT, 0, m->stream>>>(a, b, n, w->red + 16, w->dot_ticket, out, shift);
   return HSB_OK;
 }
 
@@ -1486,9 +1515,8 @@ int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
   };
   auto iteration = [&](int it) {
     vcycle(m, w, 0, w->z, w->rr);
-    dot(m, w, w->rr, w->z, n0, sc + 2);
+    dot(m, w, w->rr, w->z, n0, sc + 2, sc);   // rz (sc[2]); its previous value to sc[0]
     pcg_update_p<<<nb(n0), MGT, 0, m->stream>>>(w->p, w->z, sc, n0, it == 0);
-    shift_scalars<<<1, 1, 0, m->stream>>>(sc);
     mg_apply_cells<<<nb(L0.ncell) + 1, MGT, 0, m->stream>>>(d0, w->p, w->q, nullptr, 0, w->d_ps);
     dot(m, w, w->p, w->q, n0, sc + 1);
     pcg_update_xr<<<nb(n0), MGT, 0, m->stream>>>(w->e, w->rr, w->p, w->q, sc, n0);
