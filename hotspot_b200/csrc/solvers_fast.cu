@@ -1212,7 +1212,11 @@ int bicgstab_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
     w->pass_T = T;
     w->pass_launches = cnt;
   }
-  double emax = 1e300, rmax = 0.0;
+  // stopping as in the multigrid solver: the last correction below tol, or
+  // passes contracting so fast (rho = |e_k| / |e_k-1| < 0.1) that the next
+  // correction, rho |e_k|, is below tol / 10
+  double emax = 1e300, rmax = 0.0, eprev = 0.0;
+  bool converged = false;
   for (int ref = 0; ref < max_ref; ref++) {
     HSB_CUDA(cudaGraphLaunch(w->pass_exec, m->stream));
     HSB_CUDA(cudaStreamSynchronize(m->stream));
@@ -1228,7 +1232,18 @@ int bicgstab_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
     st->refinements += 1;
     st->cycles += BC_INNER;
     if (!(emax == emax)) return set_error(HSB_E_NOCONV, "BiCGStab steady solve broke down (NaN correction)");
-    if (emax < tol) break;
+    if (emax < tol) {
+      converged = true;
+      break;
+    }
+    if (ref > 0 && eprev > 0.0) {
+      const double rho = emax / eprev;
+      if (rho < 0.1 && 10.0 * rho * emax < tol) {
+        converged = true;
+        break;
+      }
+    }
+    eprev = emax;
     if (m->yield_fn) m->yield_fn(m->yield_ctx);
   }
   // final FP64 residual for the record
@@ -1246,7 +1261,7 @@ int bicgstab_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
   }
   st->residual = rmax;
   st->launches += launches;
-  if (emax >= tol) return set_error(HSB_E_NOCONV, "BiCGStab steady solve did not converge");
+  if (!converged) return set_error(HSB_E_NOCONV, "BiCGStab steady solve did not converge");
   return HSB_OK;
 }
 
