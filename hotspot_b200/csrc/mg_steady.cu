@@ -513,77 +513,6 @@ __global__ void mg_prolong_add(const float *__restrict__ xc, float *__restrict__
   }
 }
 
-// increment that P xc adds to fine cell (n, fi, fj) (as mg_prolong_add)
-__device__ __forceinline__ float prolong_inc(const float *__restrict__ xc, int n, int fi, int fj, int cnr, int cnc) {
-  const int ci = fi >> 1, cj = fj >> 1;
-  int ci2 = ci + ((fi & 1) ? 1 : -1), cj2 = cj + ((fj & 1) ? 1 : -1);
-  ci2 = ci2 < 0 ? 0 : ci2 >= cnr ? cnr - 1 : ci2;
-  cj2 = cj2 < 0 ? 0 : cj2 >= cnc ? cnc - 1 : cj2;
-  const float *c = xc + (long long)n * cnr * cnc;
-  return 0.5625f * c[(long long)ci * cnc + cj] + 0.1875f * c[(long long)ci2 * cnc + cj] +
-         0.1875f * c[(long long)ci * cnc + cj2] + 0.0625f * c[(long long)ci2 * cnc + cj2];
-}
-
-// Fine x += P xc followed by the package step (mg_pack_solve's work) in one
-// launch.  The package edges lie on the border cells of the spreader and
-// sink layers: the last CTA owns those cells -- it adds their prolongation
-// into the 12 edge sums, then writes them, then solves the package nodes --
-// and the other CTAs prolong every other cell.  The package values are not
-// prolonged: the solve replaces them.
-__global__ void mg_prolong_pk(MgLevelDev F, const float *__restrict__ xc, float *__restrict__ xf,
-                              const float *__restrict__ f, int cnr, int cnc, const PackSys *__restrict__ ps) {
-  const int fnr = F.nr, fnc = F.nc;
-  const long long fpl = F.plane;
-  if (blockIdx.x == gridDim.x - 1) {
-    __shared__ float esum[NXP], prhs[NXP];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int k = w; k < NXP; k += nw) {
-      float sm = 0.f;
-      const int layer = ps->elayer[k], side = ps->eside[k];
-      if (layer >= 0) {
-        const int len = side < 2 ? fnc : fnr;
-        for (int q = lane; q < len; q += 32) {
-          const int fi = side == 0 ? 0 : side == 1 ? fnr - 1 : q;
-          const int fj = side < 2 ? q : side == 2 ? 0 : fnc - 1;
-          sm += xf[(long long)layer * fpl + (long long)fi * fnc + fj] + prolong_inc(xc, layer, fi, fj, cnr, cnc);
-        }
-        for (int o = 16; o > 0; o >>= 1) sm += __shfl_down_sync(0xffffffffu, sm, o);
-      }
-      if (lane == 0) esum[k] = sm;
-    }
-    __syncthreads();   // every border value is read before any is written
-    const int per = 2 * fnc + 2 * (fnr - 2);
-    for (int q = threadIdx.x; q < 2 * per; q += blockDim.x) {
-      const int layer = q < per ? F.spidx : F.hsidx;
-      if (layer < 0 || (q >= per && F.hsidx == F.spidx)) continue;
-      const int p = q < per ? q : q - per;
-      int fi, fj;
-      if (p < fnc) { fi = 0; fj = p; }
-      else if (p < 2 * fnc) { fi = fnr - 1; fj = p - fnc; }
-      else { fi = 1 + (p - 2 * fnc) / 2; fj = ((p - 2 * fnc) & 1) ? fnc - 1 : 0; }
-      const long long c = (long long)layer * fpl + (long long)fi * fnc + fj;
-      xf[c] += prolong_inc(xc, layer, fi, fj, cnr, cnc);
-    }
-    if (threadIdx.x < NXP) prhs[threadIdx.x] = f[F.ncell + threadIdx.x] + ps->ge0[threadIdx.x] * F.scale * esum[threadIdx.x];
-    __syncthreads();
-    if (threadIdx.x < NXP) {
-      float v = 0.f;
-#pragma unroll
-      for (int o = 0; o < NXP; o++) v += F.pinv[threadIdx.x * NXP + o] * prhs[o];
-      xf[F.ncell + threadIdx.x] = v;
-    }
-    return;
-  }
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= F.ncell) return;
-  const int n = (int)(t / fpl);
-  const long long r = t - n * fpl;
-  const int fi = (int)(r / fnc), fj = (int)(r - (long long)fi * fnc);
-  const bool border = fi == 0 || fi == fnr - 1 || fj == 0 || fj == fnc - 1;
-  if (border && (n == F.spidx || n == F.hsidx)) return;   // the last CTA's
-  xf[t] += prolong_inc(xc, n, fi, fj, cnr, cnc);
-}
-
 __global__ void mg_zero(float *x, long long n) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) x[t] = 0.f;
@@ -1480,9 +1409,8 @@ static void zline(hsb_dev_model *m, const MgLevel &L, const MgLevelDev &d, float
 }
 
 // first: x counts as zero on entry (the pre-smoothing of a V-cycle level)
-// skip_pk: the post-smoothing's first package step has been done already
 static void smooth(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f, int pre, int sweeps,
-                   int first = 0, int skip_pk = 0) {
+                   int first = 0) {
   const MgLevel &L = w->lv[l];
   const MgLevelDev d = dev_level(m, L, l);
   for (int s = 0; s < sweeps; s++) {
@@ -1491,7 +1419,7 @@ static void smooth(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f,
       zline(m, L, d, x, f, 1);
       mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
     } else {
-      if (!(skip_pk && s == 0)) mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
+      mg_pack_solve<<<1, 384, 0, m->stream>>>(d, w->d_ps, x, f);
       zline(m, L, d, x, f, 1);
       zline(m, L, d, x, f, 0);
     }
@@ -1535,9 +1463,8 @@ static void vcycle(hsb_dev_model *m, MgWork *w, int l, float *x, const float *f)
   MgLevel &C = w->lv[l + 1];
   mg_restrict_f<<<nb(C.n), MGT, 0, m->stream>>>(L.r, C.f, m->nl, C.nr, C.nc, m->nx);
   vcycle(m, w, l + 1, C.x, C.f);
-  // prolongation and the post-smoothing's first package step in one launch
-  mg_prolong_pk<<<nb(L.ncell) + 1, MGT, 0, m->stream>>>(d, C.x, x, f, C.nr, C.nc, w->d_ps);
-  smooth(m, w, l, x, f, 0, MG_SWEEPS, 0, 1);
+  mg_prolong_add<<<nb(L.n), MGT, 0, m->stream>>>(C.x, x, m->nl, C.nr, C.nc, m->nx);
+  smooth(m, w, l, x, f, 0, MG_SWEEPS);
 }
 
 static int dot(hsb_dev_model *m, MgWork *w, const float *a, const float *b, long long n, double *out,
