@@ -151,7 +151,6 @@ int rk4_exact_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
 int gs_exact_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
 
 // fast-form solvers
-int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
 int rk4_fast_stages_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
 // one interval of the fast form in two halves (rk4_fast.cu)
 int rk4_fast_interval_begin(hsb_dev_model *m, double time_elapsed, hsb_stats *st, void **work,

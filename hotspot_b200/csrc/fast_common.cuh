@@ -316,10 +316,6 @@ static int coop_grid(const hsb_dev_model *m, const void *fn, size_t smem, int *g
 int fast_prepare(hsb_dev_model *m, FastWork **out);
 // stage-by-stage fast RK4 over [0, T) starting from step size h0
 int rk4_stage_run(hsb_dev_model *m, FastWork *w, double T, double h0, hsb_stats *st);
-// Krylov-form fast RK4 over one interval; *t_done < T on return means the
-// rejection budget ran out there (the state is the last accepted step) and
-// *h_next is the step size to continue with
-int rk4_krylov_run(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next);
 // the Krylov vectors and their tensor maps (allocated once per model)
 int kry_prepare(hsb_dev_model *m, FastWork *w);
 // K intervals in one launch from K device block-power vectors; *done = the

@@ -109,7 +109,7 @@ __device__ __forceinline__ int edge_node(int layer, int side, int spidx, int hsi
   return -1;
 }
 
-// y = A x on level L (cells only; package rows handled by mg_apply_pack),
+// y = A x on level L (cells; the package rows by apply_pack_rows),
 // written in difference form, gAmb x + sum g (x - x_nbr): the system is
 // nearly singular (the overall temperature level is tied to ambient only
 // through weak convection), and diag*x - sum g*x_nbr would cancel most FP32
@@ -118,7 +118,7 @@ __device__ void apply_pack_rows(const MgLevelDev &L, const PackSys *__restrict__
                                 float *__restrict__ y, const float *__restrict__ f, int mode);
 
 // ps != null: the grid has one more CTA, which applies the package rows
-// (mg_apply_pack's work, in the same launch)
+// (apply_pack_rows, in the same launch)
 __global__ void mg_apply_cells(MgLevelDev L, const float *__restrict__ x, float *__restrict__ y,
                                const float *__restrict__ f, int mode, const PackSys *__restrict__ ps) {
   // mode 0: y = A x ; mode 1: y = f - A x
@@ -151,11 +151,6 @@ __global__ void mg_apply_cells(MgLevelDev L, const float *__restrict__ x, float 
 
 // package rows (one CTA), difference form: ge sum_edge (x_k - x_c) +
 // gamb x_k + sum link (x_k - x_o)
-__global__ void mg_apply_pack(MgLevelDev L, const PackSys *__restrict__ ps, const float *__restrict__ x,
-                              float *__restrict__ y, const float *__restrict__ f, int mode) {
-  apply_pack_rows(L, ps, x, y, f, mode);
-}
-
 __device__ void apply_pack_rows(const MgLevelDev &L, const PackSys *__restrict__ ps, const float *__restrict__ x,
                                 float *__restrict__ y, const float *__restrict__ f, int mode) {
   __shared__ float esum[NXP];
@@ -597,7 +592,7 @@ __device__ __noinline__ void fz_pk(const MgLevelDev &L, const PackSys *ps, float
   __syncthreads();
 }
 
-// r = f - A x (mg_apply_cells and mg_apply_pack, mode 1)
+// r = f - A x (mg_apply_cells with its package rows, mode 1)
 __device__ __noinline__ void fz_resid(const MgLevelDev &L, const PackSys *ps, const float *x, const float *f, float *r,
                                       float *esum) {
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -1262,7 +1257,7 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
   // the coarsest level exactly: the smoother cannot resolve the near-null
   // mode of the system (the overall temperature level, tied to ambient only
   // through the weak convection), so its operator is assembled on the host,
-  // as mg_apply_cells / mg_apply_pack apply it, and inverted once
+  // as mg_apply_cells applies it, and inverted once
   {
     const int lc = w->nlev - 1;
     const MgLevel &C = w->lv[lc];

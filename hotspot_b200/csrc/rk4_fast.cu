@@ -743,22 +743,6 @@ int rk4_fast_stages_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *s
   return rc;
 }
 
-// the Krylov form; when its rejection budget runs out inside an interval,
-// the stage form finishes the interval from the last accepted step
-int rk4_fast_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
-  FastWork *w;
-  int rc;
-  if ((rc = fast_prepare(m, &w))) return rc;
-  double t_done = time_elapsed, h_next = 0.0;
-  if ((rc = rk4_krylov_run(m, w, time_elapsed, st, &t_done, &h_next))) return rc;
-  if (t_done < time_elapsed) {
-    st->fallbacks += 1;
-    if ((rc = rk4_stage_run(m, w, time_elapsed - t_done, h_next, st))) return rc;
-  }
-  st->sim_time += time_elapsed;
-  return HSB_OK;
-}
-
 // one interval in two halves, so the caller can queue work that reads the
 // result (g2b with the state buffer chosen on the device) before waiting;
 // bpow_dev: the block powers, mapped to the grid in the kernel (null: the

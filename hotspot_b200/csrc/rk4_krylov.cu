@@ -671,11 +671,6 @@ int kry_prepare(hsb_dev_model *m, FastWork *w) {
 static int krylov_launch(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next,
                          const double *bpow, int K, int *done);
 
-int rk4_krylov_run(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, double *t_done, double *h_next) {
-  int done = 0;
-  return krylov_launch(m, w, T, st, t_done, h_next, nullptr, 0, &done);
-}
-
 int rk4_krylov_trace(hsb_dev_model *m, FastWork *w, const double *bpow, int K, double T, hsb_stats *st, int *done,
                      double *t_done, double *h_next) {
   return krylov_launch(m, w, T, st, t_done, h_next, bpow, K, done);
