@@ -1163,7 +1163,9 @@ static void bc_pass(hsb_dev_model *m, BcWork *w, double *T, int inner, long long
   cudaMemcpyAsync(w->h_red + 12, w->status, sizeof(int), cudaMemcpyDeviceToHost, m->stream);
 }
 
-static const int BC_INNER = 10;
+#ifndef BC_INNER
+#define BC_INNER 10   // BiCGStab iterations per FP64 refinement pass
+#endif
 
 int bicgstab_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
   if (m->nx != HSB_EXTRA) return set_error(HSB_E_ARG, "the BiCGStab steady solver models the primary heat path only");
