@@ -200,6 +200,14 @@ def cpu_throughput(grid: int, intervals: int, procs: int):
     return rate, procs, res[0][2], sum(r[0] for r in res), max(r[1] for r in res)
 
 
+def headline_config(grid, cells, ws):
+    """The headline workload, named the same way by both arms."""
+    return {"workload": f"3-D stack 4 chip layers + spreader/sink, {grid}x{grid} over 20x20 mm, "
+                        "40 blocks per Si layer, 10 us rows",
+            "cells_per_rank": cells, "l2": "256 MB buffer rewritten between timed steps (GPU arm)",
+            "parallelism": f"replicas x{ws}"}
+
+
 def run_reference(args):
     ws, rank, _ = dist()
     if rank != 0:
@@ -212,9 +220,7 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"3-D stack 4 chip layers + spreader/sink, {args.grid}x{args.grid}, "
-                                   "20x20 mm, 40 blocks per Si layer, 10 us rows",
-                       "cells": 6 * args.grid * args.grid},
+            "config": headline_config(args.grid, 6 * args.grid * args.grid, ws),
             "cpu_baseline": {"value": rate, "unit": "cell-steps/s", "cores": cores, "kind": kind,
                              "sample": f"{intervals} rows x {cores} independent single-threaded replicas"},
             "e2e": {"value": rate, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -565,10 +571,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": K,
         "warmup": Wm, "ms_per_step": dev_ms_max / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": f"3-D stack 4 chip layers + spreader/sink, {args.grid}x{args.grid} "
-                               "over 20x20 mm, 40 blocks per Si layer, 10 us rows, FP32 stages + FP64 state",
-                   "cells_per_rank": ncell, "l2": "256 MB buffer rewritten between timed steps",
-                   "parallelism": f"replicas x{ws}"},
+        "config": headline_config(args.grid, ncell, ws),
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "steady_solves_per_s": {"fast": steady_fast, "unit": "solves/s",
