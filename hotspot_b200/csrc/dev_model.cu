@@ -471,6 +471,9 @@ int hsb_dev_set_maps(hsb_dev_model *m, const int *b2g_ptr, const int *b2g_blk,
   HSB_CUDA(cudaMemcpyAsync(m->g2b, g2b, sizeof(int) * 5 * m->total_n_blocks, cudaMemcpyHostToDevice,
                            m->stream));
   m->cell_area = cell_area;
+  // new map arrays: whatever captured the old pointers (interval graphs,
+  // derived tables) is rebuilt on next use
+  m->coef_version++;
   HSB_CUDA(cudaStreamSynchronize(m->stream));
   return HSB_OK;
 }
