@@ -492,10 +492,13 @@ static int fast_interval_graphed(hsb_dev_model *m, const double *block_power, do
   int rc;
   if ((rc = rk4_fast_ready(m, &work, &fn))) return rc;
   const int want = block_temp_out != nullptr;
+  double *second = nullptr;
+  const long long *which = nullptr;
+  fast_state_buffers(m, work, &second, &which);
   hsb_dev_model::IvGraph *g = nullptr;
   for (auto &e : m->ivg)
-    if (e.exec && e.y == m->y && e.T == T && e.out == want && e.version == m->coef_version && e.fn == fn &&
-        e.mode == m->map_mode)
+    if (e.exec && e.y == m->y && e.y2 == second && e.T == T && e.out == want && e.version == m->coef_version &&
+        e.fn == fn && e.mode == m->map_mode)
       g = &e;
   if (!g) {
     g = &m->ivg[m->ivg_next];
@@ -514,9 +517,6 @@ static int fast_interval_graphed(hsb_dev_model *m, const double *block_power, do
     void *w2 = nullptr;
     ok = ok && rk4_fast_interval_begin(m, T, &scratch, &w2, m->blk_in) == HSB_OK;
     if (ok && want) {
-      double *second;
-      const long long *which;
-      fast_state_buffers(m, w2, &second, &which);
       ok = g2b_select(m, m->y, second, which, m->blk_out) == HSB_OK &&
            cudaMemcpyAsync(m->h_blk + nb, m->blk_out, sizeof(double) * nb, cudaMemcpyDeviceToHost, m->stream) ==
                cudaSuccess;
@@ -532,6 +532,7 @@ static int fast_interval_graphed(hsb_dev_model *m, const double *block_power, do
     }
     cudaGraphDestroy(graph);
     g->y = m->y;
+    g->y2 = second;
     g->T = T;
     g->out = want;
     g->version = m->coef_version;

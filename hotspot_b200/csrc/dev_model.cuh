@@ -96,10 +96,10 @@ struct hsb_dev_model {
   long long trace_cap;
   double *h_blk;                 // pinned staging: [0, nb) block powers in, [nb, 2 nb) block temperatures out
   cudaEvent_t ev[2];             // call timing events
-  // the fast-form interval as CUDA graphs, one per (state buffer in the
-  // state role, step, output request, coefficient version, kernel, g2b mode)
+  // the fast-form interval as CUDA graphs, one per (state buffers in their
+  // roles, step, output request, coefficient version, kernel, g2b mode)
   struct IvGraph {
-    const double *y;
+    const double *y, *y2;          // the two state buffers, in their roles at capture
     double T;
     int out, version, mode;
     const void *fn;

@@ -180,3 +180,25 @@ def test_trace_equals_single_intervals(workdir, builder):
     assert np.array_equal(a.grid("trans"), b.grid("trans"))
     a.close()
     b.close()
+
+
+def test_forms_alternate_on_one_model(workdir):
+    """Switching one model between the parity and the fast forms from call to
+    call: each form keeps its own state buffers and swaps them as steps are
+    accepted, so the fast form's replayed interval graphs must follow the
+    buffers' current roles.  The trajectory stays within 0.01 K of the FP64
+    replay."""
+    from hotspot_b200 import FORM_PARITY
+    sc = W.scenario_chip2d(workdir, seed=71, grid=32, steps=12)
+    m, o = hm.from_scenario(sc), OracleModel(sc)
+    t, to = m.vector(o.init_temp), o.vector(o.init_temp)
+    forms = [FORM_FAST, FORM_FAST, FORM_PARITY, FORM_FAST, FORM_FAST, FORM_PARITY, FORM_PARITY, FORM_FAST,
+             FORM_FAST, FORM_FAST, FORM_PARITY, FORM_FAST]
+    for k, form in enumerate(forms):
+        m.set_solver(form)
+        p = m.power_vector(sc.block_power[k])
+        m.compute_temp(p.copy(), t if k == 0 else None, sc.dt)
+        o.compute_temp(p.copy(), to if k == 0 else None, sc.dt)
+        assert np.max(np.abs(t - to)) <= TOL, k
+    assert np.max(np.abs(m.grid("trans") - o.grid("trans"))) <= TOL
+    m.close()
