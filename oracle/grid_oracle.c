@@ -2,7 +2,7 @@
  * grid_oracle.c -- TEST INFRASTRUCTURE ONLY.
  *
  * CPU restatement, in plain C99, of the numerical core of HotSpot's grid
- * model, used as the checker of libhotspot_b200 in tests/, smoke() and the
+ * model, used as the test oracle of libhotspot_b200 in tests/, smoke() and the
  * CPU-baseline leg of bench.py.  It follows the reference's loops literally:
  * lexicographic (n, i, j) sweeps, the same association of every sum, no FMA
  * (-ffp-contract=off), so that on identical inputs it reproduces the

@@ -1,5 +1,5 @@
 /* grid_oracle.h -- TEST INFRASTRUCTURE ONLY: CPU restatement of the HotSpot
- * grid-model numerics used as the checker of libhotspot_b200.  Never linked
+ * grid-model numerics used as the test oracle of libhotspot_b200.  Never linked
  * into, or called by, the product. */
 #ifndef GRID_ORACLE_H
 #define GRID_ORACLE_H

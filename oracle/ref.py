@@ -3,7 +3,7 @@
 ``oracle/_ref/libhsref.so`` is the reference's own C sources (compiled where
 they lie by ``make -C oracle ref``) plus ``oracle/ref_harness.c``.  Only the
 tests, ``__graft_entry__.smoke`` and ``bench.py``'s CPU-baseline leg load it,
-and only as the checker / the timed reference arm.  It does not exist unless
+and only as the oracle / the timed reference arm.  It does not exist unless
 the reference sources were present when it was built; callers check
 ``available()`` first.
 """

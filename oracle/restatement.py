@@ -1,6 +1,6 @@
 """CPU restatement of HotSpot's grid model -- TEST INFRASTRUCTURE ONLY.
 
-The checker of libhotspot_b200: only ``tests/``, ``__graft_entry__.smoke``
+The test oracle of libhotspot_b200: only ``tests/``, ``__graft_entry__.smoke``
 and ``bench.py``'s CPU-baseline leg import this module, never the product.
 
 Model set-up runs here in Python (executed once per model, small sizes): the

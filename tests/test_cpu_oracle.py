@@ -1,7 +1,7 @@
 """The oracle, pinned: the CPU restatement must reproduce the reference's
 results exactly (bit for bit) on the golden vectors generated from the
 reference build, and on fresh seeds against the live reference build when
-it is present.  The sparse direct steady solve (the converged-FP64 checker
+it is present.  The sparse direct steady solve (the converged-FP64 oracle
 of the fast steady forms) is pinned against the reference's own
 Gauss-Seidel iterated to convergence."""
 import glob
@@ -84,7 +84,7 @@ def test_direct_steady_matches_converged_reference_gs(workdir):
 def test_reference_steady_stops_short_of_convergence(workdir):
     """The reference's stopping rule (per-sweep change < 1e-6 K) leaves it
     ~1e-4..1e-3 K from the converged fixed point: the reason the fast forms
-    are judged against the converged solution, not the replay."""
+    are checked against the converged solution, not the replay."""
     sc = W.scenario_chip2d(workdir, seed=8, grid=32, steps=2)
     o = OracleModel(sc)
     avg = o.power_vector(sc.block_power.mean(0))

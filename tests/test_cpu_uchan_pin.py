@@ -1,7 +1,7 @@
-"""Pinning the microchannel steady checker.
+"""Pinning the microchannel steady oracle.
 
 The reference solves the steady state of a microchannel model only through
-SuperLU (absent here), so the FP64 checker of the BiCGStab solver is the
+SuperLU (absent here), so the FP64 oracle of the BiCGStab solver is the
 restated system G T = P solved by sparse LU.  It is pinned to the
 reference's own model: the reference's slope function (slope_fn_grid,
 temperature_grid.c:3130-3601, run from the reference build) vanishes at the
