@@ -200,6 +200,9 @@ _SIGS = {
     "hsb_grid_get_stats": (C.c_int, [_GM, C.POINTER(Stats)]),
     "hsb_grid_get_state": (C.c_int, [_GM, C.c_int, _D]),
     "hsb_grid_set_state": (C.c_int, [_GM, C.c_int, _D]),
+    "hsb_grid_save_state": (C.c_int, [_GM, C.c_char_p]),
+    "hsb_grid_load_state": (C.c_int, [_GM, C.c_char_p]),
+    "hsb_format_grid_rows": (C.c_longlong, [_D, C.c_longlong, C.c_char_p, C.c_longlong]),
     "hsb_grid_sync_host": (C.c_int, [_GM]),
     "hsb_grid_alloc": (C.c_int, [C.POINTER(_GM), C.POINTER(ThermalConfig), C.POINTER(Flp),
                                  C.POINTER(MicrochannelConfig), C.POINTER(MaterialsList), C.c_int, C.c_int]),

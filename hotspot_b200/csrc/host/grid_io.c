@@ -2,6 +2,8 @@
  * Formats and messages follow the reference functions cited per function;
  * the grid dumps read the state resident on the device. */
 #define _GNU_SOURCE
+#include <math.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -77,10 +79,171 @@ static int layer_prefix(const grid_model_t *m, int n, char *str)
   return 0;
 }
 
+/* ------------------------------------------------------------------------
+ * Grid dump rows, "%d\t%.2f\n" per cell, without printf per value.
+ *
+ * A value v in [0, 1e7) is rounded to hundredths from x = v * 100: the
+ * product's rounding error is below 1e-7 there, so when x is at least 1e-6
+ * away from a rounding tie (x - floor(x) = 0.5) the nearest integer to x is
+ * the nearest integer to the exact 100 v, which is what printf's correctly
+ * rounded "%.2f" prints.  Other values (near ties, negative, large, inf,
+ * nan) go through snprintf.  The output is byte-identical to the reference's
+ * fprintf loop.
+ * ------------------------------------------------------------------------ */
+#define GRID_ROW_MAX 400   /* bytes one row can take (an index and any double) */
+
+static char *put_uint(char *p, unsigned long long u)
+{
+  char t[24];
+  int k = 0;
+  do {
+    t[k++] = (char)('0' + u % 10);
+    u /= 10;
+  } while (u);
+  while (k) *p++ = t[--k];
+  return p;
+}
+
+static char *put_value(char *p, double v)
+{
+  if (!signbit(v) && v < 1e7) {   /* -0.0 prints as "-0.00": snprintf */
+    const double x = v * 100.0, fl = floor(x), fr = x - fl;
+    if (fabs(fr - 0.5) >= 1e-6) {
+      const unsigned long long q = (unsigned long long)fl + (fr > 0.5 ? 1u : 0u);
+      p = put_uint(p, q / 100);
+      *p++ = '.';
+      *p++ = (char)('0' + (q % 100) / 10);
+      *p++ = (char)('0' + q % 10);
+      return p;
+    }
+  }
+  return p + snprintf(p, GRID_ROW_MAX - 16, "%.2f", v);
+}
+
+long long hsb_format_grid_rows(const double *v, long long n, char *out, long long cap)
+{
+  if (n < 0 || !out || (n && !v)) return HSB_E_ARG;
+  if (cap < n * GRID_ROW_MAX) return HSB_E_ARG;
+  char *p = out;
+  for (long long k = 0; k < n; k++) {
+    p = put_uint(p, (unsigned long long)k);
+    *p++ = '\t';
+    p = put_value(p, v[k]);
+    *p++ = '\n';
+  }
+  return (long long)(p - out);
+}
+
+/* the "Layer %d:" blocks of a grid vector, rows formatted in chunks */
+static int write_grid_layers(FILE *fp, const grid_model_t *model, const grid_model_vector_t *g)
+{
+  const long long plane = (long long)model->rows * model->cols, chunk = 8192;
+  char *buf = malloc((size_t)(chunk * GRID_ROW_MAX));
+  if (!buf) return hsb_seterr(HSB_E_NOMEM, "memory allocation error\n");
+  for (int l = 0; l < model->n_layers; l++) {
+    fprintf(fp, "Layer %d:\n", l);
+    const double *base = &g->cuboid[l][0][0];
+    for (long long k0 = 0; k0 < plane; k0 += chunk) {
+      const long long k = plane - k0 < chunk ? plane - k0 : chunk;
+      char *p = buf;
+      for (long long q = 0; q < k; q++) {   /* the row index runs over the whole plane */
+        p = put_uint(p, (unsigned long long)(k0 + q));
+        *p++ = '\t';
+        p = put_value(p, base[k0 + q]);
+        *p++ = '\n';
+      }
+      fwrite(buf, 1, (size_t)(p - buf), fp);
+    }
+  }
+  free(buf);
+  return HSB_OK;
+}
+
+/* ------------------------------------------------------------------------
+ * Binary checkpoint of the grid state (no counterpart in the reference):
+ * an 8-byte magic, the layer/row/column/extra-node counts (int32), the
+ * vector length (int64), then the transient and the steady grid vectors
+ * (FP64, native byte order).
+ * ------------------------------------------------------------------------ */
+static const char STATE_MAGIC[8] = {'H', 'S', 'B', 'G', 'R', 'I', 'D', '1'};
+
+typedef struct {
+  char magic[8];
+  int32_t layers, rows, cols, extra;
+  int64_t vlen;
+} state_header_t;
+
+static void state_header(const grid_model_t *m, state_header_t *h)
+{
+  memset(h, 0, sizeof(*h));
+  memcpy(h->magic, STATE_MAGIC, sizeof(STATE_MAGIC));
+  h->layers = m->n_layers;
+  h->rows = m->rows;
+  h->cols = m->cols;
+  h->extra = n_extra(m);
+  h->vlen = (int64_t)m->n_layers * m->rows * m->cols + h->extra;
+}
+
+int hsb_grid_save_state(grid_model_t *model, const char *path)
+{
+  if (!model || !path) return hsb_seterr(HSB_E_ARG, "null argument\n");
+  state_header_t h;
+  state_header(model, &h);
+  double *v = malloc(sizeof(double) * (size_t)h.vlen * 2);
+  if (!v) return hsb_seterr(HSB_E_NOMEM, "memory allocation error\n");
+  int rc = hsb_grid_get_state(model, 0, v);
+  if (!rc) rc = hsb_grid_get_state(model, 1, v + h.vlen);
+  if (rc) {
+    free(v);
+    return rc;
+  }
+  FILE *fp = fopen(path, "wb");
+  if (!fp) {
+    free(v);
+    return hsb_seterr(HSB_E_ARG, "unable to open %s for writing\n", path);
+  }
+  const int ok = fwrite(&h, sizeof(h), 1, fp) == 1 && fwrite(v, sizeof(double), (size_t)h.vlen * 2, fp) ==
+                 (size_t)h.vlen * 2;
+  free(v);
+  if (fclose(fp) != 0 || !ok) return hsb_seterr(HSB_E_ARG, "error writing %s\n", path);
+  return HSB_OK;
+}
+
+int hsb_grid_load_state(grid_model_t *model, const char *path)
+{
+  if (!model || !path) return hsb_seterr(HSB_E_ARG, "null argument\n");
+  state_header_t want, h;
+  state_header(model, &want);
+  FILE *fp = fopen(path, "rb");
+  if (!fp) return hsb_seterr(HSB_E_ARG, "unable to open %s for reading\n", path);
+  if (fread(&h, sizeof(h), 1, fp) != 1 || memcmp(h.magic, STATE_MAGIC, sizeof(STATE_MAGIC))) {
+    fclose(fp);
+    return hsb_seterr(HSB_E_ARG, "%s is not a grid-state checkpoint\n", path);
+  }
+  if (h.layers != want.layers || h.rows != want.rows || h.cols != want.cols || h.extra != want.extra ||
+      h.vlen != want.vlen) {
+    fclose(fp);
+    return hsb_seterr(HSB_E_ARG, "checkpoint %s holds a %dx%dx%d grid with %d extra nodes; the model has "
+                                 "%dx%dx%d with %d\n", path, h.layers, h.rows, h.cols, h.extra, want.layers,
+                      want.rows, want.cols, want.extra);
+  }
+  double *v = malloc(sizeof(double) * (size_t)h.vlen * 2);
+  if (!v) {
+    fclose(fp);
+    return hsb_seterr(HSB_E_NOMEM, "memory allocation error\n");
+  }
+  const size_t got = fread(v, sizeof(double), (size_t)h.vlen * 2, fp);
+  fclose(fp);
+  int rc = got == (size_t)h.vlen * 2 ? HSB_OK : hsb_seterr(HSB_E_ARG, "%s is truncated\n", path);
+  if (!rc) rc = hsb_grid_set_state(model, 0, v);
+  if (!rc) rc = hsb_grid_set_state(model, 1, v + h.vlen);
+  free(v);
+  return rc;
+}
+
 /* temperature_grid.c:1262-1295 */
 void dump_steady_temp_grid(grid_model_t *model, char *file)
 {
-  int i, j, n;
   FILE *fp;
   if (!model->r_ready) {
     hsb_seterr(HSB_E_ARG, "R model not ready\n");
@@ -89,12 +252,7 @@ void dump_steady_temp_grid(grid_model_t *model, char *file)
   if (hsb_grid_sync_host(model)) hsb_die();
   fp = open_out(file);
   if (!fp) die_open("error: %s could not be opened for writing\n", file);
-  for (n = 0; n < model->n_layers; n++) {
-    fprintf(fp, "Layer %d:\n", n);
-    for (i = 0; i < model->rows; i++)
-      for (j = 0; j < model->cols; j++)
-        fprintf(fp, "%d\t%.2f\n", i * model->cols + j, model->last_steady->cuboid[n][i][j]);
-  }
+  if (write_grid_layers(fp, model, model->last_steady)) hsb_die();
   close_out(fp);
 }
 
@@ -105,12 +263,7 @@ void dump_transient_temp_grid(grid_model_t *model, int trace_num, double samplin
   if (!fp) die_open("Unable to open %s for appending\n", filename);
   if (hsb_grid_sync_host(model)) hsb_die();
   fprintf(fp, "t = %lf\n", trace_num * sampling_intvl);
-  for (int l = 0; l < model->n_layers; l++) {
-    fprintf(fp, "Layer %d:\n", l);
-    for (int i = 0; i < model->rows; i++)
-      for (int j = 0; j < model->cols; j++)
-        fprintf(fp, "%d\t%.2f\n", i * model->cols + j, model->last_trans->cuboid[l][i][j]);
-  }
+  if (write_grid_layers(fp, model, model->last_trans)) hsb_die();
   fclose(fp);
 }
 

@@ -212,6 +212,18 @@ class RCModel:
         check(lib().hsb_grid_get_state(self.ptr, 0 if which == "trans" else 1, dptr(out)))
         return out
 
+    def save_state(self, path: str):
+        """Binary checkpoint of both grid vectors (hsb_grid_save_state)."""
+        check(lib().hsb_grid_save_state(self.ptr, str(path).encode()))
+
+    def load_state(self, path: str):
+        """Restore a checkpoint written by save_state on a model of the same grid."""
+        check(lib().hsb_grid_load_state(self.ptr, str(path).encode()))
+
+    def dump_transient(self, trace_num: int, sampling_intvl: float, path: str):
+        """Append the transient grid as dump_transient_temp_grid does."""
+        lib().dump_transient_temp_grid(self.ptr, int(trace_num), float(sampling_intvl), str(path).encode())
+
     def set_grid(self, which: str, v: np.ndarray):
         v = np.ascontiguousarray(v, dtype=np.float64)
         check(lib().hsb_grid_set_state(self.ptr, 0 if which == "trans" else 1, dptr(v)))

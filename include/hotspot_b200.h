@@ -103,6 +103,18 @@ int hsb_grid_get_state(grid_model_t *model, int which, double *out);
 int hsb_grid_set_state(grid_model_t *model, int which, const double *in);
 /* refresh model->last_trans / last_steady host copies from the device */
 int hsb_grid_sync_host(grid_model_t *model);
+/* Binary checkpoint of the grid state: both grid vectors (transient and
+ * steady) with the grid's dimensions, so that a run can stop and resume on
+ * another model of the same grid.  No counterpart in the reference (its
+ * only state output is the text dumps below).  Load refuses a checkpoint
+ * whose dimensions differ from the model's. */
+int hsb_grid_save_state(grid_model_t *model, const char *path);
+int hsb_grid_load_state(grid_model_t *model, const char *path);
+/* The rows "%d\t%.2f\n" (index, value) of n grid cells, as the grid dumps
+ * print them (dump_steady_temp_grid / dump_transient_temp_grid,
+ * temperature_grid.c:1262-1319), byte for byte, without a printf per value;
+ * out must hold 400 bytes per cell.  Returns the bytes written or HSB_E_ARG. */
+long long hsb_format_grid_rows(const double *values, long long n, char *out, long long cap);
 /* status-returning forms of alloc / populate / compute / steady */
 int hsb_grid_alloc(grid_model_t **out, thermal_config_t *config, flp_t *flp_default,
                    microchannel_config_t *uconf, materials_list_t *ml, int do_detailed_3D,
