@@ -40,3 +40,26 @@ def test_cli_outputs_identical(workdir, grid, seed):
         a = open(os.path.join(workdir, f"ref.{o}"), "rb").read()
         b = open(os.path.join(workdir, f"gpu.{o}"), "rb").read()
         assert len(a) > 0 and a == b, o
+
+
+@pytest.mark.skipif(not (os.path.exists(REF_BIN) and os.path.exists(DROPIN_BIN)),
+                    reason="reference build not present (make -C oracle ref dropin)")
+@pytest.mark.parametrize("detailed", ["off", "on"])
+def test_cli_layer_stack_identical(workdir, detailed):
+    """The 4-layer stack from a layer configuration file, with uniform and
+    with detailed (per-cell) R/C assignment."""
+    sc = W.scenario_stack3d(workdir, seed=93, grid=32, steps=10, n_blocks=10)
+    ptrace = W.write_ptrace(os.path.join(workdir, "p.ptrace"), sc.power_layers[0] + sc.power_layers[2],
+                            sc.block_power)
+    flp0 = sc.lcf.replace(".lcf", "_si0.flp")
+    env = {k: v for k, v in os.environ.items() if k != "HOTSPOT_B200_FORM"}
+    for tag, exe in (("ref", REF_BIN), ("gpu", DROPIN_BIN)):
+        args = [exe, "-f", flp0, "-p", ptrace, "-o", f"{tag}.ttrace", "-model_type", "grid", "-grid_rows", "32",
+                "-grid_cols", "32", "-sampling_intvl", "1e-05", "-grid_layer_file", sc.lcf, "-detailed_3D", detailed,
+                "-steady_file", f"{tag}.steady", "-grid_steady_file", f"{tag}.grid.steady"]
+        r = subprocess.run(args, cwd=workdir, capture_output=True, text=True, timeout=600, env=env)
+        assert r.returncode == 0, (tag, r.stdout[-2000:], r.stderr[-2000:])
+    for o in ("ttrace", "steady", "grid.steady"):
+        a = open(os.path.join(workdir, f"ref.{o}"), "rb").read()
+        b = open(os.path.join(workdir, f"gpu.{o}"), "rb").read()
+        assert len(a) > 0 and a == b, o
