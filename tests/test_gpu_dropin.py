@@ -4,7 +4,8 @@
 object but temperature_grid.o, against libhotspot_b200 -- what a HotSpot user
 does to put the GPU under the grid model (oracle/_ref/hotspot_b200drv).  The
 reference's own build of the same sources is oracle/_ref/hotspot.  Both run
-the same floorplan and power trace; in the default (parity) form every output
+the same floorplan and power trace (also with the secondary heat path,
+-model_secondary 1); in the default (parity) form every output
 file -- the block transient trace, the steady block temperatures and the grid
 dumps of the steady and of every transient interval -- must be identical,
 byte for byte."""
@@ -23,8 +24,8 @@ DROPIN_BIN = os.path.join(HERE, "..", "oracle", "_ref", "hotspot_b200drv")
 
 @pytest.mark.skipif(not (os.path.exists(REF_BIN) and os.path.exists(DROPIN_BIN)),
                     reason="reference build not present (make -C oracle ref dropin)")
-@pytest.mark.parametrize("grid,seed", [(32, 91), (64, 92)])
-def test_cli_outputs_identical(workdir, grid, seed):
+@pytest.mark.parametrize("grid,seed,extra", [(32, 91, []), (64, 92, []), (32, 94, ["-model_secondary", "1"])])
+def test_cli_outputs_identical(workdir, grid, seed, extra):
     sc = W.scenario_chip2d(workdir, seed=seed, grid=grid, steps=20)
     ptrace = W.write_ptrace(os.path.join(workdir, "p.ptrace"), sc.power_layers[0], sc.block_power)
     outs = ("ttrace", "steady", "grid.steady", "grid.ttrace")
@@ -33,7 +34,7 @@ def test_cli_outputs_identical(workdir, grid, seed):
         args = [exe, "-f", sc.flp, "-p", ptrace, "-o", f"{tag}.ttrace", "-model_type", "grid",
                 "-grid_rows", str(grid), "-grid_cols", str(grid), "-sampling_intvl", "3.333e-06",
                 "-steady_file", f"{tag}.steady", "-grid_steady_file", f"{tag}.grid.steady",
-                "-grid_transient_file", f"{tag}.grid.ttrace"]
+                "-grid_transient_file", f"{tag}.grid.ttrace"] + extra
         r = subprocess.run(args, cwd=workdir, capture_output=True, text=True, timeout=600, env=env)
         assert r.returncode == 0, (tag, r.stdout[-2000:], r.stderr[-2000:])
     for o in outs:
