@@ -83,6 +83,23 @@ except _abi.HotspotError as e:
     assert rc == 3 and "no CUDA device" in out
 
 
+DROPIN_BIN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "oracle", "_ref", "hotspot_b200drv")
+
+
+@pytest.mark.skipif(not os.path.exists(DROPIN_BIN), reason="drop-in CLI not built (make -C oracle dropin)")
+def test_dropin_cli_fails_loudly_without_gpu(workdir):
+    """HotSpot's own CLI linked against this library stops with the library's
+    fatal() message when no GPU is visible: there is no CPU path."""
+    from conftest import has_gpu
+    if has_gpu():
+        pytest.skip("a GPU is visible")
+    sc = W.scenario_chip2d(workdir, seed=0, grid=16, steps=2)
+    ptrace = W.write_ptrace(os.path.join(workdir, "p.ptrace"), sc.power_layers[0], sc.block_power)
+    r = subprocess.run([DROPIN_BIN, "-f", sc.flp, "-p", ptrace, "-model_type", "grid", "-grid_rows", "16",
+                        "-grid_cols", "16"], cwd=workdir, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1 and "no CUDA device" in r.stdout + r.stderr
+
+
 def test_status_api_reports_instead_of_exiting(workdir):
     rc, out = _child(PRELUDE + f"""
 sc = W.scenario_chip2d({workdir!r}, seed=0, grid=16, steps=1)
