@@ -64,3 +64,22 @@ def test_cli_layer_stack_identical(workdir, detailed):
         a = open(os.path.join(workdir, f"ref.{o}"), "rb").read()
         b = open(os.path.join(workdir, f"gpu.{o}"), "rb").read()
         assert len(a) > 0 and a == b, o
+
+
+@pytest.mark.skipif(not (os.path.exists(REF_BIN) and os.path.exists(DROPIN_BIN)),
+                    reason="reference build not present (make -C oracle ref dropin)")
+def test_cli_leakage_loop_identical(workdir):
+    """The reference's temperature-leakage fixed point (temperature.c:708-746),
+    a host loop of steady solves, over this library's steady solver."""
+    sc = W.scenario_chip2d(workdir, seed=95, grid=32, steps=4)
+    ptrace = W.write_ptrace(os.path.join(workdir, "p.ptrace"), sc.power_layers[0], sc.block_power)
+    env = {k: v for k, v in os.environ.items() if k != "HOTSPOT_B200_FORM"}
+    for tag, exe in (("ref", REF_BIN), ("gpu", DROPIN_BIN)):
+        args = [exe, "-f", sc.flp, "-p", ptrace, "-model_type", "grid", "-grid_rows", "32", "-grid_cols", "32",
+                "-leakage_used", "1", "-steady_file", f"{tag}.steady", "-grid_steady_file", f"{tag}.grid.steady"]
+        r = subprocess.run(args, cwd=workdir, capture_output=True, text=True, timeout=600, env=env)
+        assert r.returncode == 0, (tag, r.stdout[-2000:], r.stderr[-2000:])
+    for o in ("steady", "grid.steady"):
+        a = open(os.path.join(workdir, f"ref.{o}"), "rb").read()
+        b = open(os.path.join(workdir, f"gpu.{o}"), "rb").read()
+        assert len(a) > 0 and a == b, o
