@@ -77,10 +77,8 @@ def parse():
 
 
 def dist():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from hotspot_b200 import replicas
+    return replicas.world()
 
 
 class Clocks:
@@ -395,7 +393,7 @@ def leg_serving(args):
 
 def run_ours(args):
     import torch
-    from hotspot_b200 import FORM_FAST, FORM_PARITY, _abi
+    from hotspot_b200 import FORM_FAST, FORM_PARITY, _abi, replicas
     from hotspot_b200 import model as hm
     from hotspot_b200 import workloads as W
 
@@ -461,16 +459,7 @@ def run_ours(args):
         return
 
     # max over ranks of the device time; whole-job cell-steps
-    tot = np.array([dev_ms, ncell * steps_total, ker_ms], dtype=np.float64)
-    if pg:
-        t = torch.tensor(tot, device="cuda")
-        mx = t.clone()
-        pg.all_reduce(mx, op=pg.ReduceOp.MAX)
-        sm = t.clone()
-        pg.all_reduce(sm, op=pg.ReduceOp.SUM)
-        dev_ms_max, cell_steps_all = float(mx[0]), float(sm[1])
-    else:
-        dev_ms_max, cell_steps_all = dev_ms, float(ncell * steps_total)
+    dev_ms_max, cell_steps_all = replicas.reduce_timing(dev_ms, float(ncell * steps_total), pg, "cuda")
     value = cell_steps_all / (dev_ms_max / 1e3)
 
     # ---- e2e: the C-ABI call with host buffers (copies inside), wall clock ----
@@ -486,13 +475,8 @@ def run_ours(args):
         e2e_steps += m.stats()["rk4_steps"]
     barrier()
     e2e_s = time.perf_counter() - t0
-    if pg:
-        t = torch.tensor([e2e_s, ncell * e2e_steps], device="cuda", dtype=torch.float64)
-        mx = t.clone(); pg.all_reduce(mx, op=pg.ReduceOp.MAX)
-        sm = t.clone(); pg.all_reduce(sm, op=pg.ReduceOp.SUM)
-        e2e_value = float(sm[1]) / float(mx[0])
-    else:
-        e2e_value = ncell * e2e_steps / e2e_s
+    e2e_max, e2e_work = replicas.reduce_timing(e2e_s, float(ncell * e2e_steps), pg, "cuda")
+    e2e_value = e2e_work / e2e_max
 
     # ---- the same intervals as one multi-interval call (one persistent launch,
     # no host round trip between intervals; block powers copied in inside)

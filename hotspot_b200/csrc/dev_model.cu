@@ -750,6 +750,12 @@ int hsb_dev_get_state(hsb_dev_model *m, int which, double *out) {
   return HSB_OK;
 }
 
+int hsb_dev_workspaces(const hsb_dev_model *m, int *mask) {
+  if (!m || !mask) return set_error(HSB_E_ARG, "null argument");
+  *mask = (m->fast ? HSB_WS_FAST_TRANSIENT : 0) | (m->mg ? HSB_WS_MG : 0) | (m->krylov ? HSB_WS_BICGSTAB : 0);
+  return HSB_OK;
+}
+
 int hsb_dev_set_state(hsb_dev_model *m, int which, const double *in) {
   if (!m || !in) return set_error(HSB_E_ARG, "null argument");
   HSB_CUDA(cudaMemcpyAsync(which ? m->ys : m->y, in, sizeof(double) * m->vlen,

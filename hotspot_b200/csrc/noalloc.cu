@@ -52,7 +52,10 @@ static __device__ __align__(256) unsigned char hsb_noalloc_scratch[kTotal];
 namespace {
 
 std::mutex g_mu;
-void *g_addr[256];   // device address of the scratch, per device ordinal
+// device address of the scratch, per device ordinal, kept for the life of the
+// process: a cudaDeviceReset (which may reload the module elsewhere) is not
+// supported while the library is loaded
+void *g_addr[256];
 
 // once per device, with that device current
 int scratch_address(int dev, unsigned char **out) {

@@ -148,10 +148,18 @@ int hsb_dev_transient_trace(hsb_dev_model *m, const double *block_powers, int K,
  * HSB_NOALLOC_MAX_CELLS cells, 4096 rows and 16384 columns, with per-layer
  * conductances; larger, more elongated or
  * per-cell (detailed 3-D, microchannel) models are rejected with
- * HSB_E_ARG.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress), so make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race.
- * Call with the model's device current. */
+ * HSB_E_ARG.
+ *   Ordering: y and pgrid are read on the model's stream, so whatever
+ * wrote them must be complete before the call -- written on that stream, or
+ * finished by a host synchronisation or an event the stream waited on.
+ *   Blocking: the call waits on the host until the interval is done (it
+ * reads the step counters back), so it must never be issued on a stream
+ * that is being captured into a CUDA graph.
+ *   The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and keeps it for the life of the process, so
+ * cudaDeviceReset is not supported while the library is loaded.  All calls
+ * share the array: calls that overlap on the GPU race.  Call with the
+ * model's device current. */
 #define HSB_NOALLOC_MAX_CELLS 65536
 int hsb_dev_transient_noalloc(hsb_dev_model *m, double *y, const double *pgrid,
                               double time_elapsed, hsb_stats *st);
@@ -228,6 +236,14 @@ int  hsb_server_set_priority(hsb_server *s, int model, int high);
 /* run the model's work on a high-priority (high = 1) or normal stream; call
  * with no work of the model in flight */
 int hsb_dev_set_priority(hsb_dev_model *m, int high);
+
+/* which of the model's solver workspaces exist (no counterpart in the
+ * reference): the fast transient, MG-PCG and BiCGStab solvers allocate
+ * theirs on their first call; *mask = OR of HSB_WS_* */
+#define HSB_WS_FAST_TRANSIENT 1
+#define HSB_WS_MG             2
+#define HSB_WS_BICGSTAB       4
+int hsb_dev_workspaces(const hsb_dev_model *m, int *mask);
 
 /* which: 0 = transient state (last_trans), 1 = steady state (last_steady);
  * n = nl*nr*nc + n_extra doubles */

@@ -14,7 +14,7 @@ from hotspot_b200 import _abi
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INCLUDE = os.path.join(ROOT, "include")
-REFERENCE_SRC = "/root/reference"
+REFERENCE_SRC = os.environ.get("HOTSPOT_REFERENCE_SRC", "/root/reference")
 
 
 def _declared_functions():

@@ -5,12 +5,19 @@ that reserves its GPU memory at start-up, a real-time loop that cannot take
 cudaMalloc's implicit synchronisation) get one more C entry point that runs
 the fast transient form with its temporaries in a static device array.
 This test calls it through the C-ABI on a state and power vectors held in
-device memory, twice in a row, and checks each result against the regular
-entry point (compute_temp with the stage-by-stage fast form, the arithmetic
-the allocation-free entry point runs) within the parity tolerance used by the
-GPU tests.  It lives in its own file so a
-run that stops at the first failure has run every other test first; it
-passes alone in a fresh process and after the other tests.
+device memory, twice in a row, and checks each result
+  * against the regular entry point (compute_temp with the stage-by-stage
+    fast form, the arithmetic the allocation-free entry point runs), within
+    the parity tolerance used by the GPU tests, and
+  * against the FP64 oracle (the reference's arithmetic), within the fast
+    form's 0.01 K bar,
+on models that exercise the static scratch's sizing: a 2-D chip, the
+secondary heat path (28 package nodes), a 6-layer stack, and a rectangular
+grid of exactly HSB_NOALLOC_MAX_CELLS cells.  It also checks the defining
+property: the model it ran on never allocated a fast-transient workspace.
+It lives in its own file so a run that stops at the first failure has run
+every other test first; it passes alone in a fresh process and after the
+other tests.
 """
 import ctypes as C
 
@@ -24,16 +31,36 @@ from oracle.restatement import OracleModel
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-6
+TOL_FP64 = 0.01
+MAX_CELLS = 65536
 
 
-def test_noalloc_matches_regular_entry(workdir):
+def _scenario(workdir, case):
+    if case == "chip2d":
+        return W.scenario_chip2d(workdir, seed=31, grid=64, steps=3)
+    if case == "secondary":
+        sc = W.scenario_chip2d(workdir, seed=33, grid=32, steps=3)
+        sc.config["model_secondary"] = "1"
+        return sc
+    if case == "stack":
+        return W.scenario_stack3d(workdir, seed=34, grid=64, steps=3, n_blocks=12)
+    # rectangular: 4 layers x 64 x 256 = the scratch's maximum cell count
+    sc = W.scenario_chip2d(workdir, seed=35, grid=64, steps=3)
+    sc.config["grid_cols"] = "256"
+    return sc
+
+
+@pytest.mark.parametrize("case", ["chip2d", "secondary", "stack", "max_cells"])
+def test_noalloc_matches_regular_entry(workdir, case):
     import torch
 
-    sc = W.scenario_chip2d(workdir, seed=31, grid=64, steps=3)
+    sc = _scenario(workdir, case)
     L = _abi.lib()
 
     # regular entry point: the stage-by-stage fast form through compute_temp
     a = hm.from_scenario(sc)
+    if case == "max_cells":
+        assert a.n_cells == MAX_CELLS
     a.set_solver(FORM_FAST_STAGES)
     temp = a.vector(a.config.init_temp)
     p0 = a.power_vector(sc.block_power[0])
@@ -44,16 +71,25 @@ def test_noalloc_matches_regular_entry(workdir):
         a.compute_temp(a.power_vector(sc.block_power[k]).copy(), None, sc.dt)
         expected.append(a.grid("trans"))
 
+    # the oracle's FP64 replay of the reference from the same state
+    o = OracleModel(sc)
+    to = o.vector(o.init_temp)
+    o.compute_temp(o.power_vector(sc.block_power[0]), to, 0.0)
+    assert np.max(np.abs(o.grid("trans") - y0)) <= TOL
+    exact = []
+    for k in (1, 2):
+        o.compute_temp(o.power_vector(sc.block_power[k]), None, sc.dt)
+        exact.append(o.grid("trans"))
+
     # the same intervals through the allocation-free entry point
     b = hm.from_scenario(sc)
-    assert b.n_cells <= 65536
-    o = OracleModel(sc)                            # grid power vectors (bit-exact b2g)
+    assert b.n_cells <= MAX_CELLS
     dev = L.hsb_grid_device(b.ptr)
     y = torch.tensor(y0, dtype=torch.float64, device="cuda")
-    for k, exp in zip((1, 2), expected):
+    for k, exp, ex64 in zip((1, 2), expected, exact):
         pg = torch.tensor(o.b2g(b.power_vector(sc.block_power[k]).copy(), True), dtype=torch.float64,
                           device="cuda")
-        torch.cuda.synchronize()
+        torch.cuda.synchronize()        # y and pg are complete before the call reads them
         st = _abi.Stats()
         rc = L.hsb_dev_transient_noalloc(dev, C.c_void_p(y.data_ptr()), C.c_void_p(pg.data_ptr()),
                                          sc.dt, C.byref(st))
@@ -61,6 +97,10 @@ def test_noalloc_matches_regular_entry(workdir):
         assert st.rk4_steps >= 1
         got = y.cpu().numpy()
         assert np.max(np.abs(got - exp)) <= TOL
+        assert np.max(np.abs(got - ex64)) <= TOL_FP64
+    mask = C.c_int(-1)
+    assert L.hsb_dev_workspaces(dev, C.byref(mask)) == 0
+    assert mask.value & 1 == 0, "the allocation-free entry point allocated a fast-transient workspace"
     a.close()
     b.close()
 
