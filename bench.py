@@ -66,8 +66,9 @@ def parse():
     ap.add_argument("--headline-only", action="store_true", help="skip the batched / microchannel / serving legs")
     ap.add_argument("--profile-case", choices=["batch", "microchannel", "steady"], default=None,
                     help="small cases of the other kernels, for ncu captures (a few GB at most)")
+    ap.add_argument("--chip2d-rows", type=int, default=1000, help="rows of the 2-D chip leg's trace")
     ap.add_argument("--batch-chips", type=int, default=512)
-    ap.add_argument("--batch-intervals", type=int, default=10)
+    ap.add_argument("--batch-intervals", type=int, default=200)
     ap.add_argument("--serving-seconds", type=float, default=0.25,
                     help="length of the request arrival window of the serving leg at 2000 req/s")
     ap.add_argument("--serving-calm-rate", type=float, default=30.0,
@@ -228,8 +229,34 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # further legs (one GPU)
 # ---------------------------------------------------------------------------
+def cpu_batch_sample(scs, idx, dt):
+    """The reference's C code (oracle/_ref, else the oracle's restatement) on
+    one interval of each sampled chip, single-threaded: {chip: cell-steps/s}."""
+    from oracle import ref as R
+    from oracle.restatement import OracleModel
+    rates, kind = {}, "reference" if R.available() else "port"
+    for c in idx:
+        sc = scs[c]
+        o = R.RefModel(sc) if R.available() else OracleModel(sc)
+        to = o.vector(333.15)
+        o.compute_temp(o.power_vector(sc.block_power[0]), to, 0.0)
+        t0 = time.perf_counter()
+        o.compute_temp(o.power_vector(sc.block_power[1]), None, dt)
+        el = time.perf_counter() - t0
+        # the step count: the oracle replays the reference's step rule exactly
+        q = OracleModel(sc)
+        tq = q.vector(333.15)
+        q.compute_temp(q.power_vector(sc.block_power[0]), tq, 0.0)
+        steps = int(q.compute_temp(q.power_vector(sc.block_power[1]), None, dt))
+        rates[c] = q.n_cells * steps / el
+        if hasattr(o, "close"):
+            o.close()
+    return rates, kind
+
+
 def leg_batched(args, flush):
-    """512 synthetic chips advanced together by hsb_batch_transient."""
+    """512 synthetic chips advanced together: K intervals per persistent launch
+    of the temporally blocked kernel (hsb_batch_transient_trace)."""
     import torch
     from hotspot_b200 import FORM_FAST
     from hotspot_b200 import model as hm
@@ -239,7 +266,8 @@ def leg_batched(args, flush):
     rng = np.random.default_rng(2024)
     d = tempfile.mkdtemp(prefix="hsb_batch_")
     t0 = time.perf_counter()
-    scs = [W.scenario_random_chip(d, rng, f"c{i}", steps=K + 16) for i in range(args.batch_chips)]
+    tune_rows = 9
+    scs = [W.scenario_random_chip(d, rng, f"c{i}", steps=K + tune_rows + 2) for i in range(args.batch_chips)]
     models = []
     for sc in scs:
         m = hm.from_scenario(sc)
@@ -247,9 +275,9 @@ def leg_batched(args, flush):
         t = m.vector(m.config.init_temp)
         m.compute_temp(m.power_vector(sc.block_power[0]), t, 0.0)
         models.append(m)
-    setup_s = time.perf_counter() - t0
     cells = np.array([m.n_cells for m in models], dtype=np.float64)
     bt = Batch(models)
+    setup_s = time.perf_counter() - t0
     dt = scs[0].dt
 
     def pw(k):
@@ -259,20 +287,37 @@ def leg_batched(args, flush):
     for _ in range(len(bt.tuning())):      # the autotuner tries one candidate schedule per call
         bt.transient(pw(k), dt)
         k += 1
-    tuned = dict(bt.info(), candidates=len(bt.tuning()))
-    kms = cs = 0.0
-    launches = 0
-    for j in range(k, k + K):
-        flush.fill_(float(j))
-        torch.cuda.synchronize()
-        st = bt.transient(pw(j), dt)
-        kms += st["kernel_ms"]
-        launches += st["launches"]
-        cs += float(np.sum(bt.chip_steps() * cells))
+    tuned = dict(bt.info(), candidates=bt.tuning())
+    rows = [pw(k + j) for j in range(K)]
+    flush.fill_(2.0)
+    torch.cuda.synchronize()
+    st = bt.trace(rows, dt)
+    chip_steps = bt.chip_steps()
+    kms = st["kernel_ms"]
+    cs = float(np.sum(chip_steps * cells))
     rate = cs / (kms / 1e3)
     peak, peak_kind = measured_peak()
     achieved = ALG_BYTES_FP32 * rate / 1e9
+    tiles = {}
+    for c, m in enumerate(models):
+        tiles.setdefault(f"{m.rows}x{m.cols}", bt.tile(c))
     bt.close()
+    # CPU baseline: 8 chips stratified by grid side, one interval each on the
+    # reference's code, extrapolated to the batch by the drawn size mix
+    sides = [m.rows for m in models]
+    sample = []
+    for side in (512, 256, 128, 64, 32, 512, 256, 128):
+        cand = [c for c, s_ in enumerate(sides) if s_ == side and c not in sample]
+        if cand:
+            sample.append(cand[0])
+    rates, kind = cpu_batch_sample(scs, sample, dt)
+    by_side = {}
+    for c, r in rates.items():
+        by_side.setdefault(sides[c], []).append(r)
+    side_rate = {s_: float(np.mean(v)) for s_, v in by_side.items()}
+    cpu_time = sum(cells[c] * chip_steps[c] / side_rate.get(sides[c], min(side_rate.values()))
+                   for c in range(len(models)))
+    cpu_rate = cs / cpu_time
     # each chip's steady solve: all 512 at once through the serving loop, 16 in flight
     from hotspot_b200.serving import Request, Server
     from hotspot_b200 import _abi
@@ -289,18 +334,107 @@ def leg_batched(args, flush):
         m.close()
     return {"workload": f"{args.batch_chips} chips, sides 2^5..2^9, 1..8 chip layers + spreader/sink, "
                         "10..100 blocks, 3.333 us intervals", "cells": int(cells.sum()),
-            "cell_steps_per_s": rate, "intervals": K, "ms_per_interval": kms / K,
+            "cell_steps_per_s": rate, "intervals": K, "launches_timed": st["launches"],
+            "ms_per_interval": kms / K, "rk4_steps": int(chip_steps.sum()),
             "steady_solves_per_s": len(sreq) / steady_span,
             "steady_note": "every chip's steady solve (MG-PCG, FP64 refinement to 1e-5 K), all submitted at once to "
                            "the serving loop, 16 in flight on their own streams",
-            "schedule": tuned, "setup_s": setup_s, "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": "rk4_batch_kernel", "achieved": achieved, "peak": peak,
+            "schedule": tuned, "tiles_by_grid": tiles, "setup_s": setup_s,
+            "cpu_baseline": {"kind": kind, "cores": 1, "cell_steps_per_s": cpu_rate,
+                             "sample": f"{len(sample)} chips stratified by side, one interval each, "
+                                       "extrapolated to the batch's size mix and step counts",
+                             "rates_by_side": side_rate},
+            "roofline": {"bound": "hbm", "kernel": "rk4_tb_kernel", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": (lambda b: b * cs / K if b else None)(
-                             profiled_traffic("rk4_batch_kernel.md", "dram_bytes_per_cell_step")),
-                         "note": "108 B per cell-step (FP32 stages, FP64 state); traffic = DRAM bytes per "
-                                 "cell-step of the profiled 16-chip batch x this leg's cell-steps per launch"},
-            "l2": "256 MB buffer rewritten between intervals; 265M cells >> L2 anyway"}
+                         "traffic": (lambda b: b * cs if b else None)(
+                             profiled_traffic("rk4_tb_kernel_batch.md", "dram_bytes_per_cell_step")),
+                         "note": "108 B per cell-step algorithmic (FP32 stages, FP64 state); the temporally "
+                                 "blocked kernel moves far fewer bytes (traffic: DRAM bytes per cell-step of the "
+                                 "profiled 16-chip batch x this launch's cell-steps)"},
+            "l2": f"one launch of {K} intervals; the {int(cells.sum())}-cell state (FP64) is far larger than L2"}
+
+
+def leg_chip2d(args, flush):
+    """The 2-D chip (64x64, default package, 15 blocks): its 1000-row trace at
+    3.333 us plus the steady solve of the average power, in the plain FP64
+    form and the fast form, with the reference's own C code timed on the
+    host on the same rows (single-threaded, as the reference runs)."""
+    import torch
+    from hotspot_b200 import FORM_FAST, FORM_PARITY
+    from hotspot_b200 import model as hm
+    from hotspot_b200 import workloads as W
+    rows = args.chip2d_rows
+    d = tempfile.mkdtemp(prefix="hsb_c0_")
+    sc = W.scenario_chip2d(d, seed=0, grid=64, steps=rows)
+    out = {"workload": "2-D chip 64x64 (Si 0.15 mm + TIM + spreader/sink), 16x16 mm, 15 blocks, "
+                       f"{rows} rows at 3.333 us, then the steady solve of the average power"}
+    temps = {}
+    for name, form in (("plain_fp64", FORM_PARITY), ("fast", FORM_FAST)):
+        m = hm.from_scenario(sc)
+        m.set_solver(form)
+        t = m.vector(m.config.init_temp)
+        m.compute_temp(m.power_vector(sc.block_power[0]), t, 0.0)     # state and workspaces set up
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        dev_ms = ker_ms = 0.0
+        steps = launches = 0
+        tr = np.empty((rows, t.size))
+        for k in range(rows):
+            m.compute_temp(m.power_vector(sc.block_power[k]), None, sc.dt)
+            s = m.stats()
+            dev_ms += s["device_ms"]
+            ker_ms += s["kernel_ms"]
+            steps += s["rk4_steps"]
+            launches += s["launches"]
+            tr[k] = t
+        avg = m.power_vector(sc.block_power.mean(0))
+        sv = m.vector()
+        m.steady(avg.copy(), sv)
+        sms = []
+        for _ in range(3 if form == FORM_FAST else 1):
+            m.steady(avg.copy(), sv)
+            sms.append(m.stats()["device_ms"])
+        temps[name] = (tr, sv.copy())
+        cells = m.n_cells
+        out[name] = {"cell_steps_per_s": m.n_cells * steps / (dev_ms / 1e3), "ms_per_row": dev_ms / rows,
+                     "rk4_steps": steps, "gpu_launches": launches, "steady_ms": statistics.median(sms),
+                     "steady_solves_per_s": 1e3 / statistics.median(sms)}
+        m.close()
+    out["max_dT_K_fast_vs_plain"] = float(np.max(np.abs(temps["fast"][0] - temps["plain_fp64"][0])))
+    # the reference's own code on the same rows (the live build, else the oracle's C restatement)
+    from oracle import ref as R
+    if R.available():
+        o, kind = R.RefModel(sc), "reference"
+    else:
+        from oracle.restatement import OracleModel
+        o, kind = OracleModel(sc), "port"
+    to = o.vector(333.15)
+    o.compute_temp(o.power_vector(sc.block_power[0]), to, 0.0)
+    t0 = time.perf_counter()
+    worst = 0.0
+    for k in range(rows):
+        o.compute_temp(o.power_vector(sc.block_power[k]), None, sc.dt)
+        worst = max(worst, float(np.max(np.abs(to - temps["plain_fp64"][0][k]))))
+    cpu_tr = time.perf_counter() - t0
+    so = o.vector()
+    t0 = time.perf_counter()
+    o.steady(o.power_vector(sc.block_power.mean(0)), so)
+    cpu_st = time.perf_counter() - t0
+    if hasattr(o, "close"):
+        o.close()
+    steps = out["plain_fp64"]["rk4_steps"]      # the reference takes the replay's steps (bit-identical)
+    out["max_dT_K_plain_vs_reference"] = worst
+    out["max_dT_K_steady_plain_vs_reference"] = float(np.max(np.abs(so - temps["plain_fp64"][1])))
+    out["cpu_baseline"] = {"kind": kind, "cores": 1, "cell_steps_per_s": cells * steps / cpu_tr,
+                           "trace_s": cpu_tr, "steady_s": cpu_st, "steady_solves_per_s": 1.0 / cpu_st,
+                           "sample": f"the full {rows} rows and the steady solve, single-threaded"}
+    out["speedup_vs_cpu"] = {"fast_transient": out["fast"]["cell_steps_per_s"] / out["cpu_baseline"]["cell_steps_per_s"],
+                             "plain_transient": out["plain_fp64"]["cell_steps_per_s"] /
+                             out["cpu_baseline"]["cell_steps_per_s"],
+                             "fast_steady": cpu_st * 1e3 / out["fast"]["steady_ms"]}
+    out["note"] = ("16,384 cells fit L2: every form is latency- and launch-bound here (a few hundred "
+                   "microseconds of work per row); no HBM roofline is claimed")
+    return out
 
 
 def leg_microchannel(args):
@@ -583,8 +717,8 @@ def run_ours(args):
                                 "sample": f"2 rows of the same workload x {cores} independent "
                                           "single-threaded replicas"}
     if ws == 1 and not args.headline_only:
-        for name, fn in (("batched", lambda: leg_batched(args, flush)), ("microchannel", lambda: leg_microchannel(args)),
-                         ("serving", lambda: leg_serving(args))):
+        for name, fn in (("chip2d", lambda: leg_chip2d(args, flush)), ("batched", lambda: leg_batched(args, flush)),
+                         ("microchannel", lambda: leg_microchannel(args)), ("serving", lambda: leg_serving(args))):
             try:
                 line[name] = fn()
             except Exception as e:      # a failed leg is reported, the headline still prints

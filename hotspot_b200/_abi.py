@@ -18,7 +18,7 @@ STR = 512
 EXTRA, EXTRA_SEC = 12, 16
 
 # solver forms / methods (hsb_device.h)
-FORM_PARITY, FORM_FAST, FORM_FAST_STAGES = 0, 1, 2
+FORM_PARITY, FORM_FAST, FORM_FAST_STAGES, FORM_FAST_PASSES = 0, 1, 2, 3
 STEADY_AUTO, STEADY_GS_REPLAY, STEADY_MG, STEADY_BICGSTAB = 0, 1, 2, 3
 
 
@@ -237,6 +237,8 @@ _SIGS = {
     "hsb_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int]),
     "hsb_batch_destroy": (None, [C.c_void_p]),
     "hsb_batch_transient": (C.c_int, [C.c_void_p, _D, C.c_double, C.POINTER(Stats)]),
+    "hsb_batch_transient_trace": (C.c_int, [C.c_void_p, _D, C.c_int, C.c_double, C.POINTER(Stats)]),
+    "hsb_batch_chip_tile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "hsb_batch_set_schedule": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     "hsb_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong),
                                  C.POINTER(C.c_int), C.POINTER(C.c_double)]),
@@ -245,6 +247,7 @@ _SIGS = {
     "hsb_server_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_longlong]),
     "hsb_server_destroy": (None, [C.c_void_p]),
     "hsb_server_add_model": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_longlong]),
+    "hsb_server_add_replica": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "hsb_server_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "hsb_server_set_priority": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "hsb_dev_set_priority": (C.c_int, [C.c_void_p, C.c_int]),

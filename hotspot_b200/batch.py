@@ -1,6 +1,7 @@
 """Batches of grid models advanced together on one GPU (libhotspot_b200's
 hsb_batch_* entry points): every model keeps its own adaptive RK4 step
-sequence, and one persistent launch per sampling interval advances them all."""
+sequence, and one persistent launch advances them all by K sampling
+intervals."""
 from __future__ import annotations
 
 import ctypes as C
@@ -38,13 +39,27 @@ class Batch:
             _check(lib().hsb_batch_transient(self.ptr, _abi.dptr(flat), dt, C.byref(st)))
         return st.as_dict()
 
-    def set_schedule(self, ctas_per_sm: int, split: float = 1.0):
-        _check(lib().hsb_batch_set_schedule(self.ptr, int(ctas_per_sm), float(split)))
+    def trace(self, rows, dt: float) -> dict:
+        """Advance every model by len(rows) intervals of ``dt`` seconds in one
+        launch; ``rows[k]`` is interval k's list of block power vectors (one per model)."""
+        flat = np.ascontiguousarray(np.stack([np.concatenate(r) for r in rows]), dtype=np.float64)
+        st = _abi.Stats()
+        _check(lib().hsb_batch_transient_trace(self.ptr, _abi.dptr(flat), int(flat.shape[0]), dt, C.byref(st)))
+        return st.as_dict()
+
+    def set_schedule(self, policy: int, split: float = 1.0):
+        """Tile policy (0, 1, 2; see hsb_batch_set_schedule) and CTA-group split."""
+        _check(lib().hsb_batch_set_schedule(self.ptr, int(policy), float(split)))
 
     def info(self) -> dict:
-        g, cells, cps, split = C.c_int(), C.c_longlong(), C.c_int(), C.c_double()
-        _check(lib().hsb_batch_info(self.ptr, C.byref(g), C.byref(cells), C.byref(cps), C.byref(split)))
-        return {"grid": g.value, "cells": cells.value, "ctas_per_sm": cps.value, "split": split.value}
+        g, cells, pol, split = C.c_int(), C.c_longlong(), C.c_int(), C.c_double()
+        _check(lib().hsb_batch_info(self.ptr, C.byref(g), C.byref(cells), C.byref(pol), C.byref(split)))
+        return {"grid": g.value, "cells": cells.value, "policy": pol.value, "split": split.value}
+
+    def tile(self, c: int) -> tuple[int, int]:
+        r, cc = C.c_int(), C.c_int()
+        _check(lib().hsb_batch_chip_tile(self.ptr, int(c), C.byref(r), C.byref(cc)))
+        return r.value, cc.value
 
     def autotune(self, enable: bool = True):
         """Let the next calls try candidate schedules on the real work and keep the fastest."""
@@ -53,7 +68,7 @@ class Batch:
     def tuning(self) -> list[dict]:
         buf = np.zeros(4 * 64)
         n = lib().hsb_batch_tuning(self.ptr, _abi.dptr(buf), 64)
-        return [{"ctas_per_sm": int(buf[4 * k]), "split": float(buf[4 * k + 1]), "ring": int(buf[4 * k + 2]),
+        return [{"policy": int(buf[4 * k]), "split": float(buf[4 * k + 1]),
                  "ms_per_gcell_step": float(buf[4 * k + 3])} for k in range(n)]
 
     def chip_steps(self) -> np.ndarray:

@@ -565,6 +565,17 @@ static int fast_interval_graphed(hsb_dev_model *m, const double *block_power, do
   return HSB_OK;
 }
 
+// HSB_FORM_FAST_PASSES is the fast form run by its pass-by-pass kernel:
+// record the kernel choice on the model and return the form
+static int fast_form(hsb_dev_model *m, int form) {
+  if (form == HSB_FORM_FAST_PASSES) {
+    m->fast_passes = 1;
+    return HSB_FORM_FAST;
+  }
+  if (form == HSB_FORM_FAST) m->fast_passes = 0;
+  return form;
+}
+
 int hsb_dev_transient(hsb_dev_model *m, const double *block_power, const double *block_temp_in,
                       double time_elapsed, double *block_temp_out, const hsb_solver_opts *o,
                       hsb_stats *st) {
@@ -574,7 +585,7 @@ int hsb_dev_transient(hsb_dev_model *m, const double *block_power, const double 
   hsb_stats local;
   if (!st) st = &local;
   int rc;
-  const int form = o ? o->form : HSB_FORM_PARITY;
+  const int form = fast_form(m, o ? o->form : HSB_FORM_PARITY);
   // after the first interval (which sets up the workspace) the fast form
   // replays its interval from a graph
   if (form == HSB_FORM_FAST && !block_temp_in && m->fast && !m->ivg_off) {
@@ -643,7 +654,7 @@ int hsb_dev_transient_trace(hsb_dev_model *m, const double *block_powers, int K,
                             double time_elapsed, double *block_temp_out, const hsb_solver_opts *o, hsb_stats *st) {
   if (!m || !block_powers || K < 1) return set_error(HSB_E_ARG, "null argument or no intervals");
   if (!m->b2g_ptr) return set_error(HSB_E_ARG, "block-grid maps not set");
-  const int form = o ? o->form : HSB_FORM_PARITY;
+  const int form = fast_form(m, o ? o->form : HSB_FORM_PARITY);
   const size_t nb = (size_t)m->total_n_blocks + m->nx;
   hsb_stats local;
   if (!st) st = &local;

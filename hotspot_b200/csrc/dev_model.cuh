@@ -119,6 +119,9 @@ struct hsb_dev_model {
   // fast-form workspaces (allocated lazily by those solvers); coef_version
   // counts coefficient uploads so derived FP32 tables are rebuilt when stale
   int coef_version;
+  // the fast transient's kernel: 0 the temporally blocked one where it
+  // applies (rk4_tb.cu), 1 one grid-wide pass per Krylov vector (rk4_krylov.cu)
+  int fast_passes;
   void *fast;
   void (*fast_free)(void *);
   void *mg;

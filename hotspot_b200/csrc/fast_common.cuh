@@ -85,6 +85,7 @@ struct FastWork {
   const void *kfn;                // Krylov kernel variant kgrid was computed for
   int kgrid;                      // its co-resident grid
   cudaEvent_t kev[2];             // kernel timing events
+  void *tb;                       // temporally blocked kernel's resources (rk4_tb.cu), or null
 };
 
 // Layers are processed in fixed-size chunks, so that a chunk's per-cell
@@ -316,8 +317,11 @@ static int coop_grid(const hsb_dev_model *m, const void *fn, size_t smem, int *g
 int fast_prepare(hsb_dev_model *m, FastWork **out);
 // stage-by-stage fast RK4 over [0, T) starting from step size h0
 int rk4_stage_run(hsb_dev_model *m, FastWork *w, double T, double h0, hsb_stats *st);
-// the Krylov vectors and their tensor maps (allocated once per model)
+// the fast transient's kernel for the model (temporally blocked where it
+// applies, else the Krylov vectors and their tensor maps, allocated once)
 int kry_prepare(hsb_dev_model *m, FastWork *w);
+// the pass-by-pass kernel's Krylov vectors and tensor maps, whatever the model
+int kry_prepare_vectors(hsb_dev_model *m, FastWork *w);
 // K intervals in one launch from K device block-power vectors; *done = the
 // intervals completed (< K: the rejection budget ran out in interval *done at
 // *t_done, continue with step size *h_next)

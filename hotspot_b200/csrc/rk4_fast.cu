@@ -22,6 +22,7 @@
 //   * step-size control runs on the device: every CTA reads the global
 //     max-norm after the barrier and takes the identical decision.
 #include "fast_common.cuh"
+#include "rk4_tb.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -587,6 +588,7 @@ static void free_fast(void *p) {
   if (w->h_cnt) cudaFreeHost(w->h_cnt);
   if (w->kev[0]) cudaEventDestroy(w->kev[0]);
   if (w->kev[1]) cudaEventDestroy(w->kev[1]);
+  tb_res_free((TbRes *)w->tb);
   delete w;
 }
 

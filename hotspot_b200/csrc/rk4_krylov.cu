@@ -30,8 +30,11 @@
 // reads the same global norm and takes the same decision.  When a step needs
 // more than KRY_DMAX vectors (seven rejections in a row) the kernel stops at
 // the last accepted step and the stage form finishes the interval.
+#include <algorithm>
+
 #include "fast_common.cuh"
 #include "krylov_coef.cuh"
+#include "rk4_tb.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -627,7 +630,59 @@ static size_t kry_smem(int nl) {
   return kdyn_layout(nl, off);
 }
 
+int kry_prepare_vectors(hsb_dev_model *m, FastWork *w);
+
+// the temporally blocked kernel for this model: its resources, tile shape,
+// co-resident grid and the chip descriptors for both roles of the state buffers
+static int tb_prepare_single(hsb_dev_model *m, FastWork *w) {
+  int rc;
+  TbRes *r = (TbRes *)w->tb;
+  rc = tb_res_prepare(m, &r, w->pk);
+  w->tb = r;
+  if (rc) return rc;
+  if (r->chip_oi == 0) {
+    int nsm = 0, cap = 0;
+    HSB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device));
+    HSB_CUDA(cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, m->device));
+    int oi = 0, oj = 0;
+    if ((rc = tb_tile_for(m->nl, m->nr, m->nc, nsm, (size_t)cap, &oi, &oj))) return rc;
+    const size_t dyn = tb_dyn_smem(m->nl, oi, oj);
+    if ((rc = raise_smem_limit(tb_kernel(), dyn))) return rc;
+    int per_sm = 0;
+    HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tb_kernel(), TB_THREADS, dyn));
+    if (per_sm < 1) return set_error(HSB_E_ARG, "temporally blocked transient kernel does not fit an SM");
+    const long long tiles = (long long)((m->nr + oi - 1) / oi) * ((m->nc + oj - 1) / oj);
+    r->grid = (int)std::min<long long>((long long)per_sm * nsm, tiles);
+    r->dyn = dyn;
+    r->chip_oi = oi;
+    r->chip_oj = oj;
+    r->chip_y0 = r->chip_y1 = nullptr;
+  }
+  const bool same = (r->chip_y0 == m->y && r->chip_y1 == w->ytemp) || (r->chip_y0 == w->ytemp && r->chip_y1 == m->y);
+  if (!same) {
+    TChip C[2];
+    if ((rc = tb_fill_chip(m, r, m->y, w->ytemp, w->pf, r->chip_oi, r->chip_oj, &C[0]))) return rc;
+    if ((rc = tb_fill_chip(m, r, w->ytemp, m->y, w->pf, r->chip_oi, r->chip_oj, &C[1]))) return rc;
+    HSB_CUDA(cudaMemcpy(r->d_chip, C, sizeof(C), cudaMemcpyHostToDevice));
+    r->chip_y0 = m->y;
+    r->chip_y1 = w->ytemp;
+  }
+  w->kfn = tb_kernel();
+  w->kgrid = r->grid;
+  if (!w->kev[0]) {
+    HSB_CUDA(cudaEventCreate(&w->kev[0]));
+    HSB_CUDA(cudaEventCreate(&w->kev[1]));
+  }
+  return HSB_OK;
+}
+
 int kry_prepare(hsb_dev_model *m, FastWork *w) {
+  if (!m->fast_passes && tb_eligible(m)) return tb_prepare_single(m, w);
+  return kry_prepare_vectors(m, w);
+}
+
+// the pass-by-pass kernel's Krylov vectors, tensor maps and grid
+int kry_prepare_vectors(hsb_dev_model *m, FastWork *w) {
   int rc;
   if (!w->N) {
     w->nstride = (m->ncell + 63) / 64 * 64;
@@ -677,9 +732,44 @@ int rk4_krylov_trace(hsb_dev_model *m, FastWork *w, const double *bpow, int K, d
 }
 
 // the launch and the copy of its counters to the host, without waiting
+// the temporally blocked kernel's launch (one chip, every co-resident CTA)
+static int tb_enqueue(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, const double *bpow, int K) {
+  TbRes *r = (TbRes *)w->tb;
+  const TChip *chips = r->d_chip + (m->y == r->chip_y0 ? 0 : 1);
+  const int4 *work = nullptr;
+  const int *wptr = nullptr;
+  long long *out = w->cnt;
+  long long nbtot = (long long)m->total_n_blocks + m->nx;
+  long long max_attempts = 10000000;
+  HSB_CUDA(cudaMemsetAsync(w->cnt, 0, sizeof(long long) * 8, m->stream));
+  HSB_CUDA(cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, m->stream));
+  void *args[] = {&chips, &work, &wptr, &out, &T, &K, &bpow, &nbtot, &max_attempts};
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(r->grid);
+  cfg.blockDim = dim3(TB_THREADS);
+  cfg.dynamicSmemBytes = r->dyn;
+  cfg.stream = m->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  HSB_CUDA(cudaStreamIsCapturing(m->stream, &cap));
+  const unsigned rec = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+  HSB_CUDA(cudaEventRecordWithFlags(w->kev[0], m->stream, rec));
+  HSB_CUDA(cudaLaunchKernelExC(&cfg, tb_kernel(), args));
+  HSB_CUDA(cudaEventRecordWithFlags(w->kev[1], m->stream, rec));
+  HSB_CUDA(cudaMemcpyAsync(w->h_cnt, w->cnt, sizeof(long long) * 8, cudaMemcpyDeviceToHost, m->stream));
+  st->launches += 1;
+  return HSB_OK;
+}
+
 int rk4_krylov_enqueue(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, const double *bpow, int K) {
   int rc;
   if ((rc = kry_prepare(m, w))) return rc;
+  if (w->kfn == tb_kernel()) return tb_enqueue(m, w, T, st, bpow, K);
   KryArgs A;
   memset(&A, 0, sizeof(A));
   A.m_y = w->kmap_y;

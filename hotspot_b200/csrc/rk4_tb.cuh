@@ -1,0 +1,78 @@
+// rk4_tb.cuh -- descriptors of the temporally blocked fast transient kernel
+// (rk4_tb.cu), shared with the single-model launcher (rk4_krylov.cu) and the
+// batch (rk4_batch.cu).
+#pragma once
+#include "fast_common.cuh"
+
+namespace hsb {
+
+#define TB_THREADS 512
+#define TB_WARPS (TB_THREADS / 32)
+#define TB_SLOTS 2            // own cells per thread: a sub-tile holds at most TB_THREADS * TB_SLOTS
+#define TB_NLMIN 3
+#define TB_NLMAX 12
+#define TB_DMAX 19            // highest Krylov degree in the kernel (first attempt 7, +4 per rejection)
+#define TB_JMAX (TB_DMAX - 1) // edge-response table depth: L_cc^j, j < TB_JMAX
+#define TB_OUT 8              // per-chip result words (layout of FastWork::cnt)
+#define TB_BAR_LIMIT (1 << 25)
+
+// FP32 layer coefficients as the kernel reads them: two float4 loads
+struct alignas(16) TLayer {
+  float gNS, gEW, gDn, invC;        // lateral, to the layer below, 1/C
+  float gEdgeNS, gEdgeEW, gAmb;     // to the package node at the boundary, to ambient (sink, PCB)
+  int nbase;                        // W node of this layer's package group (W, E, N, S), -1: none
+};
+
+// one chip (model) as the kernel sees it
+struct TChip {
+  double *y[2];                     // state buffers: y[out[6]] holds the state at launch
+  float *pf;                        // FP32 grid power
+  double *pgrid;                    // FP64 grid power (K = 0: source; K > 0: the last interval's, written)
+  long long boff;                   // K > 0: this chip's block powers of interval k at bpow + k * nbtot + boff
+  const int *b2g_ptr, *b2g_blk;
+  const double *b2g_occ, *b2g_area;
+  double cell_area;
+  const TLayer *L;
+  const PackF *pk;
+  const double *er;                 // [TB_JMAX][ne][ne] edge responses
+  double *part;                     // [TB_DMAX + 1][NEDGE][segmax] per-tile edge sums
+  unsigned long long *err;          // [3] rotating error-norm slots
+  unsigned *bar;                    // [2] chip barrier: arrivals, generation
+  long long ncell, plane;
+  double ambient;
+  int nl, nr, nc, nx, ne;
+  int eg_layer[5], eg_node[5];      // per package group: its layer (-1: absent), its W node
+  int oi, oj, nti, ntj, ntiles;     // own tiles
+  int segmax;
+  int rcap;                         // region cells per layer of one buffer
+};
+
+// per-model resources
+struct TbRes {
+  TLayer *L;
+  PackF *pk;
+  double *er;
+  double *part;
+  unsigned long long *err;
+  unsigned *bar;
+  TChip *d_chip;                    // [2]: state in the first buffer / in the second
+  const double *chip_y0, *chip_y1;  // the buffers d_chip[0] describes (y, ytemp)
+  int chip_oi, chip_oj;
+  int version, ne, segmax;
+  int eg_layer[5], eg_node[5];
+  int grid;                         // co-resident CTAs of a single-model launch
+  size_t dyn;                       // dynamic shared memory of that launch
+};
+
+bool tb_eligible(const hsb_dev_model *m);
+const void *tb_kernel();
+size_t tb_static_smem();
+size_t tb_dyn_smem(int nl, int oi, int oj);
+int tb_tile_for(int nl, int nr, int nc, int ctas, size_t smem_cap, int *oi, int *oj);
+double tb_tile_work(int oi, int oj);
+int tb_res_prepare(hsb_dev_model *m, TbRes **r, const PackF *pk_dev);
+void tb_res_free(TbRes *r);
+int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1, float *pf, int oi, int oj,
+                 TChip *C);
+
+}  // namespace hsb

@@ -62,6 +62,7 @@ struct hsb_server {
     bool warm = false;   // workspace allocated by an earlier request
     bool busy = false;
     int high = 0;        // priority class
+    int cls = 0;         // the pool: index of the first model registered for this class
   };
   std::vector<Model> models;
 };
@@ -90,15 +91,40 @@ int hsb_server_add_model(hsb_server *s, hsb_dev_model *m, int form, double stead
   e.opts.steady_tol = steady_tol;
   e.opts.max_iters = 0;
   e.workspace = workspace_bytes;
+  e.cls = (int)s->models.size();
+  s->models.push_back(e);
+  return (int)s->models.size() - 1;
+}
+
+int hsb_server_add_replica(hsb_server *s, int model, hsb_dev_model *m) {
+  if (!s || !m || model < 0 || model >= (int)s->models.size()) return set_error(HSB_E_ARG, "unknown model");
+  const hsb_server::Model &p = s->models[s->models[model].cls];
+  if (m->nl != p.m->nl || m->nr != p.m->nr || m->nc != p.m->nc || m->nx != p.m->nx ||
+      m->total_n_blocks != p.m->total_n_blocks)
+    return set_error(HSB_E_ARG, "a replica must have its pool's grid and block vector");
+  hsb_server::Model e;
+  e.m = m;
+  e.opts = p.opts;
+  e.workspace = p.workspace;
+  e.cls = p.cls;
+  if (p.high) {
+    const int rc = hsb_dev_set_priority(m, 1);
+    if (rc) return rc;
+    e.high = 1;
+  }
   s->models.push_back(e);
   return (int)s->models.size() - 1;
 }
 
 int hsb_server_set_priority(hsb_server *s, int model, int high) {
   if (!s || model < 0 || model >= (int)s->models.size()) return set_error(HSB_E_ARG, "unknown model");
-  const int rc = hsb_dev_set_priority(s->models[model].m, high);
-  if (rc) return rc;
-  s->models[model].high = high ? 1 : 0;
+  const int cls = s->models[model].cls;
+  for (auto &M : s->models)   // the whole pool
+    if (M.cls == cls) {
+      const int rc = hsb_dev_set_priority(M.m, high);
+      if (rc) return rc;
+      M.high = high ? 1 : 0;
+    }
   return HSB_OK;
 }
 
@@ -161,6 +187,7 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
   std::mutex mu;
   std::condition_variable cv;
   std::vector<int> state(n, 0);   // 0 pending, 1 running, 2 done
+  std::vector<int> served_by(n, -1);
   int done = 0, running = 0, running_high = 0, running_low = 0, paused_low = 0;
   bool any_high = false;   // a high-priority request is in this run
   for (int k = 0; k < n; k++) any_high = any_high || s->models[reqs[k].model].high;
@@ -189,18 +216,37 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
           next_arrival = std::min(next_arrival, r.arrival);
           continue;
         }
-        hsb_server::Model &M = s->models[r.model];
-        if (M.busy) continue;
+        // the pool member to serve it: the named model, or any idle replica
+        // of its pool (a transient that continues the state of the named
+        // model -- no initial temperatures -- needs that model)
+        const int cls = s->models[r.model].cls;
+        const bool any = !(r.kind == HSB_REQ_TRANSIENT && !r.temp_in);
+        int pick = -1;
+        for (int q = any ? cls : r.model; q < (int)s->models.size(); q++) {
+          hsb_server::Model &Q = s->models[q];
+          if (Q.cls != cls || Q.busy) {
+            if (!any) break;
+            continue;
+          }
+          if (!Q.warm) {   // first use: admission by free device memory
+            if (!mem_known) {
+              cudaSetDevice(Q.m->device);
+              cudaMemGetInfo(&free_b, &total_b);
+              mem_known = true;
+            }
+            if ((long long)free_b < Q.workspace + s->reserve) {
+              if (!any) break;
+              continue;
+            }
+          }
+          if (pick < 0 || (Q.warm && !s->models[pick].warm)) pick = q;   // warm members first
+          if (!any || Q.warm) break;
+        }
+        if (pick < 0) continue;
+        hsb_server::Model &M = s->models[pick];
         if (!M.high && running_low >= s->workers) continue;   // the other threads are kept for high priority
         if (!M.high && running_high > 0) continue;             // no new background work while a priority request runs
-        if (!M.warm) {   // first use: admission by free device memory
-          if (!mem_known) {
-            cudaSetDevice(M.m->device);
-            cudaMemGetInfo(&free_b, &total_b);
-            mem_known = true;
-          }
-          if ((long long)free_b < M.workspace + s->reserve) continue;
-        }
+        served_by[k] = pick;
         // high-priority models first, then the least work, then the earliest arrival
         if (best < 0) {
           best = k;
@@ -218,7 +264,7 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
         // nothing runs, nothing more arrives: what is left waits on memory
         // that no request will free -- fail those requests
         for (int k = 0; k < n; k++)
-          if (state[k] == 0 && reqs[k].arrival <= t && !s->models[reqs[k].model].busy) {
+          if (state[k] == 0 && reqs[k].arrival <= t) {
             reqs[k].status = set_error(HSB_E_NOMEM, "request not admitted: not enough free device memory");
             reqs[k].start = reqs[k].finish = t;
             state[k] = 2;
@@ -235,7 +281,7 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
         continue;
       }
       hsb_request &r = reqs[best];
-      hsb_server::Model &M = s->models[r.model];
+      hsb_server::Model &M = s->models[served_by[best]];
       state[best] = 1;
       running++;
       const bool high = M.high != 0;

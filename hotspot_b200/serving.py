@@ -68,6 +68,15 @@ class Server:
         self.models.append(model)
         return idx
 
+    def add_replica(self, model: int, replica) -> int:
+        """Register ``replica`` (same grid and floorplans) as another member of
+        ``model``'s pool: requests naming the pool run on whichever member is idle."""
+        idx = lib().hsb_server_add_replica(self.ptr, int(model), lib().hsb_grid_device(replica.ptr))
+        if idx < 0:
+            _check(idx)
+        self.models.append(replica)
+        return idx
+
     def set_priority(self, model: int, high: bool = True):
         """Dispatch this model's requests first and run them on a high-priority stream."""
         _check(lib().hsb_server_set_priority(self.ptr, int(model), int(bool(high))))
@@ -114,7 +123,7 @@ class Server:
 @dataclass
 class Mix:
     requests: list
-    classes: dict = field(default_factory=dict)   # (kind, side, layers) -> model index
+    classes: dict = field(default_factory=dict)   # (kind, side, layers) -> model (pool) index
     models: list = field(default_factory=list)
 
 
@@ -122,7 +131,8 @@ def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.
                 steady_frac: float = 0.7, transient_steps: int = 500, dt: float = 3.333e-6,
                 steady_sides=(64, 128, 256, 512, 1024), transient_sides=(64, 128, 256),
                 max_layers: int = 8, model_factory=None, high_priority_cells: int = 0,
-                high_priority_classes=(), reuse: Mix | None = None) -> Mix:
+                high_priority_classes=(), reuse: Mix | None = None, replicas: int = 1,
+                replica_max_side: int = 256) -> Mix:
     """Seeded Poisson arrivals at `rate` req/s for `duration` s.  Steady
     requests: side drawn log-uniformly from `steady_sides`, 1..max_layers
     chip layers; transients: `transient_steps` intervals of `dt` on
@@ -133,7 +143,9 @@ def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.
     Steady classes of at most `high_priority_cells` cells, and the steady
     classes named in `high_priority_classes` as (side, chip layers), get the
     high priority class.  `reuse`: the resident models of an earlier mix on
-    the same server serve the classes they cover."""
+    the same server serve the classes they cover.  `replicas`: resident
+    models per class of side at most `replica_max_side` (a pool; requests of
+    one class then run concurrently on its idle members)."""
     from . import model as hm
     rng = np.random.default_rng(seed)
     mix = Mix(requests=[])
@@ -161,6 +173,10 @@ def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.
             mix.classes[key] = server.add_model(m, FORM_FAST, 1e-5)
             if steady and (m.n_cells <= high_priority_cells or (side, layers) in set(high_priority_classes)):
                 server.set_priority(mix.classes[key], True)
+            for _ in range(replicas - 1 if side <= replica_max_side else 0):
+                rep = model_factory(sc)
+                mix.models.append(rep)
+                server.add_replica(mix.classes[key], rep)
         mi = mix.classes[key]
         m = server.models[mi]
         nblk = sum(m.layer_units[l] for l in range(m.n_layers) if m.layer_power[l])

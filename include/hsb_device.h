@@ -40,6 +40,8 @@ extern "C" {
 #define HSB_FORM_PARITY  0    /* FP64, replays the reference's operation order */
 #define HSB_FORM_FAST    1    /* FP32 stencil work, FP64 state/refinement       */
 #define HSB_FORM_FAST_STAGES 2  /* the fast transient evaluated stage by stage     */
+#define HSB_FORM_FAST_PASSES 3  /* the fast transient with one grid-wide pass per Krylov
+                                   vector (no temporal blocking); same arithmetic */
 
 /* steady methods */
 #define HSB_STEADY_AUTO       0  /* GS replay for FORM_PARITY; MG-PCG (or BiCGStab with advection) for FORM_FAST */
@@ -168,31 +170,39 @@ int hsb_dev_transient_noalloc(hsb_dev_model *m, double *y, const double *pgrid,
  * reference, which simulates one chip per process; each chip's arithmetic is
  * the fast transient form of compute_temp_grid, temperature_grid.c:3603-3704).
  *
- * A batch references n existing device models (per-layer conductances,
- * primary heat path, one device); hsb_batch_transient advances all of them by
- * one sampling interval in ONE persistent cooperative launch.  block_power
- * holds every model's power vector (total_n_blocks + 12 entries each, model
- * after model) or NULL to keep the grid powers of the last call.  Each model
- * keeps its own adaptive step sequence; its state stays in its own device
- * model (hsb_dev_get_state, g2b through the model's entry points). */
+ * A batch references n existing device models (per-layer conductances, 3 to
+ * 12 layers, primary or secondary heat path, one device);
+ * hsb_batch_transient_trace advances all of them by K sampling intervals in
+ * ONE persistent cooperative launch of the temporally blocked kernel,
+ * replayed from a CUDA graph.  block_powers holds K rows, each row every
+ * model's power vector (total_n_blocks + n_extra entries each, model after
+ * model), or NULL to keep the grid powers of the last call (then K = 1).
+ * Each model keeps its own adaptive step sequence; its state stays in its
+ * own device model (hsb_dev_get_state, g2b through the model's entry
+ * points).  hsb_batch_transient is the call with K = 1. */
 struct hsb_batch;
 typedef struct hsb_batch hsb_batch;
 int  hsb_batch_create(hsb_batch **out, hsb_dev_model *const *models, int n);
 void hsb_batch_destroy(hsb_batch *b);
 int  hsb_batch_transient(hsb_batch *b, const double *block_power, double time_elapsed, hsb_stats *st);
-/* schedule: co-resident CTAs per SM (>= 1), and how finely large models are
- * split over CTA groups (1.0 = in proportion to their share of the work) */
-int  hsb_batch_set_schedule(hsb_batch *b, int ctas_per_sm, double split);
-int  hsb_batch_info(hsb_batch *b, int *grid, long long *cells, int *ctas_per_sm, double *split);
+int  hsb_batch_transient_trace(hsb_batch *b, const double *block_powers, int K, double time_elapsed,
+                               hsb_stats *st);
+/* schedule: tile policy (0: 16x64 tiles on chips of side >= 256, 16x32 on
+ * 64..128, 32x32 below; 1: 32x32 tiles; 2: 16x32 tiles), and how finely big
+ * models are split over CTA groups (1.0 = in proportion to their share of
+ * the work) */
+int  hsb_batch_set_schedule(hsb_batch *b, int policy, double split);
+int  hsb_batch_info(hsb_batch *b, int *grid, long long *cells, int *policy, double *split);
 /* accepted RK4 steps of each model in the last call (n entries) */
 int  hsb_batch_chip_steps(hsb_batch *b, long long *steps);
+/* own-tile shape (rows x columns) of model c under the current schedule */
+int  hsb_batch_chip_tile(hsb_batch *b, int c, int *rows, int *cols);
 /* autotuner: when enabled, the next calls each run one candidate schedule
- * (CTAs per SM, split, Krylov-pass ring length) on the real work -- the
- * schedule never changes the results -- and the fastest per cell-step is
+ * (tile policy, split) on the real work and the fastest per cell-step is
  * kept, and remembered for batches of the same shape in this process */
 int  hsb_batch_autotune(hsb_batch *b, int enable);
-/* the autotuner's measurements: 4 doubles per candidate (ctas_per_sm, split,
- * ring, ms per 1e9 cell-steps), up to n candidates; returns the count */
+/* the autotuner's measurements: 4 doubles per candidate (policy, split, 0,
+ * ms per 1e9 cell-steps), up to n candidates; returns the count */
 int  hsb_batch_tuning(hsb_batch *b, double *out, int n);
 
 /* ---- serving (no counterpart in the reference): steady and transient
@@ -206,7 +216,7 @@ int  hsb_batch_tuning(hsb_batch *b, double *out, int n);
 #define HSB_REQ_TRANSIENT 1
 
 typedef struct hsb_request {
-  int model;                 /* index from hsb_server_add_model */
+  int model;                 /* index from hsb_server_add_model / _add_replica (its pool serves it) */
   int kind;                  /* HSB_REQ_STEADY or HSB_REQ_TRANSIENT */
   int steps;                 /* transient: sampling intervals */
   double dt;                 /* transient: interval length (s) */
@@ -224,9 +234,16 @@ typedef struct hsb_server hsb_server;
 int  hsb_server_create(hsb_server **out, int workers, long long reserve_bytes);
 void hsb_server_destroy(hsb_server *s);
 /* register a resident model; form HSB_FORM_*, steady_tol (K, 0 = default),
- * workspace_bytes = device memory its first solve allocates; returns its index */
+ * workspace_bytes = device memory its first solve allocates; returns its
+ * index, which also names the model's pool */
 int  hsb_server_add_model(hsb_server *s, hsb_dev_model *m, int form, double steady_tol,
                           long long workspace_bytes);
+/* register m (same grid and block vector) as another member of `model`'s
+ * pool, with its form, tolerance, workspace and priority; returns its index.
+ * A request naming any member of a pool may be served by any idle member
+ * (warm members first), except a transient request without temp_in, which
+ * continues the state of the model it names and waits for that model. */
+int  hsb_server_add_replica(hsb_server *s, int model, hsb_dev_model *m);
 /* serve n requests (released at their arrival times); returns when all are done */
 int  hsb_server_run(hsb_server *s, hsb_request *reqs, int n);
 /* priority class of a registered model: its requests are dispatched before

@@ -308,6 +308,9 @@ static void rk4_core(const orc_model *m, const double *y, const double *k1, cons
   for (i = 0; i < n; i++) yout[i] = y[i] + h * (k1[i] + 2 * k2[i] + 2 * k3[i] + k4[i]) / 6.0;
 }
 
+/* RK4 attempts (accepted and rejected) since the library was loaded */
+long long orc_attempts = 0;
+
 double orc_rk4(const orc_model *m, double *y, const double *p, double *h)
 {
   const size_t n = (size_t)m->nl * m->nr * m->nc + m->nx;
@@ -319,6 +322,7 @@ double orc_rk4(const orc_model *m, double *y, const double *p, double *h)
   orc_slope(m, y, p, k1);
   do {
     *h = new_h;
+    orc_attempts++;
     rk4_core(m, y, k1, p, n, *h, ytemp, k2, k3, k4, t);
     rk4_core(m, y, k1, p, n, (*h) / 2.0, t1, k2, k3, k4, t);
     orc_slope(m, t1, p, k1);

@@ -1,0 +1,106 @@
+"""The temporally blocked fast transient (the default kernel of HSB_FORM_FAST
+for models with per-layer conductances) against
+
+* the same arithmetic run one grid-wide pass per Krylov vector
+  (HSB_FORM_FAST_PASSES): the same accepted steps and attempts, block and
+  grid temperatures within 1e-4 K (both are FP32-vector forms; they differ
+  only in the order of the FP64 sums of increment, error and edge sums);
+* the oracle's FP64 replay of the reference: 0.01 K.
+
+Cases cover tiles that are all boundary ("ring") tiles (16x16), grids with
+interior tiles (256x256), rectangular grids, the secondary heat path (28
+package nodes, 20 edges), 3-D stacks, and long sampling intervals whose
+adaptive steps are rejected (the retry recomputes its vectors with a larger
+halo in sub-tiles).
+"""
+import numpy as np
+import pytest
+
+from hotspot_b200 import FORM_FAST, FORM_FAST_PASSES
+from hotspot_b200 import model as hm
+from hotspot_b200 import workloads as W
+from oracle.restatement import OracleModel
+
+pytestmark = pytest.mark.gpu
+TOL_FORMS = 1e-4
+TOL_FP64 = 0.01
+
+
+def _scenario(workdir, case):
+    if case == "chip2d16":
+        return W.scenario_chip2d(workdir, seed=81, grid=16, steps=8)
+    if case == "chip2d64":
+        return W.scenario_chip2d(workdir, seed=82, grid=64, steps=8)
+    if case == "rect32x64":
+        sc = W.scenario_chip2d(workdir, seed=83, grid=32, steps=8)
+        sc.config["grid_cols"] = "64"
+        return sc
+    if case == "rect128x32":
+        sc = W.scenario_chip2d(workdir, seed=84, grid=128, steps=6)
+        sc.config["grid_cols"] = "32"
+        return sc
+    if case == "secondary":
+        sc = W.scenario_chip2d(workdir, seed=85, grid=32, steps=6)
+        sc.config["model_secondary"] = "1"
+        return sc
+    if case == "stack64":
+        return W.scenario_stack3d(workdir, seed=86, grid=64, steps=6, n_blocks=12)
+    if case == "stack256":
+        return W.scenario_stack3d(workdir, seed=87, grid=256, steps=4)
+    if case == "long_chip2d":        # 1 ms rows: steps are rejected and retried
+        sc = W.scenario_chip2d(workdir, seed=88, grid=32, steps=4)
+        sc.dt = 1e-3
+        return sc
+    if case == "long_stack":
+        sc = W.scenario_stack3d(workdir, seed=89, grid=64, steps=3, n_blocks=10)
+        sc.dt = 1e-3
+        return sc
+    raise ValueError(case)
+
+
+def _run(sc, form, rows):
+    m = hm.from_scenario(sc)
+    m.set_solver(form)
+    t = m.vector(m.config.init_temp)
+    temps, steps, attempts, fallbacks = [], 0, 0, 0
+    for k in range(rows):
+        m.compute_temp(m.power_vector(sc.block_power[k]), t if k == 0 else None, sc.dt)
+        s = m.stats()
+        steps += s["rk4_steps"]
+        attempts += s["rk4_attempts"]
+        fallbacks += s["fallbacks"]
+        temps.append(t.copy())
+    g = m.grid("trans")
+    m.close()
+    return np.array(temps), g, steps, attempts, fallbacks
+
+
+CASES = ["chip2d16", "chip2d64", "rect32x64", "rect128x32", "secondary", "stack64", "stack256", "long_chip2d",
+         "long_stack"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_blocked_matches_pass_by_pass(workdir, case):
+    sc = _scenario(workdir, case)
+    rows = min(sc.steps, sc.block_power.shape[0])
+    ta, ga, sa, aa, fa = _run(sc, FORM_FAST, rows)
+    tb, gb, sb, ab, fb = _run(sc, FORM_FAST_PASSES, rows)
+    assert (sa, aa) == (sb, ab), (sa, aa, sb, ab)
+    assert fa == fb
+    assert np.max(np.abs(ta - tb)) <= TOL_FORMS
+    assert np.max(np.abs(ga - gb)) <= TOL_FORMS
+    if case.startswith("long"):
+        assert aa > sa, "the long rows were meant to reject some steps"
+
+
+@pytest.mark.parametrize("case", ["chip2d64", "secondary", "stack64", "long_chip2d"])
+def test_blocked_against_fp64_oracle(workdir, case):
+    sc = _scenario(workdir, case)
+    rows = min(sc.steps, sc.block_power.shape[0], 4)
+    ta, ga, *_ = _run(sc, FORM_FAST, rows)
+    o = OracleModel(sc)
+    to = o.vector(o.init_temp)
+    for k in range(rows):
+        o.compute_temp(o.power_vector(sc.block_power[k]), to if k == 0 else None, sc.dt)
+        assert np.max(np.abs(ta[k] - to)) <= TOL_FP64, k
+    assert np.max(np.abs(ga - o.grid("trans"))) <= TOL_FP64
