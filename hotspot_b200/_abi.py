@@ -18,7 +18,7 @@ STR = 512
 EXTRA, EXTRA_SEC = 12, 16
 
 # solver forms / methods (hsb_device.h)
-FORM_PARITY, FORM_FAST, FORM_FAST_STAGES, FORM_FAST_PASSES = 0, 1, 2, 3
+FORM_PARITY, FORM_FAST, FORM_FAST_STAGES, FORM_FAST_PASSES, FORM_FP64_BLOCKED = 0, 1, 2, 3, 4
 STEADY_AUTO, STEADY_GS_REPLAY, STEADY_MG, STEADY_BICGSTAB = 0, 1, 2, 3
 
 

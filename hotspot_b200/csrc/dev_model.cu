@@ -565,11 +565,12 @@ static int fast_interval_graphed(hsb_dev_model *m, const double *block_power, do
   return HSB_OK;
 }
 
-// HSB_FORM_FAST_PASSES is the fast form run by its pass-by-pass kernel:
-// record the kernel choice on the model and return the form
+// HSB_FORM_FAST_PASSES and HSB_FORM_FP64_BLOCKED are the fast form's
+// interval run by another kernel (pass by pass; all-FP64 blocked): record the
+// kernel choice on the model and return the form
 static int fast_form(hsb_dev_model *m, int form) {
-  if (form == HSB_FORM_FAST_PASSES) {
-    m->fast_passes = 1;
+  if (form == HSB_FORM_FAST_PASSES || form == HSB_FORM_FP64_BLOCKED) {
+    m->fast_passes = form == HSB_FORM_FAST_PASSES ? 1 : 2;
     return HSB_FORM_FAST;
   }
   if (form == HSB_FORM_FAST) m->fast_passes = 0;
@@ -714,7 +715,8 @@ int hsb_dev_steady(hsb_dev_model *m, const double *block_power, double *block_te
   int method = o->steady_method;
   if (method == HSB_STEADY_AUTO) {
     if (m->uchan_mask) method = HSB_STEADY_BICGSTAB;
-    else if (o->form != HSB_FORM_PARITY && m->nx == HSB_EXTRA) method = HSB_STEADY_MG;
+    else if (o->form != HSB_FORM_PARITY && o->form != HSB_FORM_FP64_BLOCKED && m->nx == HSB_EXTRA)
+      method = HSB_STEADY_MG;
     else method = HSB_STEADY_GS_REPLAY;
   }
   if (method == HSB_STEADY_GS_REPLAY && m->uchan_mask)

@@ -120,7 +120,8 @@ struct hsb_dev_model {
   // counts coefficient uploads so derived FP32 tables are rebuilt when stale
   int coef_version;
   // the fast transient's kernel: 0 the temporally blocked one where it
-  // applies (rk4_tb.cu), 1 one grid-wide pass per Krylov vector (rk4_krylov.cu)
+  // applies (rk4_tb.cu), 1 one grid-wide pass per Krylov vector (rk4_krylov.cu),
+  // 2 the temporally blocked one with FP64 passes
   int fast_passes;
   void *fast;
   void (*fast_free)(void *);
@@ -151,6 +152,9 @@ int g2b_on(hsb_dev_model *m, const double *grid_dev, double *blk_dev, cudaStream
 
 // exact-replay solvers
 int rk4_exact_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st);
+// the exact replay over [0, T) starting from step size h0 (the rest of an
+// interval another form could not finish)
+int rk4_exact_run(hsb_dev_model *m, double T, double h0, hsb_stats *st);
 int gs_exact_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
 
 // fast-form solvers

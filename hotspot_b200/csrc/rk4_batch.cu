@@ -132,7 +132,7 @@ static int batch_tiles(hsb_batch *b) {
     TChip &C = b->h_chips[c];
     double *y0 = C.y[0], *y1 = C.y[1];
     int rc;
-    if ((rc = tb_fill_chip(m, r, y0, y1, w->pf, oi, oj, &C))) return rc;
+    if ((rc = tb_fill_chip(m, r, y0, y1, w->pf, w->t1, oi, oj, &C))) return rc;
     C.bar = b->d_bar + 2 * c;
     C.boff = b->boff[c];
     b->dyn = std::max(b->dyn, tb_dyn_smem(m->nl, oi, oj));

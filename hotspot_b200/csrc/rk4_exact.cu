@@ -187,18 +187,22 @@ static int rk4_step(hsb_dev_model *m, const StencilArgs &A, double *h, double *n
 #define DELTA 1.0e-6
 #define HMIN(x, y) (((x) < (y)) ? (x) : (y))
 
-int rk4_exact_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
+int rk4_exact_run(hsb_dev_model *m, double time_elapsed, double h0, hsb_stats *st) {
   const StencilArgs A = make_args(m, m->L0, m->nr, m->nc);
   double t, h = 0.0, new_h;
   int rc;
   // temperature_grid.c:3676-3692
-  for (t = 0, new_h = MIN_STEP; t < time_elapsed && new_h >= MIN_STEP * DELTA; t += h) {
+  for (t = 0, new_h = h0; t < time_elapsed && new_h >= MIN_STEP * DELTA; t += h) {
     h = new_h;
     if ((rc = rk4_step(m, A, &h, &new_h, st))) return rc;
     new_h = HMIN(new_h, time_elapsed - t - h);
   }
   st->sim_time += t;
   return HSB_OK;
+}
+
+int rk4_exact_interval(hsb_dev_model *m, double time_elapsed, hsb_stats *st) {
+  return rk4_exact_run(m, time_elapsed, MIN_STEP, st);
 }
 
 }  // namespace hsb

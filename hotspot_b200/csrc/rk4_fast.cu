@@ -764,10 +764,12 @@ int rk4_fast_interval_end(hsb_dev_model *m, void *work, double time_elapsed, hsb
   double t_done = time_elapsed, h_next = 0.0;
   *fell_back = 0;
   if ((rc = rk4_krylov_complete(m, w, time_elapsed, st, &t_done, &h_next, &done))) return rc;
-  if (t_done < time_elapsed) {
+  if (t_done < time_elapsed) {   // the rest of the interval: the stage form (all-FP64 variant: the replay)
     st->fallbacks += 1;
     *fell_back = 1;
-    if ((rc = rk4_stage_run(m, w, time_elapsed - t_done, h_next, st))) return rc;
+    rc = m->fast_passes == 2 ? rk4_exact_run(m, time_elapsed - t_done, h_next, st)
+                             : rk4_stage_run(m, w, time_elapsed - t_done, h_next, st);
+    if (rc) return rc;
   }
   st->sim_time += time_elapsed;
   return HSB_OK;
@@ -813,7 +815,9 @@ int rk4_fast_trace(hsb_dev_model *m, const double *bpow_dev, int K, double time_
     if ((rc = b2g(m, bpow_dev + (long long)k * nb, m->pgrid, HSB_V_POWER))) return rc;
     st->launches += 1;
     st->fallbacks += 1;
-    if ((rc = rk4_stage_run(m, w, time_elapsed - t_done, h_next, st))) return rc;
+    rc = m->fast_passes == 2 ? rk4_exact_run(m, time_elapsed - t_done, h_next, st)
+                             : rk4_stage_run(m, w, time_elapsed - t_done, h_next, st);
+    if (rc) return rc;
     i0 = k + 1;
   }
   // the last interval's grid power is in pgrid: the kernel wrote it, or the

@@ -640,35 +640,44 @@ static int tb_prepare_single(hsb_dev_model *m, FastWork *w) {
   rc = tb_res_prepare(m, &r, w->pk);
   w->tb = r;
   if (rc) return rc;
-  if (r->chip_oi == 0) {
+  const int v = m->fast_passes == 2 ? 1 : 0;   // kernel variant: FP32 or FP64 passes
+  const bool fp64 = v == 1;
+  if (r->chip_oi[v] == 0) {
     int nsm = 0, cap = 0;
     HSB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device));
     HSB_CUDA(cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, m->device));
     int oi = 0, oj = 0;
-    if ((rc = tb_tile_for(m->nl, m->nr, m->nc, nsm, (size_t)cap, &oi, &oj))) return rc;
-    const size_t dyn = tb_dyn_smem(m->nl, oi, oj);
-    if ((rc = raise_smem_limit(tb_kernel(), dyn))) return rc;
+    if ((rc = tb_tile_for(m->nl, m->nr, m->nc, nsm, (size_t)cap, &oi, &oj, fp64))) return rc;
+    const size_t dyn = tb_dyn_smem(m->nl, oi, oj, fp64);
+    if ((rc = raise_smem_limit(tb_kernel(fp64), dyn))) return rc;
     int per_sm = 0;
-    HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tb_kernel(), TB_THREADS, dyn));
+    HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tb_kernel(fp64), TB_THREADS, dyn));
     if (per_sm < 1) return set_error(HSB_E_ARG, "temporally blocked transient kernel does not fit an SM");
     const long long tiles = (long long)((m->nr + oi - 1) / oi) * ((m->nc + oj - 1) / oj);
-    r->grid = (int)std::min<long long>((long long)per_sm * nsm, tiles);
-    r->dyn = dyn;
-    r->chip_oi = oi;
-    r->chip_oj = oj;
+    r->grid[v] = (int)std::min<long long>((long long)per_sm * nsm, tiles);
+    r->dyn[v] = dyn;
+    r->chip_oi[v] = oi;
+    r->chip_oj[v] = oj;
     r->chip_y0 = r->chip_y1 = nullptr;
   }
   const bool same = (r->chip_y0 == m->y && r->chip_y1 == w->ytemp) || (r->chip_y0 == w->ytemp && r->chip_y1 == m->y);
   if (!same) {
-    TChip C[2];
-    if ((rc = tb_fill_chip(m, r, m->y, w->ytemp, w->pf, r->chip_oi, r->chip_oj, &C[0]))) return rc;
-    if ((rc = tb_fill_chip(m, r, w->ytemp, m->y, w->pf, r->chip_oi, r->chip_oj, &C[1]))) return rc;
+    // descriptors of both variants (those not configured yet are placeholders)
+    TChip C[4];
+    memset(C, 0, sizeof(C));
+    for (int q = 0; q < 2; q++) {
+      if (!r->chip_oi[q]) continue;
+      if ((rc = tb_fill_chip(m, r, m->y, w->ytemp, w->pf, w->t1, r->chip_oi[q], r->chip_oj[q], &C[2 * q])))
+        return rc;
+      if ((rc = tb_fill_chip(m, r, w->ytemp, m->y, w->pf, w->t1, r->chip_oi[q], r->chip_oj[q], &C[2 * q + 1])))
+        return rc;
+    }
     HSB_CUDA(cudaMemcpy(r->d_chip, C, sizeof(C), cudaMemcpyHostToDevice));
     r->chip_y0 = m->y;
     r->chip_y1 = w->ytemp;
   }
-  w->kfn = tb_kernel();
-  w->kgrid = r->grid;
+  w->kfn = tb_kernel(fp64);
+  w->kgrid = r->grid[v];
   if (!w->kev[0]) {
     HSB_CUDA(cudaEventCreate(&w->kev[0]));
     HSB_CUDA(cudaEventCreate(&w->kev[1]));
@@ -677,7 +686,9 @@ static int tb_prepare_single(hsb_dev_model *m, FastWork *w) {
 }
 
 int kry_prepare(hsb_dev_model *m, FastWork *w) {
-  if (!m->fast_passes && tb_eligible(m)) return tb_prepare_single(m, w);
+  if (m->fast_passes != 1 && tb_eligible(m)) return tb_prepare_single(m, w);
+  if (m->fast_passes == 2)
+    return set_error(HSB_E_ARG, "the all-FP64 blocked form takes models with per-layer conductances and 3..12 layers");
   return kry_prepare_vectors(m, w);
 }
 
@@ -735,7 +746,8 @@ int rk4_krylov_trace(hsb_dev_model *m, FastWork *w, const double *bpow, int K, d
 // the temporally blocked kernel's launch (one chip, every co-resident CTA)
 static int tb_enqueue(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, const double *bpow, int K) {
   TbRes *r = (TbRes *)w->tb;
-  const TChip *chips = r->d_chip + (m->y == r->chip_y0 ? 0 : 1);
+  const int v = w->kfn == tb_kernel(true) ? 1 : 0;
+  const TChip *chips = r->d_chip + 2 * v + (m->y == r->chip_y0 ? 0 : 1);
   const int4 *work = nullptr;
   const int *wptr = nullptr;
   long long *out = w->cnt;
@@ -746,9 +758,9 @@ static int tb_enqueue(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, co
   void *args[] = {&chips, &work, &wptr, &out, &T, &K, &bpow, &nbtot, &max_attempts};
   cudaLaunchConfig_t cfg;
   memset(&cfg, 0, sizeof(cfg));
-  cfg.gridDim = dim3(r->grid);
+  cfg.gridDim = dim3(r->grid[v]);
   cfg.blockDim = dim3(TB_THREADS);
-  cfg.dynamicSmemBytes = r->dyn;
+  cfg.dynamicSmemBytes = r->dyn[v];
   cfg.stream = m->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -759,7 +771,7 @@ static int tb_enqueue(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, co
   HSB_CUDA(cudaStreamIsCapturing(m->stream, &cap));
   const unsigned rec = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
   HSB_CUDA(cudaEventRecordWithFlags(w->kev[0], m->stream, rec));
-  HSB_CUDA(cudaLaunchKernelExC(&cfg, tb_kernel(), args));
+  HSB_CUDA(cudaLaunchKernelExC(&cfg, w->kfn, args));
   HSB_CUDA(cudaEventRecordWithFlags(w->kev[1], m->stream, rec));
   HSB_CUDA(cudaMemcpyAsync(w->h_cnt, w->cnt, sizeof(long long) * 8, cudaMemcpyDeviceToHost, m->stream));
   st->launches += 1;
@@ -769,7 +781,7 @@ static int tb_enqueue(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, co
 int rk4_krylov_enqueue(hsb_dev_model *m, FastWork *w, double T, hsb_stats *st, const double *bpow, int K) {
   int rc;
   if ((rc = kry_prepare(m, w))) return rc;
-  if (w->kfn == tb_kernel()) return tb_enqueue(m, w, T, st, bpow, K);
+  if (w->kfn == tb_kernel(false) || w->kfn == tb_kernel(true)) return tb_enqueue(m, w, T, st, bpow, K);
   KryArgs A;
   memset(&A, 0, sizeof(A));
   A.m_y = w->kmap_y;

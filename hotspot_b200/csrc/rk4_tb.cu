@@ -64,8 +64,14 @@ static_assert(TB_SLOTS == 2, "slot 1 holds the error sums when increment and err
 __device__ Coef g_tb_first[3];
 __device__ int g_tb_first_ready;
 
+// layer table and package inputs in the vector type of the kernel variant
+template <typename V> struct TLay;
+template <> struct TLay<float> { typedef TLayer T; };
+template <> struct TLay<double> { typedef TLayerD T; };
+
+template <typename V>
 struct TSh {
-  TLayer L[TB_NLMAX];
+  typename TLay<V>::T L[TB_NLMAX];
   double Vp[TB_DMAX + 1][NXMAX];       // package parts of V_0 .. V_dE
   double yp[NXMAX];                    // package part of the state
   double es[TB_DMAX + 1][NEDGE];       // this tile's edge sums: [0] of y - y_node, [m + 1] of A_m
@@ -73,7 +79,7 @@ struct TSh {
   double wred[TB_WARPS];
   Coef E, D, F1, K, E1, D1, F11;
   double ps[PMAX];
-  float xs[NXMAX];                     // package inputs of the pass (FP32, as the cells see them)
+  V xs[NXMAX];                         // package inputs of the pass (in the cells' arithmetic)
   double gmax, pmax, hprev;
   int lost;
   int dE, dD, eLo, sep, SI, SJ;        // the attempt's plan
@@ -82,7 +88,8 @@ struct TSh {
 // ---------------------------------------------------------------------------
 // chip barrier over `size` CTAs (bounded wait; size 1: a CTA barrier)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void tsync(const TChip &C, int size, unsigned &gen, TSh &sh) {
+template <typename V>
+__device__ __forceinline__ void tsync(const TChip &C, int size, unsigned &gen, TSh<V> &sh) {
   __syncthreads();
   if (size > 1 && threadIdx.x == 0) {
     __threadfence();
@@ -107,16 +114,20 @@ __device__ __forceinline__ void tsync(const TChip &C, int size, unsigned &gen, T
   __syncthreads();
 }
 
+// the grid power in the kernel variant's type
+template <typename V> __device__ __forceinline__ const V *tb_power_of(const TChip &C);
+template <> __device__ __forceinline__ const float *tb_power_of<float>(const TChip &C) { return C.pf; }
+template <> __device__ __forceinline__ const double *tb_power_of<double>(const TChip &C) { return C.pd; }
+
 // ---------------------------------------------------------------------------
 // one stencil pass over the region rectangle [m+1, RI-m-1) x [m+1, RJ-m-1):
 // P0: dst = V_0 = (p + L y) / C from the state deviations in src;
 // else dst = h L src.  Package inputs from sh.xs (BND: grid-boundary cells
 // present in the region).  The operation order per cell is rk4_krylov.cu's.
 // ---------------------------------------------------------------------------
-template <int NL, bool BND, bool P0>
-__device__ __forceinline__ void tb_pass(const TChip &C, const TSh &sh, const float *__restrict__ src,
-                                        float *__restrict__ dst, int RI, int RJ, int m, int gi0, int gj0,
-                                        float hf) {
+template <typename V, int NL, bool BND, bool P0>
+__device__ __forceinline__ void tb_pass(const TChip &C, const TSh<V> &sh, const V *__restrict__ src,
+                                        V *__restrict__ dst, int RI, int RJ, int m, int gi0, int gj0, V hf) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int LP = RI * RJ;
   const int ra = m + 1, rb = RI - m - 1, ca = m + 1, cb = RJ - m - 1;
@@ -127,36 +138,48 @@ __device__ __forceinline__ void tb_pass(const TChip &C, const TSh &sh, const flo
     for (int c = ca + lane; c < cb; c += 32) {
       const int gj = gj0 + c;
       if (BND && (unsigned)gj >= (unsigned)nc) continue;
-      const float *p = src + r * RJ + c;
-      float *o = dst + r * RJ + c;
+      const V *p = src + r * RJ + c;
+      V *o = dst + r * RJ + c;
       const bool hN = !BND || gi > 0, hS = !BND || gi < nr - 1, hW = !BND || gj > 0, hE = !BND || gj < nc - 1;
-      const float *pw = P0 ? C.pf + (long long)gi * nc + gj : nullptr;
-      float up = 0.f, cur = p[0], gup = 0.f;
+      const V *pw = nullptr;
+      if constexpr (P0) pw = tb_power_of<V>(C) + (long long)gi * nc + gj;
+      V up = 0, cur = p[0], gup = 0;
 #pragma unroll
       for (int n = 0; n < NL; n++) {
-        const float *pn = p + n * LP;
-        const float4 L4 = *reinterpret_cast<const float4 *>(&sh.L[n]);   // gNS, gEW, gDn, invC
-        const float4 E4 = *reinterpret_cast<const float4 *>(&sh.L[n].gEdgeNS);  // gEdgeNS, gEdgeEW, gAmb, nbase
-        const float dn = n < NL - 1 ? pn[LP] : 0.f;
-        float s = 0.f;
-        if (hN) s += L4.x * (pn[-RJ] - cur);
-        if (hS) s += L4.x * (pn[RJ] - cur);
-        if (hE) s += L4.y * (pn[1] - cur);
-        if (hW) s += L4.y * (pn[-1] - cur);
+        const V *pn = p + n * LP;
+        V gNS, gEW, gDn, invC, gEdgeNS, gEdgeEW, gAmb;
+        int nb;
+        if constexpr (sizeof(V) == 4) {   // two vector loads of the FP32 table
+          const float4 L4 = *reinterpret_cast<const float4 *>(&sh.L[n]);          // gNS, gEW, gDn, invC
+          const float4 E4 = *reinterpret_cast<const float4 *>(&sh.L[n].gEdgeNS);  // gEdgeNS, gEdgeEW, gAmb, nbase
+          gNS = L4.x; gEW = L4.y; gDn = L4.z; invC = L4.w;
+          gEdgeNS = E4.x; gEdgeEW = E4.y; gAmb = E4.z;
+          nb = __float_as_int(E4.w);
+        } else {
+          gNS = sh.L[n].gNS; gEW = sh.L[n].gEW; gDn = sh.L[n].gDn; invC = sh.L[n].invC;
+          gEdgeNS = sh.L[n].gEdgeNS; gEdgeEW = sh.L[n].gEdgeEW; gAmb = sh.L[n].gAmb;
+          nb = sh.L[n].nbase;
+        }
+        const V dn = n < NL - 1 ? pn[LP] : V(0);
+        V s = 0;
+        if (hN) s += gNS * (pn[-RJ] - cur);
+        if (hS) s += gNS * (pn[RJ] - cur);
+        if (hE) s += gEW * (pn[1] - cur);
+        if (hW) s += gEW * (pn[-1] - cur);
         if (n > 0) s += gup * (up - cur);
-        if (n < NL - 1) s += L4.z * (dn - cur);
-        s -= E4.z * cur;                         // sink / PCB to ambient (0 elsewhere)
+        if (n < NL - 1) s += gDn * (dn - cur);
+        s -= gAmb * cur;                         // sink / PCB to ambient (0 elsewhere)
         if (BND) {
-          const int nb = __float_as_int(E4.w);
           if (nb >= 0) {
-            if (gi == 0) s += E4.x * (sh.xs[nb + 2] - cur);
-            if (gi == nr - 1) s += E4.x * (sh.xs[nb + 3] - cur);
-            if (gj == nc - 1) s += E4.y * (sh.xs[nb + 1] - cur);
-            if (gj == 0) s += E4.y * (sh.xs[nb + 0] - cur);
+            if (gi == 0) s += gEdgeNS * (sh.xs[nb + 2] - cur);
+            if (gi == nr - 1) s += gEdgeNS * (sh.xs[nb + 3] - cur);
+            if (gj == nc - 1) s += gEdgeEW * (sh.xs[nb + 1] - cur);
+            if (gj == 0) s += gEdgeEW * (sh.xs[nb + 0] - cur);
           }
         }
-        o[n * LP] = P0 ? (__ldg(pw + (long long)n * C.plane) + s) * L4.w : s * (L4.w * hf);
-        gup = L4.z;
+        if constexpr (P0) o[n * LP] = (__ldg(pw + (long long)n * C.plane) + s) * invC;
+        else o[n * LP] = s * (invC * hf);
+        gup = gDn;
         up = cur;
         cur = dn;
       }
@@ -164,11 +187,11 @@ __device__ __forceinline__ void tb_pass(const TChip &C, const TSh &sh, const flo
   }
 }
 
-template <int NL, bool P0>
-__device__ __forceinline__ void tb_pass_any(bool bnd, const TChip &C, const TSh &sh, const float *src, float *dst,
-                                            int RI, int RJ, int m, int gi0, int gj0, float hf) {
-  if (bnd) tb_pass<NL, true, P0>(C, sh, src, dst, RI, RJ, m, gi0, gj0, hf);
-  else tb_pass<NL, false, P0>(C, sh, src, dst, RI, RJ, m, gi0, gj0, hf);
+template <typename V, int NL, bool P0>
+__device__ __forceinline__ void tb_pass_any(bool bnd, const TChip &C, const TSh<V> &sh, const V *src, V *dst,
+                                            int RI, int RJ, int m, int gi0, int gj0, V hf) {
+  if (bnd) tb_pass<V, NL, true, P0>(C, sh, src, dst, RI, RJ, m, gi0, gj0, hf);
+  else tb_pass<V, NL, false, P0>(C, sh, src, dst, RI, RJ, m, gi0, gj0, hf);
 }
 
 // the sides of the grid a sub-tile's own cells lie on: bit 0 N, 1 S, 2 W, 3 E
@@ -178,7 +201,8 @@ __device__ __forceinline__ int tb_sides(const TChip &C, int i0, int j0, int SI, 
 
 // edge sums over the sub-tile's own cells on the boundary: slot 0 from the
 // FP64 state (minus the node temperature), slot m + 1 from A_m in smem
-__device__ __forceinline__ void tb_edge_sums(const TChip &C, TSh &sh, const float *v, const double *yb, int slot,
+template <typename V>
+__device__ __forceinline__ void tb_edge_sums(const TChip &C, TSh<V> &sh, const V *v, const double *yb, int slot,
                                              int RI, int RJ, int H, int i0, int j0, int SI, int SJ, int sides) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int LP = RI * RJ;
@@ -207,8 +231,8 @@ __device__ __forceinline__ void tb_edge_sums(const TChip &C, TSh &sh, const floa
 // package input only through V_0; OUT: finish the own cells (candidate
 // state, error); SUMS: edge sums into sh.es.  phase 2 (V): package input
 // sh.Vp through every pass; OUT always.
-template <int NL>
-__device__ void tb_subtile(const TChip &C, TSh &sh, float *buf0, float *buf1, const double *__restrict__ yb,
+template <typename V, int NL>
+__device__ void tb_subtile(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, const double *__restrict__ yb,
                            double *__restrict__ yn, int i0, int j0, bool phase2, bool out, bool sums,
                            double h, double &errl) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -239,7 +263,7 @@ __device__ void tb_subtile(const TChip &C, TSh &sh, float *buf0, float *buf1, co
 #pragma unroll
     for (int n = 0; n < NL; n++) acc[s][n] = 0.0;
 
-  // the state box as FP32 deviations from ambient
+  // the state box as deviations from ambient in the kernel's type
   for (int r = w; r < RI; r += TB_WARPS) {
     const int gi = gi0 + r;
     if ((unsigned)gi >= (unsigned)nr) continue;
@@ -248,21 +272,21 @@ __device__ void tb_subtile(const TChip &C, TSh &sh, float *buf0, float *buf1, co
       if ((unsigned)gj >= (unsigned)nc) continue;
       const double *py = yb + (long long)gi * nc + gj;
 #pragma unroll
-      for (int n = 0; n < NL; n++) buf0[n * LP + r * RJ + c] = (float)(__ldcg(py + (long long)n * C.plane) - amb);
+      for (int n = 0; n < NL; n++) buf0[n * LP + r * RJ + c] = (V)(__ldcg(py + (long long)n * C.plane) - amb);
     }
   }
-  if (tid < C.nx) sh.xs[tid] = (float)(sh.yp[tid] - amb);
+  if (tid < C.nx) sh.xs[tid] = (V)(sh.yp[tid] - amb);
   __syncthreads();
-  if (sums) tb_edge_sums(C, sh, nullptr, yb, 0, RI, RJ, H, i0, j0, SI, SJ, sides);
+  if (sums) tb_edge_sums<V>(C, sh, nullptr, yb, 0, RI, RJ, H, i0, j0, SI, SJ, sides);
 
-  float *src = buf0, *dst = buf1;
-  const float hf = (float)h;
+  V *src = buf0, *dst = buf1;
+  const V hf = (V)h;
   for (int m = 0; m <= dE; m++) {
-    if (m == 0) tb_pass_any<NL, true>(bnd, C, sh, src, dst, RI, RJ, 0, gi0, gj0, 1.f);
-    else tb_pass_any<NL, false>(bnd, C, sh, src, dst, RI, RJ, m, gi0, gj0, hf);
+    if (m == 0) tb_pass_any<V, NL, true>(bnd, C, sh, src, dst, RI, RJ, 0, gi0, gj0, V(1));
+    else tb_pass_any<V, NL, false>(bnd, C, sh, src, dst, RI, RJ, m, gi0, gj0, hf);
     __syncthreads();
     // the next pass's package inputs (phase 1: none after V_0)
-    if (tid < C.nx) sh.xs[tid] = phase2 ? (float)sh.Vp[m][tid] : 0.f;
+    if (tid < C.nx) sh.xs[tid] = phase2 ? (V)sh.Vp[m][tid] : V(0);
     if (out) {
       const double cd = m <= dD ? sh.D.c[m] : 0.0, ce = m >= eLo ? sh.E.c[m] : 0.0;
       if (sep) {
@@ -294,8 +318,8 @@ __device__ void tb_subtile(const TChip &C, TSh &sh, float *buf0, float *buf1, co
         }
       }
     }
-    if (sums && m < dE) tb_edge_sums(C, sh, dst, yb, m + 1, RI, RJ, H, i0, j0, SI, SJ, sides);
-    float *t = src;
+    if (sums && m < dE) tb_edge_sums<V>(C, sh, dst, yb, m + 1, RI, RJ, H, i0, j0, SI, SJ, sides);
+    V *t = src;
     src = dst;
     dst = t;
     __syncthreads();
@@ -321,7 +345,8 @@ __device__ void tb_subtile(const TChip &C, TSh &sh, float *buf0, float *buf1, co
 // the package recursion: V^p_0 .. V^p_dE from the chip's edge sums of y and
 // of A_0 .. A_{dE-1} (sh.SA) and the edge-response table (one warp; lanes
 // are edges, then nodes)
-__device__ __forceinline__ void tb_package(const TChip &C, TSh &sh, double h) {
+template <typename V>
+__device__ __forceinline__ void tb_package(const TChip &C, TSh<V> &sh, double h) {
   const int lane = threadIdx.x & 31;
   const int nx = C.nx, ne = C.ne, dE = sh.dE;
   const PackF &P = *C.pk;
@@ -371,7 +396,8 @@ __device__ __forceinline__ void tb_package(const TChip &C, TSh &sh, double h) {
 
 // the attempt's coefficients (thread 0); returns 0, or 3 when the degree is
 // beyond what a sub-tile of this chip can hold
-__device__ int tb_plan(const TChip &C, TSh &sh, double h, bool first) {
+template <typename V>
+__device__ int tb_plan(const TChip &C, TSh<V> &sh, double h, bool first) {
   if (first) {
     for (int q = 0; q < PMAX; q++) sh.ps[q] = h;
     sh.E.n = sh.E1.n;
@@ -414,7 +440,8 @@ __device__ int tb_plan(const TChip &C, TSh &sh, double h, bool first) {
   return 3;
 }
 
-// FP32 grid power of interval iv for this CTA's tiles
+// grid power of interval iv for this CTA's tiles, in the kernel's type
+template <typename V>
 __device__ void tb_power(const TChip &C, int rank, int size, int K, int iv, const double *bpow, long long nbtot) {
   const double *b = K > 0 ? bpow + (long long)iv * nbtot + C.boff : nullptr;
   const bool last = K > 0 && iv == K - 1;
@@ -425,13 +452,15 @@ __device__ void tb_power(const TChip &C, int rank, int size, int K, int iv, cons
       const int n = k / (ni * nj), rem = k - n * (ni * nj), oi = rem / nj, oj = rem - (rem / nj) * nj;
       const long long qq = (long long)n * C.plane + (long long)(i0 + oi) * C.nc + (j0 + oj);
       if (K == 0) {
-        C.pf[qq] = (float)C.pgrid[qq];
+        if constexpr (sizeof(V) == 4) C.pf[qq] = (float)C.pgrid[qq];
+        else C.pd[qq] = C.pgrid[qq];
       } else {
         double val = 0.0;
         for (int e = C.b2g_ptr[qq]; e < C.b2g_ptr[qq + 1]; e++)
           val += C.b2g_occ[e] * b[C.b2g_blk[e]] / C.b2g_area[e];   // blist_avg, temperature_grid.c:331
         val *= C.cell_area;
-        C.pf[qq] = (float)val;
+        if constexpr (sizeof(V) == 4) C.pf[qq] = (float)val;
+        else C.pd[qq] = val;
         if (last) C.pgrid[qq] = val;
       }
     }
@@ -440,13 +469,17 @@ __device__ void tb_power(const TChip &C, int rank, int size, int K, int iv, cons
 
 // K sampling intervals (K = 0: one, power from C.pgrid) of one chip by a
 // group of `size` CTAs of which this is `rank`
-template <int NL>
-__device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh &sh, float *dyn, double T, int K,
+template <typename V, int NL>
+__device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh<V> &sh, V *dyn, double T, int K,
                         const double *bpow, long long nbtot, long long max_attempts) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int nx = C.nx;
-  float *buf0 = dyn, *buf1 = dyn + (size_t)C.rcap * NL;
-  if (tid < NL) sh.L[tid] = C.L[tid];
+  V *buf0 = dyn, *buf1 = dyn + (size_t)C.rcap * NL;
+  if constexpr (sizeof(V) == 4) {
+    if (tid < NL) sh.L[tid] = C.L[tid];
+  } else {
+    if (tid < NL) sh.L[tid] = C.Ld[tid];
+  }
   int cur = (int)out[6];
   if (tid < nx) sh.yp[tid] = __ldcg(C.y[cur] + C.ncell + tid);
   unsigned gen = 0;
@@ -457,7 +490,7 @@ __device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh 
   int iv = 0;
   if (rank == 0 && tid < 3) C.err[tid] = 0ull;
   for (iv = 0; iv < nint && !status && !sh.lost; iv++) {
-    tb_power(C, rank, size, K, iv, bpow, nbtot);
+    tb_power<V>(C, rank, size, K, iv, bpow, nbtot);
     tsync(C, size, gen, sh);
     t = 0.0;
     new_h = 1e-7;
@@ -493,7 +526,7 @@ __device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh 
               const bool ring = i0 < dE || j0 < dE || i0 + SI > C.nr - dE || j0 + SJ > C.nc - dE;
               const bool sums = tb_sides(C, i0, j0, SI, SJ) != 0;
               if (!ring || sums)
-                tb_subtile<NL>(C, sh, buf0, buf1, yb, yn, i0, j0, false, !ring, sums, h, errl);
+                tb_subtile<V, NL>(C, sh, buf0, buf1, yb, yn, i0, j0, false, !ring, sums, h, errl);
             }
           if (tsides) {   // this tile's partial edge sums
             const int ti = tt / C.ntj, tj = tt % C.ntj;
@@ -520,7 +553,7 @@ __device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh 
           if (lane == 0) sh.SA[slot][e] = s;
         }
         __syncthreads();
-        if (w == 0) tb_package(C, sh, h);
+        if (w == 0) tb_package<V>(C, sh, h);
         if (rank == 0 && tid == 0) C.err[(a + 1) % 3] = 0ull;
         __syncthreads();
         // ---- phase 2: V on the tiles within dE cells of the boundary
@@ -531,7 +564,7 @@ __device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh 
               const int i0 = ti0 + si, j0 = tj0 + sj;
               if (i0 >= C.nr || j0 >= C.nc) continue;
               const bool ring = i0 < dE || j0 < dE || i0 + SI > C.nr - dE || j0 + SJ > C.nc - dE;
-              if (ring) tb_subtile<NL>(C, sh, buf0, buf1, yb, yn, i0, j0, true, true, false, h, errl);
+              if (ring) tb_subtile<V, NL>(C, sh, buf0, buf1, yb, yn, i0, j0, true, true, false, h, errl);
             }
         }
         // ---- the error norm: cells (all CTAs of the chip) and package nodes
@@ -604,12 +637,14 @@ __device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh 
   }
 }
 
+template <typename V>
 __global__ void __launch_bounds__(TB_THREADS, 1)
     rk4_tb_kernel(const TChip *__restrict__ chips, const int4 *__restrict__ work, const int *__restrict__ wptr,
                   long long *__restrict__ out, double T, int K, const double *__restrict__ bpow, long long nbtot,
                   long long max_attempts) {
-  extern __shared__ __align__(16) float tdyn[];
-  __shared__ TSh sh;
+  extern __shared__ __align__(16) unsigned char tdyn_raw[];
+  V *tdyn = reinterpret_cast<V *>(tdyn_raw);
+  __shared__ TSh<V> sh;
   if (threadIdx.x == 0) {
     sh.lost = 0;
     // first-attempt coefficients for h = 1 (they scale with h), computed once
@@ -643,7 +678,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
     long long *o = out + (long long)it.x * TB_OUT;
     switch (C.nl) {
 #define TB_CASE(n) \
-  case n: tb_chip<n>(C, it.y, it.z, o, sh, tdyn, T, K, bpow, nbtot, max_attempts); break;
+  case n: tb_chip<V, n>(C, it.y, it.z, o, sh, tdyn, T, K, bpow, nbtot, max_attempts); break;
       TB_CASE(3) TB_CASE(4) TB_CASE(5) TB_CASE(6) TB_CASE(7) TB_CASE(8) TB_CASE(9) TB_CASE(10) TB_CASE(11)
       TB_CASE(12)
 #undef TB_CASE
@@ -657,11 +692,6 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
 // the edge-response table ER[j][e'][e] = sum over edge e of (L_cc^j L_cp
 // u_{e'}), FP64, from the model's FP64 layer coefficients
 // ---------------------------------------------------------------------------
-struct TLayerD {
-  double gNS, gEW, gDn, invC, gEdgeNS, gEdgeEW, gAmb;
-  int nbase;
-};
-
 __global__ void tb_er_seed(const TLayerD *__restrict__ L, int nl, int nr, int nc, int layer, int side,
                            double *__restrict__ u) {
   const long long n = (long long)nl * nr * nc;
@@ -762,9 +792,11 @@ bool tb_eligible(const hsb_dev_model *m) {
   return true;
 }
 
-size_t tb_static_smem() { return sizeof(TSh); }
+size_t tb_static_smem(bool fp64) { return fp64 ? sizeof(TSh<double>) : sizeof(TSh<float>); }
 
-const void *tb_kernel() { return (const void *)rk4_tb_kernel; }
+const void *tb_kernel(bool fp64) {
+  return fp64 ? (const void *)rk4_tb_kernel<double> : (const void *)rk4_tb_kernel<float>;
+}
 
 // layer tables (FP32 for the kernel, FP64 for the edge-response table)
 static void tb_tables(const hsb_dev_model *m, TLayer *Lf, TLayerD *Ld, int eg_layer[5], int eg_node[5], int *ne) {
@@ -848,13 +880,13 @@ double tb_tile_work(int oi, int oj) {
 // own-tile shape for a model with `ctas` co-resident CTAs: among the
 // candidates whose two region buffers fit next to the static shared memory,
 // the one with the least work for the busiest CTA (tiles dealt round-robin)
-int tb_tile_for(int nl, int nr, int nc, int ctas, size_t smem_cap, int *oi, int *oj) {
+int tb_tile_for(int nl, int nr, int nc, int ctas, size_t smem_cap, int *oi, int *oj, bool fp64) {
   static const int cand[][2] = {{16, 64}, {32, 32}, {16, 32}, {8, 64}, {8, 32}, {8, 16}};
   int best = -1;
   double best_cost = 0.0;
   for (int k = 0; k < 6; k++) {
     const size_t rc = (size_t)(cand[k][0] + 16) * (cand[k][1] + 16);
-    if (2 * rc * nl * 4 + tb_static_smem() > smem_cap) continue;
+    if (2 * rc * nl * (fp64 ? 8 : 4) + tb_static_smem(fp64) > smem_cap) continue;
     const long long tiles = (long long)((nr + cand[k][0] - 1) / cand[k][0]) * ((nc + cand[k][1] - 1) / cand[k][1]);
     const double cost = (double)((tiles + ctas - 1) / ctas) * tb_tile_work(cand[k][0], cand[k][1]);
     if (best < 0 || cost < best_cost) {
@@ -868,14 +900,17 @@ int tb_tile_for(int nl, int nr, int nc, int ctas, size_t smem_cap, int *oi, int 
   return HSB_OK;
 }
 
-size_t tb_dyn_smem(int nl, int oi, int oj) { return (size_t)2 * (oi + 16) * (oj + 16) * nl * 4; }
+size_t tb_dyn_smem(int nl, int oi, int oj, bool fp64) {
+  return (size_t)2 * (oi + 16) * (oj + 16) * nl * (fp64 ? 8 : 4);
+}
 
-int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1, float *pf, int oi, int oj,
-                 TChip *C) {
+int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1, float *pf, double *pd, int oi,
+                 int oj, TChip *C) {
   memset(C, 0, sizeof(*C));
   C->y[0] = const_cast<double *>(y0);
   C->y[1] = const_cast<double *>(y1);
   C->pf = pf;
+  C->pd = pd;
   C->pgrid = m->pgrid;
   C->boff = 0;
   C->b2g_ptr = m->b2g_ptr;
@@ -884,6 +919,7 @@ int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1,
   C->b2g_area = m->b2g_area;
   C->cell_area = m->cell_area;
   C->L = r->L;
+  C->Ld = r->Ld;
   C->pk = r->pk;
   C->er = r->er;
   C->part = r->part;
@@ -914,7 +950,7 @@ int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1,
 
 void tb_res_free(TbRes *r) {
   if (!r) return;
-  void *d[] = {r->L, r->part, r->err, r->bar, r->d_chip};   // pk is the fast workspace's; er the cache's
+  void *d[] = {r->L, r->Ld, r->part, r->err, r->bar, r->d_chip};   // pk is the fast workspace's; er the cache's
   for (void *p : d)
     if (p) cudaFree(p);
   delete r;
@@ -945,19 +981,22 @@ int tb_res_prepare(hsb_dev_model *m, TbRes **out, const PackF *pk_dev) {
     // partial edge sums per own tile along each edge: the smallest tile is 8 wide
     r->segmax = (std::max(m->nr, m->nc) + 7) / 8;
     HSB_CUDA(cudaMalloc(&r->L, sizeof(TLayer) * TB_NLMAX));
+    HSB_CUDA(cudaMalloc(&r->Ld, sizeof(TLayerD) * TB_NLMAX));
     HSB_CUDA(cudaMalloc(&r->part, sizeof(double) * (TB_DMAX + 1) * NEDGE * r->segmax));
     HSB_CUDA(cudaMalloc(&r->err, sizeof(unsigned long long) * 4));
     HSB_CUDA(cudaMalloc(&r->bar, sizeof(unsigned) * 2));
     HSB_CUDA(cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, m->stream));
-    HSB_CUDA(cudaMalloc(&r->d_chip, sizeof(TChip)));
+    HSB_CUDA(cudaMalloc(&r->d_chip, sizeof(TChip) * 4));
   }
   r->pk = const_cast<PackF *>(pk_dev);
   if (r->version == m->coef_version) return HSB_OK;
   TLayer Lf[TB_NLMAX];
   TLayerD Ld[TB_NLMAX];
   memset(Lf, 0, sizeof(Lf));
+  memset(Ld, 0, sizeof(Ld));
   tb_tables(m, Lf, Ld, r->eg_layer, r->eg_node, &r->ne);
   HSB_CUDA(cudaMemcpyAsync(r->L, Lf, sizeof(TLayer) * m->nl, cudaMemcpyHostToDevice, m->stream));
+  HSB_CUDA(cudaMemcpyAsync(r->Ld, Ld, sizeof(TLayerD) * m->nl, cudaMemcpyHostToDevice, m->stream));
   // the edge-response table: from the cache, or computed and added to it
   std::vector<double> coef;
   for (int l = 0; l < m->nl; l++) {

@@ -23,16 +23,24 @@ struct alignas(16) TLayer {
   int nbase;                        // W node of this layer's package group (W, E, N, S), -1: none
 };
 
+// the same in FP64, for the all-FP64 variant of the kernel
+struct alignas(16) TLayerD {
+  double gNS, gEW, gDn, invC, gEdgeNS, gEdgeEW, gAmb;
+  int nbase, pad;
+};
+
 // one chip (model) as the kernel sees it
 struct TChip {
   double *y[2];                     // state buffers: y[out[6]] holds the state at launch
-  float *pf;                        // FP32 grid power
+  float *pf;                        // FP32 grid power (FP32 kernel)
+  double *pd;                       // FP64 grid power (FP64 kernel; a scratch vector of ncell doubles)
   double *pgrid;                    // FP64 grid power (K = 0: source; K > 0: the last interval's, written)
   long long boff;                   // K > 0: this chip's block powers of interval k at bpow + k * nbtot + boff
   const int *b2g_ptr, *b2g_blk;
   const double *b2g_occ, *b2g_area;
   double cell_area;
   const TLayer *L;
+  const TLayerD *Ld;
   const PackF *pk;
   const double *er;                 // [TB_JMAX][ne][ne] edge responses
   double *part;                     // [TB_DMAX + 1][NEDGE][segmax] per-tile edge sums
@@ -50,29 +58,31 @@ struct TChip {
 // per-model resources
 struct TbRes {
   TLayer *L;
+  TLayerD *Ld;
   PackF *pk;
   double *er;
   double *part;
   unsigned long long *err;
   unsigned *bar;
-  TChip *d_chip;                    // [2]: state in the first buffer / in the second
-  const double *chip_y0, *chip_y1;  // the buffers d_chip[0] describes (y, ytemp)
-  int chip_oi, chip_oj;
+  TChip *d_chip;                    // [variant * 2 + role]: FP32 / FP64 kernel; state in the first buffer / second
+  const double *chip_y0, *chip_y1;  // the buffers d_chip[v * 2] describes (y, ytemp)
+  int chip_oi[2], chip_oj[2];       // per variant: own tile (0: not chosen yet)
   int version, ne, segmax;
   int eg_layer[5], eg_node[5];
-  int grid;                         // co-resident CTAs of a single-model launch
-  size_t dyn;                       // dynamic shared memory of that launch
+  int grid[2];                      // per variant: co-resident CTAs of a single-model launch
+  size_t dyn[2];                    // per variant: dynamic shared memory of that launch
 };
 
+// fp64: the all-FP64 variant (stencil passes in FP64 too)
 bool tb_eligible(const hsb_dev_model *m);
-const void *tb_kernel();
-size_t tb_static_smem();
-size_t tb_dyn_smem(int nl, int oi, int oj);
-int tb_tile_for(int nl, int nr, int nc, int ctas, size_t smem_cap, int *oi, int *oj);
+const void *tb_kernel(bool fp64 = false);
+size_t tb_static_smem(bool fp64 = false);
+size_t tb_dyn_smem(int nl, int oi, int oj, bool fp64 = false);
+int tb_tile_for(int nl, int nr, int nc, int ctas, size_t smem_cap, int *oi, int *oj, bool fp64 = false);
 double tb_tile_work(int oi, int oj);
 int tb_res_prepare(hsb_dev_model *m, TbRes **r, const PackF *pk_dev);
 void tb_res_free(TbRes *r);
-int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1, float *pf, int oi, int oj,
-                 TChip *C);
+int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1, float *pf, double *pd, int oi,
+                 int oj, TChip *C);
 
 }  // namespace hsb

@@ -42,6 +42,9 @@ extern "C" {
 #define HSB_FORM_FAST_STAGES 2  /* the fast transient evaluated stage by stage     */
 #define HSB_FORM_FAST_PASSES 3  /* the fast transient with one grid-wide pass per Krylov
                                    vector (no temporal blocking); same arithmetic */
+#define HSB_FORM_FP64_BLOCKED 4 /* transient: the temporally blocked Krylov form with every
+                                   stencil pass in FP64 (per-layer models of 3..12 layers),
+                                   within 1e-6 K of the FP64 replay; steady as HSB_FORM_PARITY */
 
 /* steady methods */
 #define HSB_STEADY_AUTO       0  /* GS replay for FORM_PARITY; MG-PCG (or BiCGStab with advection) for FORM_FAST */

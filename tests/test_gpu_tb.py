@@ -7,6 +7,10 @@ for models with per-layer conductances) against
   only in the order of the FP64 sums of increment, error and edge sums);
 * the oracle's FP64 replay of the reference: 0.01 K.
 
+The same kernel with every stencil pass in FP64 (HSB_FORM_FP64_BLOCKED)
+must stay within 1e-6 K of the FP64 replay of the reference's RK4 with the
+same accepted steps.
+
 Cases cover tiles that are all boundary ("ring") tiles (16x16), grids with
 interior tiles (256x256), rectangular grids, the secondary heat path (28
 package nodes, 20 edges), 3-D stacks, and long sampling intervals whose
@@ -16,7 +20,7 @@ halo in sub-tiles).
 import numpy as np
 import pytest
 
-from hotspot_b200 import FORM_FAST, FORM_FAST_PASSES
+from hotspot_b200 import FORM_FAST, FORM_FAST_PASSES, FORM_FP64_BLOCKED, FORM_PARITY
 from hotspot_b200 import model as hm
 from hotspot_b200 import workloads as W
 from oracle.restatement import OracleModel
@@ -104,3 +108,18 @@ def test_blocked_against_fp64_oracle(workdir, case):
         o.compute_temp(o.power_vector(sc.block_power[k]), to if k == 0 else None, sc.dt)
         assert np.max(np.abs(ta[k] - to)) <= TOL_FP64, k
     assert np.max(np.abs(ga - o.grid("trans"))) <= TOL_FP64
+
+
+TOL_REPLAY = 1e-6
+
+
+@pytest.mark.parametrize("case", ["chip2d16", "chip2d64", "secondary", "stack64", "stack256", "rect128x32",
+                                  "long_chip2d", "long_stack"])
+def test_fp64_blocked_matches_replay(workdir, case):
+    sc = _scenario(workdir, case)
+    rows = min(sc.steps, sc.block_power.shape[0])
+    ta, ga, sa, aa, fa = _run(sc, FORM_FP64_BLOCKED, rows)
+    tb, gb, sb, ab, fb = _run(sc, FORM_PARITY, rows)
+    assert sa == sb and aa == ab, (sa, aa, sb, ab)
+    assert np.max(np.abs(ta - tb)) <= TOL_REPLAY
+    assert np.max(np.abs(ga - gb)) <= TOL_REPLAY
