@@ -69,8 +69,12 @@ def parse():
     ap.add_argument("--chip2d-rows", type=int, default=1000, help="rows of the 2-D chip leg's trace")
     ap.add_argument("--batch-chips", type=int, default=512)
     ap.add_argument("--batch-intervals", type=int, default=200)
-    ap.add_argument("--serving-seconds", type=float, default=0.25,
+    ap.add_argument("--serving-seconds", type=float, default=1.0,
                     help="length of the request arrival window of the serving leg at 2000 req/s")
+    ap.add_argument("--serving-probe-rate", type=float, default=220.0,
+                    help="rate of the SLO-class probe stream added to the 2000 req/s mix")
+    ap.add_argument("--serving-replicas", type=int, default=3,
+                    help="resident models per serving class of side <= 256")
     ap.add_argument("--serving-calm-rate", type=float, default=30.0,
                     help="offered rate of the serving leg's second, sustainable run")
     ap.add_argument("--serving-calm-seconds", type=float, default=4.0)
@@ -476,25 +480,30 @@ def leg_microchannel(args):
 
 
 def leg_serving(args):
-    """The serving mix through hsb_server_run: at the offered 2000 req/s, and
-    at a sustainable rate where latency reflects service rather than queueing."""
+    """The serving mix through hsb_server_run: at the offered 2000 req/s (with
+    a probe stream of the latency-SLO class so its p99 rests on >= 200
+    samples), and at a sustainable rate where latency reflects service
+    rather than queueing."""
     from hotspot_b200.serving import Request, Server, latency_report, serving_mix
     d = tempfile.mkdtemp(prefix="hsb_srv_")
-    srv = Server(workers=8)
+    workers = 8
+    srv = Server(workers=workers)
     t0 = time.perf_counter()
     hp = [(256, 4)]              # the latency-SLO class (256x256, 4 chip layers, steady): high priority
-    mix = serving_mix(d, srv, seed=4, rate=2000.0, duration=args.serving_seconds, high_priority_classes=hp)
+    mix = serving_mix(d, srv, seed=4, rate=2000.0, duration=args.serving_seconds, high_priority_classes=hp,
+                      replicas=args.serving_replicas, probe_rate=args.serving_probe_rate, probe_class=hp[0])
     calm = serving_mix(d, srv, seed=5, rate=args.serving_calm_rate, duration=args.serving_calm_seconds,
-                       high_priority_classes=hp, reuse=mix)
-    # every resident model serves one request before the clock starts
+                       high_priority_classes=hp, reuse=mix, replicas=args.serving_replicas)
+    # every resident model (every member of every pool) serves one request before the clock starts
     warm = []
     for _, mi in mix.classes.items():
         r0 = next((r for r in mix.requests + calm.requests if r.model == mi), None)
         if r0 is None:
             continue
         steps = 1 if r0.kind == 0 else 2
-        warm.append(Request(r0.model, r0.kind, r0.power if steps == 1 else r0.power[:2], 0.0, r0.temp_in,
-                            steps, r0.dt, r0.tag))
+        for _ in range(mix.members.get(mi, 1)):
+            warm.append(Request(r0.model, r0.kind, r0.power if steps == 1 else r0.power[:2], 0.0, r0.temp_in,
+                                steps, r0.dt, r0.tag))
     srv.run(warm)
     setup_s = time.perf_counter() - t0
 
@@ -510,14 +519,16 @@ def leg_serving(args):
                 "latency_steady_256x256_4layers": latency_report(reqs, tag),
                 "service_ms_steady_256x256_4layers": float(np.median(svc)) if svc else None}
     srv.run(mix.requests)
-    loaded = report(mix.requests, 2000.0, args.serving_seconds)
+    loaded = report(mix.requests, 2000.0 + args.serving_probe_rate, args.serving_seconds)
     srv.run(calm.requests)
     sustainable = report(calm.requests, args.serving_calm_rate, args.serving_calm_seconds)
-    res = {"workload": "Poisson arrivals: 70% steady (sides 64..1024, 1..8 chip layers), 30% 500-interval "
-                       "transients (sides 64..256); one resident model per class; the 256x256x4-layer steady "
-                       "class (the latency SLO) in the high-priority class, with 2 reserved workers; other "
-                       "requests pause between transient chunks and steady refinement passes while it runs",
-           "models": len(mix.models), "workers": 8, "offered_2000_req_per_s": loaded,
+    res = {"workload": "Poisson arrivals at 2000 req/s: 70% steady (sides 64..1024, 1..8 chip layers), 30% "
+                       "500-interval transients (sides 64..256); plus a probe stream of the latency-SLO class "
+                       f"(256x256, 4 chip layers, steady) at {args.serving_probe_rate:g} req/s; "
+                       f"{args.serving_replicas} resident models per class of side <= 256 (a pool), one above; "
+                       "the SLO class in the high-priority class with 2 reserved workers; other requests pause "
+                       "between transient chunks and steady refinement passes while it runs",
+           "models": len(mix.models), "workers": workers, "offered_2000_req_per_s": loaded,
            "sustainable_rate": sustainable, "setup_s": setup_s}
     srv.close()
     for m in mix.models:

@@ -125,6 +125,7 @@ class Mix:
     requests: list
     classes: dict = field(default_factory=dict)   # (kind, side, layers) -> model (pool) index
     models: list = field(default_factory=list)
+    members: dict = field(default_factory=dict)   # pool index -> number of resident models in it
 
 
 def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.0, duration: float = 1.0,
@@ -132,7 +133,7 @@ def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.
                 steady_sides=(64, 128, 256, 512, 1024), transient_sides=(64, 128, 256),
                 max_layers: int = 8, model_factory=None, high_priority_cells: int = 0,
                 high_priority_classes=(), reuse: Mix | None = None, replicas: int = 1,
-                replica_max_side: int = 256) -> Mix:
+                replica_max_side: int = 256, probe_rate: float = 0.0, probe_class=(256, 4)) -> Mix:
     """Seeded Poisson arrivals at `rate` req/s for `duration` s.  Steady
     requests: side drawn log-uniformly from `steady_sides`, 1..max_layers
     chip layers; transients: `transient_steps` intervals of `dt` on
@@ -145,15 +146,21 @@ def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.
     high priority class.  `reuse`: the resident models of an earlier mix on
     the same server serve the classes they cover.  `replicas`: resident
     models per class of side at most `replica_max_side` (a pool; requests of
-    one class then run concurrently on its idle members)."""
+    one class then run concurrently on its idle members).  `probe_rate`: an
+    extra seeded Poisson stream of steady requests of `probe_class` (side,
+    chip layers) at that rate over the same window, tagged like the class's
+    own requests, so a latency percentile of that class rests on enough
+    samples."""
     from . import model as hm
     rng = np.random.default_rng(seed)
     mix = Mix(requests=[])
     if reuse is not None:
-        mix.classes, mix.models = reuse.classes, reuse.models
-    t = 0.0
+        mix.classes, mix.models, mix.members = reuse.classes, reuse.models, reuse.members
     model_factory = model_factory or hm.from_scenario
     scen = {}
+    # arrivals: the mix, then the probe stream, merged in time order
+    arrivals = []
+    t = 0.0
     while True:
         t += rng.exponential(1.0 / rate)
         if t >= duration:
@@ -162,6 +169,17 @@ def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.
         sides = steady_sides if steady else transient_sides
         side = int(sides[rng.integers(0, len(sides))])
         layers = int(rng.integers(1, max_layers + 1))
+        arrivals.append((t, steady, side, layers))
+    if probe_rate > 0:
+        prng = np.random.default_rng([seed, 7919])
+        t = 0.0
+        while True:
+            t += prng.exponential(1.0 / probe_rate)
+            if t >= duration:
+                break
+            arrivals.append((t, True, int(probe_class[0]), int(probe_class[1])))
+        arrivals.sort(key=lambda a: a[0])
+    for t, steady, side, layers in arrivals:
         key = ("steady" if steady else "transient", side, layers)
         if key not in mix.classes:
             crng = np.random.default_rng([seed, side, layers, int(steady)])
@@ -173,10 +191,12 @@ def serving_mix(workdir: str, server: Server, seed: int = 0, rate: float = 2000.
             mix.classes[key] = server.add_model(m, FORM_FAST, 1e-5)
             if steady and (m.n_cells <= high_priority_cells or (side, layers) in set(high_priority_classes)):
                 server.set_priority(mix.classes[key], True)
+            mix.members[mix.classes[key]] = 1
             for _ in range(replicas - 1 if side <= replica_max_side else 0):
                 rep = model_factory(sc)
                 mix.models.append(rep)
                 server.add_replica(mix.classes[key], rep)
+                mix.members[mix.classes[key]] += 1
         mi = mix.classes[key]
         m = server.models[mi]
         nblk = sum(m.layer_units[l] for l in range(m.n_layers) if m.layer_power[l])

@@ -86,3 +86,42 @@ def test_admission_refuses_what_does_not_fit(workdir):
     assert r.status == -3                               # HSB_E_NOMEM
     srv.close()
     m.close()
+
+
+def test_pool_members_serve_one_class(workdir):
+    """A pool of resident models of one class: requests naming the pool run on
+    whichever member is idle, concurrently; each result equals the result of
+    the same request alone on the pool's first model, bit for bit (members
+    are built from the same scenario and every request carries its inputs)."""
+    rng = np.random.default_rng(93)
+    sc = W.scenario_random_chip(workdir, rng, "p", side=128, chip_layers=3, steps=0)
+    members = [hm.from_scenario(sc) for _ in range(3)]
+    srv = Server(workers=4)
+    pool = srv.add_model(members[0], _abi.FORM_FAST, 1e-6)
+    for m in members[1:]:
+        srv.add_replica(pool, m)
+    m = members[0]
+    nblk = sum(m.layer_units[l] for l in range(m.n_layers) if m.layer_power[l])
+    reqs, t = [], 0.0
+    r2 = np.random.default_rng(94)
+    for k in range(12):
+        t += r2.exponential(1.0 / 5000.0)
+        if k % 2:
+            reqs.append(Request(pool, _abi.REQ_STEADY, m.power_vector(r2.uniform(0.5, 20.0, nblk)), t, tag="s"))
+        else:
+            trace = W.ar1_power(r2, r2.uniform(0.5, 20.0, nblk), 20)
+            p = np.stack([m.power_vector(trace[s]) for s in range(20)])
+            reqs.append(Request(pool, _abi.REQ_TRANSIENT, p, t, temp_in=m.vector(m.config.init_temp), steps=20,
+                                dt=3.333e-6, tag="t"))
+    alone = [Request(r.model, r.kind, r.power, 0.0, r.temp_in, r.steps, r.dt, r.tag) for r in reqs]
+    for r in alone:
+        srv.run([r])
+    srv.run(reqs)
+    for a, b in zip(alone, reqs):
+        assert a.status == 0 and b.status == 0
+        assert np.array_equal(a.out, b.out), (a.tag, np.max(np.abs(a.out - b.out)))
+    spans = sorted((r.start, r.finish) for r in reqs)
+    assert any(spans[k + 1][0] < spans[k][1] for k in range(len(spans) - 1)), "no two requests of the pool overlapped"
+    srv.close()
+    for mm in members:
+        mm.close()
