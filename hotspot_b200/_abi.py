@@ -230,6 +230,7 @@ _SIGS = {
                                           C.POINTER(Stats)]),
     "hsb_dev_get_state": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "hsb_dev_workspaces": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "hsb_dev_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "hsb_dev_set_state": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "hsb_abi_sizes": (C.c_int, [C.POINTER(C.c_longlong), C.c_int]),
     "hsb_dev_transient_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,

@@ -763,6 +763,13 @@ int hsb_dev_get_state(hsb_dev_model *m, int which, double *out) {
   return HSB_OK;
 }
 
+int hsb_dev_set_tile(hsb_dev_model *m, int rows, int cols) {
+  if (!m || rows < 0 || cols < 0 || (rows == 0) != (cols == 0)) return set_error(HSB_E_ARG, "bad tile");
+  m->tile_oi = rows;
+  m->tile_oj = cols;
+  return HSB_OK;
+}
+
 int hsb_dev_workspaces(const hsb_dev_model *m, int *mask) {
   if (!m || !mask) return set_error(HSB_E_ARG, "null argument");
   *mask = (m->fast ? HSB_WS_FAST_TRANSIENT : 0) | (m->mg ? HSB_WS_MG : 0) | (m->krylov ? HSB_WS_BICGSTAB : 0);

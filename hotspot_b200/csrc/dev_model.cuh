@@ -123,6 +123,7 @@ struct hsb_dev_model {
   // applies (rk4_tb.cu), 1 one grid-wide pass per Krylov vector (rk4_krylov.cu),
   // 2 the temporally blocked one with FP64 passes
   int fast_passes;
+  int tile_oi, tile_oj;          // the blocked kernel's own tile requested for this model (0: automatic)
   void *fast;
   void (*fast_free)(void *);
   void *mg;

@@ -955,12 +955,18 @@ __global__ void pcg_update_xr(float *__restrict__ x, float *__restrict__ r, cons
   }
 }
 
-// p = z + beta p with beta = rz_new / rz_old
+// p = z + beta p with beta = rz_new / rz_old; the first iteration sets p = z
+// without reading p (whatever the buffer held, NaN bit patterns included)
 __global__ void pcg_update_p(float *__restrict__ p, const float *__restrict__ z, const double *__restrict__ sc,
                              long long n, int first) {
-  const float beta = first ? 0.f : (float)(sc[2] / sc[0]);
   long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) p[k] = z[k] + beta * p[k];
+  if (k >= n) return;
+  if (first) {
+    p[k] = z[k];
+    return;
+  }
+  const float beta = (float)(sc[2] / sc[0]);
+  p[k] = z[k] + beta * p[k];
 }
 
 // T += e; the max |e| (K) into *emax_bits (zeroed by the caller)
@@ -1058,6 +1064,15 @@ static MgLevelDev dev_level(const hsb_dev_model *m, const MgLevel &L, int lvl) {
 
 static void free_mg(void *p);
 
+// workspace arrays start zeroed: no kernel of the solver depends on what an
+// earlier allocation left in the memory it reuses
+template <typename Tp>
+static cudaError_t mg_alloc(Tp **p, size_t bytes) {
+  cudaError_t e = cudaMalloc((void **)p, bytes);
+  if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);
+  return e;
+}
+
 static int mg_setup(hsb_dev_model *m, MgWork **out) {
   MgWork *w = new MgWork();
   w->coef_version = -1;
@@ -1077,35 +1092,35 @@ static int mg_setup(hsb_dev_model *m, MgWork **out) {
   w->nlev = (int)w->lv.size();
   for (int l = 0; l < w->nlev; l++) {
     MgLevel &L = w->lv[l];
-    HSB_CUDA(cudaMalloc(&L.gE, sizeof(float) * L.ncell));
-    HSB_CUDA(cudaMalloc(&L.gS, sizeof(float) * L.ncell));
-    HSB_CUDA(cudaMalloc(&L.gB, sizeof(float) * L.ncell));
-    HSB_CUDA(cudaMalloc(&L.diag, sizeof(float) * L.ncell));
-    HSB_CUDA(cudaMalloc(&L.gAmbL, sizeof(float) * HSB_MAX_LAYERS));
-    HSB_CUDA(cudaMalloc(&L.gEdgeNS, sizeof(float) * HSB_MAX_LAYERS));
-    HSB_CUDA(cudaMalloc(&L.gEdgeEW, sizeof(float) * HSB_MAX_LAYERS));
-    HSB_CUDA(cudaMalloc(&L.x, sizeof(float) * L.n));
-    HSB_CUDA(cudaMalloc(&L.f, sizeof(float) * L.n));
-    HSB_CUDA(cudaMalloc(&L.r, sizeof(float) * L.n));
-    HSB_CUDA(cudaMalloc(&L.pinv, sizeof(float) * NXP * NXP));
+    HSB_CUDA(mg_alloc(&L.gE, sizeof(float) * L.ncell));
+    HSB_CUDA(mg_alloc(&L.gS, sizeof(float) * L.ncell));
+    HSB_CUDA(mg_alloc(&L.gB, sizeof(float) * L.ncell));
+    HSB_CUDA(mg_alloc(&L.diag, sizeof(float) * L.ncell));
+    HSB_CUDA(mg_alloc(&L.gAmbL, sizeof(float) * HSB_MAX_LAYERS));
+    HSB_CUDA(mg_alloc(&L.gEdgeNS, sizeof(float) * HSB_MAX_LAYERS));
+    HSB_CUDA(mg_alloc(&L.gEdgeEW, sizeof(float) * HSB_MAX_LAYERS));
+    HSB_CUDA(mg_alloc(&L.x, sizeof(float) * L.n));
+    HSB_CUDA(mg_alloc(&L.f, sizeof(float) * L.n));
+    HSB_CUDA(mg_alloc(&L.r, sizeof(float) * L.n));
+    HSB_CUDA(mg_alloc(&L.pinv, sizeof(float) * NXP * NXP));
   }
   const long long n0 = w->lv[0].n, ncell = m->ncell;
-  HSB_CUDA(cudaMalloc(&w->gE64, sizeof(double) * ncell));
-  HSB_CUDA(cudaMalloc(&w->gS64, sizeof(double) * ncell));
-  HSB_CUDA(cudaMalloc(&w->gB64, sizeof(double) * ncell));
-  HSB_CUDA(cudaMalloc(&w->gAmb64, sizeof(double) * (HSB_MAX_LAYERS + 3 * NXP + NXP * NXP)));
-  HSB_CUDA(cudaMalloc(&w->gEdgeNS64, sizeof(double) * HSB_MAX_LAYERS));
-  HSB_CUDA(cudaMalloc(&w->gEdgeEW64, sizeof(double) * HSB_MAX_LAYERS));
-  HSB_CUDA(cudaMalloc(&w->r64, sizeof(double) * n0));
-  HSB_CUDA(cudaMalloc(&w->b64, sizeof(double) * n0));
-  HSB_CUDA(cudaMalloc(&w->p, sizeof(float) * n0));
-  HSB_CUDA(cudaMalloc(&w->q, sizeof(float) * n0));
-  HSB_CUDA(cudaMalloc(&w->z, sizeof(float) * n0));
-  HSB_CUDA(cudaMalloc(&w->e, sizeof(float) * n0));
-  HSB_CUDA(cudaMalloc(&w->rr, sizeof(float) * n0));
-  HSB_CUDA(cudaMalloc(&w->red, sizeof(double) * 4096));
-  HSB_CUDA(cudaMalloc(&w->d_ps, sizeof(PackSys)));
-  HSB_CUDA(cudaMalloc(&w->dot_ticket, sizeof(unsigned)));
+  HSB_CUDA(mg_alloc(&w->gE64, sizeof(double) * ncell));
+  HSB_CUDA(mg_alloc(&w->gS64, sizeof(double) * ncell));
+  HSB_CUDA(mg_alloc(&w->gB64, sizeof(double) * ncell));
+  HSB_CUDA(mg_alloc(&w->gAmb64, sizeof(double) * (HSB_MAX_LAYERS + 3 * NXP + NXP * NXP)));
+  HSB_CUDA(mg_alloc(&w->gEdgeNS64, sizeof(double) * HSB_MAX_LAYERS));
+  HSB_CUDA(mg_alloc(&w->gEdgeEW64, sizeof(double) * HSB_MAX_LAYERS));
+  HSB_CUDA(mg_alloc(&w->r64, sizeof(double) * n0));
+  HSB_CUDA(mg_alloc(&w->b64, sizeof(double) * n0));
+  HSB_CUDA(mg_alloc(&w->p, sizeof(float) * n0));
+  HSB_CUDA(mg_alloc(&w->q, sizeof(float) * n0));
+  HSB_CUDA(mg_alloc(&w->z, sizeof(float) * n0));
+  HSB_CUDA(mg_alloc(&w->e, sizeof(float) * n0));
+  HSB_CUDA(mg_alloc(&w->rr, sizeof(float) * n0));
+  HSB_CUDA(mg_alloc(&w->red, sizeof(double) * 4096));
+  HSB_CUDA(mg_alloc(&w->d_ps, sizeof(PackSys)));
+  HSB_CUDA(mg_alloc(&w->dot_ticket, sizeof(unsigned)));
   HSB_CUDA(cudaMemset(w->dot_ticket, 0, sizeof(unsigned)));
   if (w->lv[0].plane >= (1LL << 31) - MGT) return set_error(HSB_E_ARG, "multigrid: more than 2^31 columns per layer");
 

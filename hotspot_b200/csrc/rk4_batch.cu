@@ -53,8 +53,11 @@ void policy_tile(int policy, int nr, int nc, int nl, size_t cap, int *oi, int *o
   const int *t = side >= 256 ? P.big : side >= 64 ? P.mid : P.small;
   *oi = t[0];
   *oj = t[1];
-  // smaller tiles when the layer count does not fit shared memory
-  while (2 * (size_t)(*oi + 16) * (*oj + 16) * nl * 4 + tb_static_smem() > cap && (*oi > 8 || *oj > 16)) {
+  // smaller tiles when the layer count does not fit shared memory or the
+  // threads' accumulator slots
+  while ((2 * (size_t)tb_rcap(nl, *oi, *oj, false, cap) * nl * 4 + tb_static_smem() > cap ||
+          *oi * *oj > TB_THREADS * tb_slots_rt(false, nl)) &&
+         (*oi > 8 || *oj > 16)) {
     if (*oj >= *oi * 2) *oj /= 2;
     else *oi /= 2;
   }
@@ -132,10 +135,10 @@ static int batch_tiles(hsb_batch *b) {
     TChip &C = b->h_chips[c];
     double *y0 = C.y[0], *y1 = C.y[1];
     int rc;
-    if ((rc = tb_fill_chip(m, r, y0, y1, w->pf, w->t1, oi, oj, &C))) return rc;
+    if ((rc = tb_fill_chip(m, r, y0, y1, w->pf, w->t1, oi, oj, false, b->cap, &C))) return rc;
     C.bar = b->d_bar + 2 * c;
     C.boff = b->boff[c];
-    b->dyn = std::max(b->dyn, tb_dyn_smem(m->nl, oi, oj));
+    b->dyn = std::max(b->dyn, tb_dyn_smem(m->nl, oi, oj, false, b->cap));
   }
   if (b->dyn + tb_static_smem() > b->cap) return set_error(HSB_E_ARG, "batch tiles do not fit shared memory");
   HSB_CUDA(cudaMemcpy(b->d_chips, b->h_chips.data(), sizeof(TChip) * b->n, cudaMemcpyHostToDevice));

@@ -642,13 +642,18 @@ static int tb_prepare_single(hsb_dev_model *m, FastWork *w) {
   if (rc) return rc;
   const int v = m->fast_passes == 2 ? 1 : 0;   // kernel variant: FP32 or FP64 passes
   const bool fp64 = v == 1;
+  if (m->tile_oi > 0 && (r->chip_oi[v] != m->tile_oi || r->chip_oj[v] != m->tile_oj)) r->chip_oi[v] = 0;
   if (r->chip_oi[v] == 0) {
     int nsm = 0, cap = 0;
     HSB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device));
     HSB_CUDA(cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, m->device));
-    int oi = 0, oj = 0;
-    if ((rc = tb_tile_for(m->nl, m->nr, m->nc, nsm, (size_t)cap, &oi, &oj, fp64))) return rc;
-    const size_t dyn = tb_dyn_smem(m->nl, oi, oj, fp64);
+    int oi = m->tile_oi, oj = m->tile_oj;
+    if (oi <= 0 && (rc = tb_tile_for(m->nl, m->nr, m->nc, nsm, (size_t)cap, &oi, &oj, fp64))) return rc;
+    if (oi * oj > TB_THREADS * tb_slots_rt(fp64, m->nl) ||
+        2 * (size_t)tb_rcap(m->nl, oi, oj, fp64, (size_t)cap) * m->nl * (fp64 ? 8 : 4) + tb_static_smem(fp64) >
+            (size_t)cap)
+      return set_error(HSB_E_ARG, "requested tile of the blocked transient kernel does not fit");
+    const size_t dyn = tb_dyn_smem(m->nl, oi, oj, fp64, (size_t)cap);
     if ((rc = raise_smem_limit(tb_kernel(fp64), dyn))) return rc;
     int per_sm = 0;
     HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tb_kernel(fp64), TB_THREADS, dyn));
@@ -658,6 +663,7 @@ static int tb_prepare_single(hsb_dev_model *m, FastWork *w) {
     r->dyn[v] = dyn;
     r->chip_oi[v] = oi;
     r->chip_oj[v] = oj;
+    r->cap = (size_t)cap;
     r->chip_y0 = r->chip_y1 = nullptr;
   }
   const bool same = (r->chip_y0 == m->y && r->chip_y1 == w->ytemp) || (r->chip_y0 == w->ytemp && r->chip_y1 == m->y);
@@ -667,9 +673,11 @@ static int tb_prepare_single(hsb_dev_model *m, FastWork *w) {
     memset(C, 0, sizeof(C));
     for (int q = 0; q < 2; q++) {
       if (!r->chip_oi[q]) continue;
-      if ((rc = tb_fill_chip(m, r, m->y, w->ytemp, w->pf, w->t1, r->chip_oi[q], r->chip_oj[q], &C[2 * q])))
+      if ((rc = tb_fill_chip(m, r, m->y, w->ytemp, w->pf, w->t1, r->chip_oi[q], r->chip_oj[q], q == 1, r->cap,
+                             &C[2 * q])))
         return rc;
-      if ((rc = tb_fill_chip(m, r, w->ytemp, m->y, w->pf, w->t1, r->chip_oi[q], r->chip_oj[q], &C[2 * q + 1])))
+      if ((rc = tb_fill_chip(m, r, w->ytemp, m->y, w->pf, w->t1, r->chip_oi[q], r->chip_oj[q], q == 1, r->cap,
+                             &C[2 * q + 1])))
         return rc;
     }
     HSB_CUDA(cudaMemcpy(r->d_chip, C, sizeof(C), cudaMemcpyHostToDevice));

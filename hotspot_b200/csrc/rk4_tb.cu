@@ -59,7 +59,12 @@
 
 namespace hsb {
 
-static_assert(TB_SLOTS == 2, "slot 1 holds the error sums when increment and error terms overlap");
+// own cells per thread (accumulator slots): two for the FP32 kernel on up to
+// six layers, else one, so that the FP64 sums of every layer stay in registers
+template <typename V, int NL>
+__host__ __device__ constexpr int tb_slots() {
+  return (sizeof(V) == 4 && NL <= 6) ? 2 : 1;
+}
 
 __device__ Coef g_tb_first[3];
 __device__ int g_tb_first_ready;
@@ -245,21 +250,24 @@ __device__ void tb_subtile(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, const d
   const int sides = tb_sides(C, i0, j0, SI, SJ);
   const double amb = C.ambient;
   const bool sep = sh.sep != 0;
+  constexpr int S = tb_slots<V, NL>();
   // own cells of this thread: slot s -> own index tid + s * TB_THREADS
-  int q[TB_SLOTS];
-  long long g[TB_SLOTS];
-  bool ok[TB_SLOTS];
+  int q[S];
+  long long g[S];
+  bool ok[S];
 #pragma unroll
-  for (int s = 0; s < TB_SLOTS; s++) {
+  for (int s = 0; s < S; s++) {
     const int idx = tid + s * TB_THREADS;
     const int oi = idx / SJ, oj = idx - (idx / SJ) * SJ;
-    ok[s] = out && (sep || s == 0) && idx < SI * SJ && i0 + oi < nr && j0 + oj < nc;
+    ok[s] = out && idx < SI * SJ && i0 + oi < nr && j0 + oj < nc;
     q[s] = (oi + H) * RJ + (oj + H);
     g[s] = (long long)(i0 + oi) * nc + (j0 + oj);
   }
-  double acc[TB_SLOTS][NL];
+  // per own cell and layer: the increment sum, then the error sum (sep); or
+  // the error sum only, the increment going straight to the candidate state
+  double acc[S][NL];
 #pragma unroll
-  for (int s = 0; s < TB_SLOTS; s++)
+  for (int s = 0; s < S; s++)
 #pragma unroll
     for (int n = 0; n < NL; n++) acc[s][n] = 0.0;
 
@@ -293,14 +301,14 @@ __device__ void tb_subtile(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, const d
         const double cf = m <= dD ? cd : ce;
         if (cf != 0.0) {
 #pragma unroll
-          for (int s = 0; s < TB_SLOTS; s++)
+          for (int s = 0; s < S; s++)
             if (ok[s])
 #pragma unroll
               for (int n = 0; n < NL; n++) acc[s][n] += cf * (double)dst[n * LP + q[s]];
         }
         if (m == dD) {   // the increment is complete: the candidate state, then the error sums
 #pragma unroll
-          for (int s = 0; s < TB_SLOTS; s++)
+          for (int s = 0; s < S; s++)
             if (ok[s])
 #pragma unroll
               for (int n = 0; n < NL; n++) {
@@ -309,13 +317,19 @@ __device__ void tb_subtile(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, const d
                 acc[s][n] = 0.0;
               }
         }
-      } else if (ok[0]) {   // overlapping increment and error terms: slot 0 only, both sums
+      } else {   // overlapping increment and error terms (a retry): the increment in the candidate state
 #pragma unroll
-        for (int n = 0; n < NL; n++) {
-          const double v = (double)dst[n * LP + q[0]];
-          acc[0][n] += cd * v;
-          acc[1][n] += ce * v;
-        }
+        for (int s = 0; s < S; s++)
+          if (ok[s])
+#pragma unroll
+            for (int n = 0; n < NL; n++) {
+              const double v = (double)dst[n * LP + q[s]];
+              if (m <= dD) {
+                const long long cc = (long long)n * C.plane + g[s];
+                yn[cc] = (m == 0 ? __ldcg(yb + cc) : yn[cc]) + cd * v;
+              }
+              acc[s][n] += ce * v;
+            }
       }
     }
     if (sums && m < dE) tb_edge_sums<V>(C, sh, dst, yb, m + 1, RI, RJ, H, i0, j0, SI, SJ, sides);
@@ -325,20 +339,11 @@ __device__ void tb_subtile(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, const d
     __syncthreads();
   }
   if (out) {
-    if (sep) {
 #pragma unroll
-      for (int s = 0; s < TB_SLOTS; s++)
-        if (ok[s])
+    for (int s = 0; s < S; s++)
+      if (ok[s])
 #pragma unroll
-          for (int n = 0; n < NL; n++) errl = fmax(errl, fabs(acc[s][n]));
-    } else if (ok[0]) {
-#pragma unroll
-      for (int n = 0; n < NL; n++) {
-        const long long cc = (long long)n * C.plane + g[0];
-        yn[cc] = __ldcg(yb + cc) + acc[0][n];
-        errl = fmax(errl, fabs(acc[1][n]));
-      }
-    }
+        for (int n = 0; n < NL; n++) errl = fmax(errl, fabs(acc[s][n]));
   }
 }
 
@@ -429,7 +434,7 @@ __device__ int tb_plan(const TChip &C, TSh<V> &sh, double h, bool first) {
   if (dE > TB_DMAX) return 3;
   // sub-tile: the own tile, halved until its box fits the buffers and its
   // own cells fit the threads' accumulator slots
-  const int H = dE + 1, slots = sep ? TB_SLOTS : 1;
+  const int H = dE + 1, slots = tb_slots_rt(sizeof(V) == 8, C.nl);
   for (int SJ = C.oj; SJ >= 8; SJ >>= 1)
     for (int SI = C.oi; SI >= 1; SI >>= 1)
       if ((SI + 2 * H) * (SJ + 2 * H) <= C.rcap && SI * SJ <= TB_THREADS * slots) {
@@ -877,6 +882,18 @@ double tb_tile_work(int oi, int oj) {
   return w;
 }
 
+// region cells per layer of one buffer for an own tile: the first attempt's
+// box (halo 8), and -- where it fits -- at least a 48 x 48 box, so that a
+// retry's larger halo (12, 16, 20 after one, two, three rejections) still
+// finds a sub-tile of 24 x 24, 16 x 16 or 8 x 8 cells
+int tb_rcap(int nl, int oi, int oj, bool fp64, size_t smem_cap) {
+  const int base = (oi + 16) * (oj + 16);
+  const long long fit =
+      ((long long)smem_cap - (long long)tb_static_smem(fp64)) / (2LL * nl * (fp64 ? 8 : 4));
+  const long long want = base > 2304 ? base : 2304;
+  return (int)(want < fit ? want : (fit > base ? fit : base));
+}
+
 // own-tile shape for a model with `ctas` co-resident CTAs: among the
 // candidates whose two region buffers fit next to the static shared memory,
 // the one with the least work for the busiest CTA (tiles dealt round-robin)
@@ -885,8 +902,9 @@ int tb_tile_for(int nl, int nr, int nc, int ctas, size_t smem_cap, int *oi, int 
   int best = -1;
   double best_cost = 0.0;
   for (int k = 0; k < 6; k++) {
-    const size_t rc = (size_t)(cand[k][0] + 16) * (cand[k][1] + 16);
+    const size_t rc = (size_t)tb_rcap(nl, cand[k][0], cand[k][1], fp64, smem_cap);
     if (2 * rc * nl * (fp64 ? 8 : 4) + tb_static_smem(fp64) > smem_cap) continue;
+    if (cand[k][0] * cand[k][1] > TB_THREADS * tb_slots_rt(fp64, nl)) continue;
     const long long tiles = (long long)((nr + cand[k][0] - 1) / cand[k][0]) * ((nc + cand[k][1] - 1) / cand[k][1]);
     const double cost = (double)((tiles + ctas - 1) / ctas) * tb_tile_work(cand[k][0], cand[k][1]);
     if (best < 0 || cost < best_cost) {
@@ -900,12 +918,12 @@ int tb_tile_for(int nl, int nr, int nc, int ctas, size_t smem_cap, int *oi, int 
   return HSB_OK;
 }
 
-size_t tb_dyn_smem(int nl, int oi, int oj, bool fp64) {
-  return (size_t)2 * (oi + 16) * (oj + 16) * nl * (fp64 ? 8 : 4);
+size_t tb_dyn_smem(int nl, int oi, int oj, bool fp64, size_t smem_cap) {
+  return (size_t)2 * tb_rcap(nl, oi, oj, fp64, smem_cap) * nl * (fp64 ? 8 : 4);
 }
 
 int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1, float *pf, double *pd, int oi,
-                 int oj, TChip *C) {
+                 int oj, bool fp64, size_t smem_cap, TChip *C) {
   memset(C, 0, sizeof(*C));
   C->y[0] = const_cast<double *>(y0);
   C->y[1] = const_cast<double *>(y1);
@@ -943,7 +961,7 @@ int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1,
   C->ntj = (m->nc + oj - 1) / oj;
   C->ntiles = C->nti * C->ntj;
   C->segmax = r->segmax;
-  C->rcap = (oi + 16) * (oj + 16);
+  C->rcap = tb_rcap(m->nl, oi, oj, fp64, smem_cap);
   if (C->nti > r->segmax || C->ntj > r->segmax) return set_error(HSB_E_ARG, "tile grid exceeds the edge partials");
   return HSB_OK;
 }

@@ -8,13 +8,17 @@ namespace hsb {
 
 #define TB_THREADS 512
 #define TB_WARPS (TB_THREADS / 32)
-#define TB_SLOTS 2            // own cells per thread: a sub-tile holds at most TB_THREADS * TB_SLOTS
 #define TB_NLMIN 3
 #define TB_NLMAX 12
 #define TB_DMAX 19            // highest Krylov degree in the kernel (first attempt 7, +4 per rejection)
 #define TB_JMAX (TB_DMAX - 1) // edge-response table depth: L_cc^j, j < TB_JMAX
 #define TB_OUT 8              // per-chip result words (layout of FastWork::cnt)
 #define TB_BAR_LIMIT (1 << 25)
+
+// own cells per thread (the kernel's FP64 accumulator slots): two for the
+// FP32 kernel on up to six layers, else one; a tile or sub-tile holds at most
+// TB_THREADS x that many own cells
+__host__ __device__ inline int tb_slots_rt(bool fp64, int nl) { return (!fp64 && nl <= 6) ? 2 : 1; }
 
 // FP32 layer coefficients as the kernel reads them: two float4 loads
 struct alignas(16) TLayer {
@@ -69,6 +73,7 @@ struct TbRes {
   int chip_oi[2], chip_oj[2];       // per variant: own tile (0: not chosen yet)
   int version, ne, segmax;
   int eg_layer[5], eg_node[5];
+  size_t cap;                       // the device's shared memory per CTA (opt-in)
   int grid[2];                      // per variant: co-resident CTAs of a single-model launch
   size_t dyn[2];                    // per variant: dynamic shared memory of that launch
 };
@@ -77,12 +82,13 @@ struct TbRes {
 bool tb_eligible(const hsb_dev_model *m);
 const void *tb_kernel(bool fp64 = false);
 size_t tb_static_smem(bool fp64 = false);
-size_t tb_dyn_smem(int nl, int oi, int oj, bool fp64 = false);
+int tb_rcap(int nl, int oi, int oj, bool fp64, size_t smem_cap);
+size_t tb_dyn_smem(int nl, int oi, int oj, bool fp64, size_t smem_cap);
 int tb_tile_for(int nl, int nr, int nc, int ctas, size_t smem_cap, int *oi, int *oj, bool fp64 = false);
 double tb_tile_work(int oi, int oj);
 int tb_res_prepare(hsb_dev_model *m, TbRes **r, const PackF *pk_dev);
 void tb_res_free(TbRes *r);
 int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1, float *pf, double *pd, int oi,
-                 int oj, TChip *C);
+                 int oj, bool fp64, size_t smem_cap, TChip *C);
 
 }  // namespace hsb

@@ -202,6 +202,11 @@ class RCModel:
                    steady_tol: float = 0.0, max_iters: int = 0):
         check(lib().hsb_grid_set_solver(self.ptr, form, steady_method, steady_tol, max_iters))
 
+    def set_tile(self, rows: int, cols: int):
+        """Own-tile shape of the temporally blocked transient kernel (0, 0: automatic)."""
+        if lib().hsb_dev_set_tile(lib().hsb_grid_device(self.ptr), int(rows), int(cols)) != 0:
+            raise _abi.HotspotError(lib().hsb_dev_last_error().decode(errors="replace").strip())
+
     def stats(self) -> dict:
         s = _abi.Stats()
         check(lib().hsb_grid_get_stats(self.ptr, C.byref(s)))

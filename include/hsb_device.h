@@ -257,6 +257,14 @@ int  hsb_server_set_priority(hsb_server *s, int model, int high);
  * with no work of the model in flight */
 int hsb_dev_set_priority(hsb_dev_model *m, int high);
 
+/* own-tile shape (rows x columns) of the temporally blocked transient kernel
+ * for this model (no counterpart in the reference): 0, 0 lets the library
+ * choose by its cost model; otherwise rows x columns must be at most 1024
+ * own cells (512 for more than six layers) and fit shared memory.  The
+ * arithmetic of a cell does not depend on the tile; only the order of the
+ * FP64 sums over grid edges does. */
+int hsb_dev_set_tile(hsb_dev_model *m, int rows, int cols);
+
 /* which of the model's solver workspaces exist (no counterpart in the
  * reference): the fast transient, MG-PCG and BiCGStab solvers allocate
  * theirs on their first call; *mask = OR of HSB_WS_* */

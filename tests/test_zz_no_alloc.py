@@ -9,8 +9,8 @@ device memory, twice in a row, and checks each result
   * against the regular entry point (compute_temp with the stage-by-stage
     fast form, the arithmetic the allocation-free entry point runs), within
     the parity tolerance used by the GPU tests, and
-  * against the FP64 oracle (the reference's arithmetic), within the fast
-    form's 0.01 K bar,
+  * against the reference's own FP64 code (the live build; else the
+    oracle's restatement), within the fast form's 0.01 K bar,
 on models that exercise the static scratch's sizing: a 2-D chip, the
 secondary heat path (28 package nodes), a 6-layer stack, and a rectangular
 grid of exactly HSB_NOALLOC_MAX_CELLS cells.  It also checks the defining
@@ -27,6 +27,7 @@ import pytest
 from hotspot_b200 import FORM_FAST_STAGES, _abi
 from hotspot_b200 import model as hm
 from hotspot_b200 import workloads as W
+from oracle import ref as R
 from oracle.restatement import OracleModel
 
 pytestmark = pytest.mark.gpu
@@ -71,9 +72,13 @@ def test_noalloc_matches_regular_entry(workdir, case):
         a.compute_temp(a.power_vector(sc.block_power[k]).copy(), None, sc.dt)
         expected.append(a.grid("trans"))
 
-    # the oracle's FP64 replay of the reference from the same state
-    o = OracleModel(sc)
-    to = o.vector(o.init_temp)
+    # the reference's own FP64 code from the same state (the live build;
+    # else the oracle's restatement, which covers the primary heat path)
+    live = R.available()
+    if not live and case == "secondary":
+        pytest.skip("the secondary heat path needs the live reference build")
+    o = R.RefModel(sc) if live else OracleModel(sc)
+    to = o.vector(333.15)
     o.compute_temp(o.power_vector(sc.block_power[0]), to, 0.0)
     assert np.max(np.abs(o.grid("trans") - y0)) <= TOL
     exact = []
@@ -87,8 +92,9 @@ def test_noalloc_matches_regular_entry(workdir, case):
     dev = L.hsb_grid_device(b.ptr)
     y = torch.tensor(y0, dtype=torch.float64, device="cuda")
     for k, exp, ex64 in zip((1, 2), expected, exact):
-        pg = torch.tensor(o.b2g(b.power_vector(sc.block_power[k]).copy(), True), dtype=torch.float64,
-                          device="cuda")
+        p = b.power_vector(sc.block_power[k])
+        pgrid = o.power_grid(p.copy()) if live else o.b2g(p.copy(), True)
+        pg = torch.tensor(pgrid, dtype=torch.float64, device="cuda")
         torch.cuda.synchronize()        # y and pg are complete before the call reads them
         st = _abi.Stats()
         rc = L.hsb_dev_transient_noalloc(dev, C.c_void_p(y.data_ptr()), C.c_void_p(pg.data_ptr()),
@@ -103,6 +109,8 @@ def test_noalloc_matches_regular_entry(workdir, case):
     assert mask.value & 1 == 0, "the allocation-free entry point allocated a fast-transient workspace"
     a.close()
     b.close()
+    if live:
+        o.close()
 
 
 def test_noalloc_rejects_oversized_models(workdir):
