@@ -36,7 +36,10 @@ int raise_smem_limit(const void *fn, size_t bytes) {
   size_t &have = cur[{dev, fn}];
   if (bytes <= have) return HSB_OK;
   const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e != cudaSuccess) return cuda_check(e, "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
+  if (e != cudaSuccess) {
+    cudaGetLastError();   // a refused attribute must not surface again in a later check
+    return cuda_check(e, "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
+  }
   have = bytes;
   return HSB_OK;
 }

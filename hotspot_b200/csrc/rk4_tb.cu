@@ -351,7 +351,7 @@ __device__ void tb_subtile(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, const d
 // of A_0 .. A_{dE-1} (sh.SA) and the edge-response table (one warp; lanes
 // are edges, then nodes)
 template <typename V>
-__device__ __forceinline__ void tb_package(const TChip &C, TSh<V> &sh, double h) {
+__device__ __noinline__ void tb_package(const TChip &C, TSh<V> &sh, double h) {
   const int lane = threadIdx.x & 31;
   const int nx = C.nx, ne = C.ne, dE = sh.dE;
   const PackF &P = *C.pk;
@@ -402,7 +402,7 @@ __device__ __forceinline__ void tb_package(const TChip &C, TSh<V> &sh, double h)
 // the attempt's coefficients (thread 0); returns 0, or 3 when the degree is
 // beyond what a sub-tile of this chip can hold
 template <typename V>
-__device__ int tb_plan(const TChip &C, TSh<V> &sh, double h, bool first) {
+__device__ __noinline__ int tb_plan(const TChip &C, TSh<V> &sh, double h, bool first) {
   if (first) {
     for (int q = 0; q < PMAX; q++) sh.ps[q] = h;
     sh.E.n = sh.E1.n;
@@ -797,7 +797,23 @@ bool tb_eligible(const hsb_dev_model *m) {
   return true;
 }
 
-size_t tb_static_smem(bool fp64) { return fp64 ? sizeof(TSh<double>) : sizeof(TSh<float>); }
+// static shared memory of the kernel variant as compiled (the shared state
+// plus the shared arrays of its device functions)
+size_t tb_static_smem(bool fp64) {
+  static size_t have[2] = {0, 0};
+  static std::once_flag once[2];
+  const int v = fp64 ? 1 : 0;
+  std::call_once(once[v], [v] {
+    cudaFuncAttributes a;
+    const void *fn = v ? (const void *)rk4_tb_kernel<double> : (const void *)rk4_tb_kernel<float>;
+    if (cudaFuncGetAttributes(&a, fn) == cudaSuccess) have[v] = a.sharedSizeBytes;
+    else {
+      cudaGetLastError();
+      have[v] = v ? sizeof(TSh<double>) + 1024 : sizeof(TSh<float>) + 1024;
+    }
+  });
+  return have[v];
+}
 
 const void *tb_kernel(bool fp64) {
   return fp64 ? (const void *)rk4_tb_kernel<double> : (const void *)rk4_tb_kernel<float>;
@@ -882,16 +898,15 @@ double tb_tile_work(int oi, int oj) {
   return w;
 }
 
-// region cells per layer of one buffer for an own tile: the first attempt's
-// box (halo 8), and -- where it fits -- at least a 48 x 48 box, so that a
-// retry's larger halo (12, 16, 20 after one, two, three rejections) still
-// finds a sub-tile of 24 x 24, 16 x 16 or 8 x 8 cells
+// region cells per layer of one buffer for an own tile: every cell the
+// shared memory of a CTA holds (at least the first attempt's box, halo 8),
+// so that a retry's larger halo (12, 16, ... after one, two, ... rejections)
+// still finds a sub-tile
 int tb_rcap(int nl, int oi, int oj, bool fp64, size_t smem_cap) {
   const int base = (oi + 16) * (oj + 16);
   const long long fit =
       ((long long)smem_cap - (long long)tb_static_smem(fp64)) / (2LL * nl * (fp64 ? 8 : 4));
-  const long long want = base > 2304 ? base : 2304;
-  return (int)(want < fit ? want : (fit > base ? fit : base));
+  return (int)(fit > base ? fit : base);
 }
 
 // own-tile shape for a model with `ctas` co-resident CTAs: among the

@@ -10,7 +10,7 @@ namespace hsb {
 #define TB_WARPS (TB_THREADS / 32)
 #define TB_NLMIN 3
 #define TB_NLMAX 12
-#define TB_DMAX 19            // highest Krylov degree in the kernel (first attempt 7, +4 per rejection)
+#define TB_DMAX 27            // highest Krylov degree in the kernel (first attempt 7, +4 per rejection)
 #define TB_JMAX (TB_DMAX - 1) // edge-response table depth: L_cc^j, j < TB_JMAX
 #define TB_OUT 8              // per-chip result words (layout of FastWork::cnt)
 #define TB_BAR_LIMIT (1 << 25)

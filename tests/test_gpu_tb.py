@@ -141,6 +141,7 @@ def test_fp64_blocked_matches_replay(workdir, case):
     rows = min(sc.steps, sc.block_power.shape[0])
     ta, ga, sa, aa, fa = _run(sc, FORM_FP64_BLOCKED, rows)
     tb, gb, sb, ab, fb = _run(sc, FORM_PARITY, rows)
+    assert fa == 0, "a retry outgrew the kernel"
     assert sa == sb and aa == ab, (sa, aa, sb, ab)
     assert np.max(np.abs(ta - tb)) <= TOL_REPLAY
     assert np.max(np.abs(ga - gb)) <= TOL_REPLAY
