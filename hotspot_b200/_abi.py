@@ -240,6 +240,10 @@ _SIGS = {
     "hsb_batch_transient": (C.c_int, [C.c_void_p, _D, C.c_double, C.POINTER(Stats)]),
     "hsb_batch_transient_trace": (C.c_int, [C.c_void_p, _D, C.c_int, C.c_double, C.POINTER(Stats)]),
     "hsb_batch_chip_tile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "hsb_batch_set_ctas": (C.c_int, [C.c_void_p, C.c_int]),
+    "hsb_batch_run_subset": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_int, _D, C.c_int, C.c_double,
+                                       C.POINTER(Stats)]),
+    "hsb_batch_offsets": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     "hsb_batch_set_schedule": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     "hsb_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong),
                                  C.POINTER(C.c_int), C.POINTER(C.c_double)]),

@@ -77,6 +77,12 @@ struct hsb_batch {
   int grid = 0;
   size_t dyn = 0, cap = 0;
   int nsm = 0;
+  int cta_cap = 0;      // at most this many CTAs per launch (0: every co-resident CTA)
+  // work lists of launches over a subset of the chips (hsb_batch_run_subset)
+  int4 *d_swork = nullptr;
+  int *d_swptr = nullptr, *h_swptr = nullptr;
+  int4 *h_swork = nullptr;
+  int scap = 0;         // entries the subset list buffers hold
   cudaStream_t stream = nullptr;
   // schedule
   double split = 1.0;   // a chip gets about split * (its share of the work) CTAs
@@ -109,10 +115,12 @@ struct hsb_batch {
 
 static void batch_free(hsb_batch *b) {
   if (!b) return;
-  void *d[] = {b->d_chips, b->d_work, b->d_wptr, b->d_out, b->d_bar, b->d_bpow};
+  void *d[] = {b->d_chips, b->d_work, b->d_wptr, b->d_out, b->d_bar, b->d_bpow, b->d_swork, b->d_swptr};
   for (void *p : d)
     if (p) cudaFree(p);
   if (b->h_out) cudaFreeHost(b->h_out);
+  if (b->h_swork) cudaFreeHost(b->h_swork);
+  if (b->h_swptr) cudaFreeHost(b->h_swptr);
   if (b->h_bpow) cudaFreeHost(b->h_bpow);
   for (auto &g : b->graph)
     if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -145,40 +153,38 @@ static int batch_tiles(hsb_batch *b) {
   return raise_smem_limit(tb_kernel(), b->dyn);
 }
 
-// CTA work lists for the current schedule
-static int batch_schedule(hsb_batch *b) {
-  int rc;
-  if ((rc = batch_tiles(b))) return rc;
-  int per_sm = 0;
-  HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tb_kernel(), TB_THREADS, b->dyn));
-  if (per_sm < 1) return set_error(HSB_E_ARG, "batch kernel does not fit an SM");
-  const int G = per_sm * b->nsm;
+// CTA work lists of the chips in `chips` over G CTAs: a chip worth more than
+// a CTA's fair share gets a group of CTAs (chip-local barriers), the rest are
+// packed onto single CTAs, longest first onto the least loaded
+static void batch_lists(const hsb_batch *b, const std::vector<int> &chips, int G, std::vector<int4> &work,
+                        std::vector<int> &wptr) {
+  const int n = (int)chips.size();
   // work of a chip: its tiles x the work of a tile x layers
-  std::vector<double> wk(b->n);
+  std::vector<double> wk(n);
   double W = 0;
-  for (int c = 0; c < b->n; c++) {
-    const TChip &C = b->h_chips[c];
-    wk[c] = (double)C.ntiles * tb_tile_work(C.oi, C.oj) * C.nl;
-    W += wk[c];
+  for (int k = 0; k < n; k++) {
+    const TChip &C = b->h_chips[chips[k]];
+    wk[k] = (double)C.ntiles * tb_tile_work(C.oi, C.oj) * C.nl;
+    W += wk[k];
   }
-  std::vector<int> order(b->n);
-  for (int c = 0; c < b->n; c++) order[c] = c;
+  std::vector<int> order(n);
+  for (int k = 0; k < n; k++) order[k] = k;
   std::sort(order.begin(), order.end(), [&](int a, int c) { return wk[a] > wk[c]; });
   const double share = W / G;
-  std::vector<int> g(b->n, 1);
+  std::vector<int> g(n, 1);
   double w_small = 0.0, sum_g = 0.0;
-  for (int c = 0; c < b->n; c++) {
+  for (int k = 0; k < n; k++) {
     // a chip worth more than one fair share gets enough CTAs that none of
     // them carries more than a share (rounded up), at most one per tile
-    const double ratio = wk[c] / share * b->split;
+    const double ratio = wk[k] / share * b->split;
     int q = ratio > 1.0 ? (int)ceil(ratio) : 1;
-    if (q > b->h_chips[c].ntiles) q = b->h_chips[c].ntiles;
+    if (q > b->h_chips[chips[k]].ntiles) q = b->h_chips[chips[k]].ntiles;
     if (q >= 2) {
-      g[c] = q;
+      g[k] = q;
       sum_g += q;
     } else {
-      g[c] = 1;
-      w_small += wk[c];
+      g[k] = 1;
+      w_small += wk[k];
     }
   }
   int g_small = (int)ceil(w_small / share);
@@ -187,23 +193,23 @@ static int batch_schedule(hsb_batch *b) {
   const double avail = G - g_small;
   if (sum_g > avail) {   // scale the groups down to the CTAs left
     const double f = avail / sum_g;
-    for (int c = 0; c < b->n; c++)
-      if (g[c] >= 2) {
-        int q = (int)(g[c] * f);
+    for (int k = 0; k < n; k++)
+      if (g[k] >= 2) {
+        int q = (int)(g[k] * f);
         if (q < 2) {
           q = 1;
-          w_small += wk[c];
+          w_small += wk[k];
         }
-        g[c] = q;
+        g[k] = q;
       }
   }
   std::vector<std::vector<int4>> lists;
   std::vector<double> load;
-  for (int c : order)
-    if (g[c] >= 2)
-      for (int r = 0; r < g[c]; r++) {
-        lists.push_back({make_int4(c, r, g[c], 0)});
-        load.push_back(wk[c] / g[c]);
+  for (int k : order)
+    if (g[k] >= 2)
+      for (int r = 0; r < g[k]; r++) {
+        lists.push_back({make_int4(chips[k], r, g[k], 0)});
+        load.push_back(wk[k] / g[k]);
       }
   const int base = (int)lists.size();
   const int remaining = G - base > 0 ? G - base : 1;
@@ -211,26 +217,43 @@ static int batch_schedule(hsb_batch *b) {
     lists.push_back({});
     load.push_back(0.0);
   }
-  for (int c : order) {   // the rest, longest first onto the least loaded CTA
-    if (g[c] >= 2) continue;
+  for (int k : order) {
+    if (g[k] >= 2) continue;
     int best = base;
-    for (int k = base; k < (int)lists.size(); k++)
-      if (load[k] < load[best]) best = k;
-    lists[best].push_back(make_int4(c, 0, 1, 0));
-    load[best] += wk[c];
+    for (int q = base; q < (int)lists.size(); q++)
+      if (load[q] < load[best]) best = q;
+    lists[best].push_back(make_int4(chips[k], 0, 1, 0));
+    load[best] += wk[k];
   }
-  {
-    std::vector<std::vector<int4>> keep;
-    for (auto &l : lists)
-      if (!l.empty()) keep.push_back(l);
-    lists.swap(keep);
+  work.clear();
+  wptr.assign(1, 0);
+  for (auto &l : lists) {
+    if (l.empty()) continue;
+    for (auto &a : l) work.push_back(a);
+    wptr.push_back((int)work.size());
   }
-  std::vector<int> wptr(lists.size() + 1, 0);
+}
+
+// co-resident CTAs of a launch (at most the cap set by hsb_batch_set_ctas)
+static int batch_ctas(hsb_batch *b, int *G) {
+  int per_sm = 0;
+  HSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tb_kernel(), TB_THREADS, b->dyn));
+  if (per_sm < 1) return set_error(HSB_E_ARG, "batch kernel does not fit an SM");
+  *G = per_sm * b->nsm;
+  if (b->cta_cap > 0 && *G > b->cta_cap) *G = b->cta_cap;
+  return HSB_OK;
+}
+
+// CTA work lists for the current schedule (every chip)
+static int batch_schedule(hsb_batch *b) {
+  int rc, G;
+  if ((rc = batch_tiles(b))) return rc;
+  if ((rc = batch_ctas(b, &G))) return rc;
+  std::vector<int> all(b->n);
+  for (int c = 0; c < b->n; c++) all[c] = c;
   std::vector<int4> work;
-  for (size_t k = 0; k < lists.size(); k++) {
-    for (auto &a : lists[k]) work.push_back(a);
-    wptr[k + 1] = (int)work.size();
-  }
+  std::vector<int> wptr;
+  batch_lists(b, all, G, work, wptr);
   if (b->d_work) cudaFree(b->d_work);
   if (b->d_wptr) cudaFree(b->d_wptr);
   b->d_work = nullptr;
@@ -239,7 +262,7 @@ static int batch_schedule(hsb_batch *b) {
   HSB_CUDA(cudaMalloc(&b->d_wptr, sizeof(int) * wptr.size()));
   HSB_CUDA(cudaMemcpy(b->d_work, work.data(), sizeof(int4) * work.size(), cudaMemcpyHostToDevice));
   HSB_CUDA(cudaMemcpy(b->d_wptr, wptr.data(), sizeof(int) * wptr.size(), cudaMemcpyHostToDevice));
-  b->grid = (int)lists.size();
+  b->grid = (int)wptr.size() - 1;
   b->version++;
   return HSB_OK;
 }
@@ -559,6 +582,144 @@ int hsb_batch_transient_trace(hsb_batch *b, const double *block_powers, int K, d
 
 int hsb_batch_transient(hsb_batch *b, const double *block_power, double time_elapsed, hsb_stats *st) {
   return hsb_batch_transient_trace(b, block_power, 1, time_elapsed, st);
+}
+
+int hsb_batch_set_ctas(hsb_batch *b, int ctas) {
+  if (!b || ctas < 0) return set_error(HSB_E_ARG, "bad CTA cap");
+  b->cta_cap = ctas;
+  return batch_schedule(b);
+}
+
+int hsb_batch_run_subset(hsb_batch *b, const int *chips, int n, const double *block_powers, int K,
+                         double time_elapsed, hsb_stats *st) {
+  if (!b || !chips || n < 1 || !block_powers || K < 1) return set_error(HSB_E_ARG, "bad subset launch");
+  hsb_stats local;
+  if (!st) st = &local;
+  cudaSetDevice(b->device);
+  int rc, G;
+  for (int k = 0; k < n; k++)
+    if (chips[k] < 0 || chips[k] >= b->n) return set_error(HSB_E_ARG, "chip index out of range");
+  if ((rc = batch_bpow(b, K))) return rc;
+  if ((rc = batch_ctas(b, &G))) return rc;
+  std::vector<int> sub(chips, chips + n);
+  std::vector<int4> work;
+  std::vector<int> wptr;
+  batch_lists(b, sub, G, work, wptr);
+  const int need = (int)std::max(work.size(), wptr.size()) + 1;
+  if (need > b->scap) {
+    void *p[] = {b->d_swork, b->d_swptr};
+    for (void *q : p)
+      if (q) cudaFree(q);
+    if (b->h_swork) cudaFreeHost(b->h_swork);
+    if (b->h_swptr) cudaFreeHost(b->h_swptr);
+    b->d_swork = nullptr;
+    b->d_swptr = nullptr;
+    b->h_swork = nullptr;
+    b->h_swptr = nullptr;
+    b->scap = 0;
+    const int cap = need * 2;
+    HSB_CUDA(cudaMalloc(&b->d_swork, sizeof(int4) * cap));
+    HSB_CUDA(cudaMalloc(&b->d_swptr, sizeof(int) * cap));
+    HSB_CUDA(cudaMallocHost(&b->h_swork, sizeof(int4) * cap));
+    HSB_CUDA(cudaMallocHost(&b->h_swptr, sizeof(int) * cap));
+    b->scap = cap;
+  }
+  memcpy(b->h_swork, work.data(), sizeof(int4) * work.size());
+  memcpy(b->h_swptr, wptr.data(), sizeof(int) * wptr.size());
+  // the listed chips' block powers of every interval, and their state buffers
+  for (int k = 0; k < K; k++)
+    for (int c : sub) {
+      const long long o = (long long)k * b->nbtotal + b->boff[c];
+      memcpy(b->h_bpow + o, block_powers + o, sizeof(double) * (b->boff[c + 1] - b->boff[c]));
+    }
+  for (int c : sub) {
+    hsb_dev_model *m = b->models[c];
+    const long long cur = m->y == b->h_chips[c].y[0] ? 0 : 1;
+    if (m->y != b->h_chips[c].y[cur] || ((FastWork *)m->fast)->ytemp != b->h_chips[c].y[cur ^ 1])
+      return set_error(HSB_E_ARG, "a batch model's state buffers were reallocated");
+    b->h_out[(size_t)c * TB_OUT + 6] = cur;
+  }
+  HSB_CUDA(cudaMemcpyAsync(b->d_out, b->h_out, sizeof(long long) * TB_OUT * b->n, cudaMemcpyHostToDevice,
+                           b->stream));
+  HSB_CUDA(cudaMemcpyAsync(b->d_bpow, b->h_bpow, sizeof(double) * b->nbtotal * K, cudaMemcpyHostToDevice,
+                           b->stream));
+  HSB_CUDA(cudaMemcpyAsync(b->d_swork, b->h_swork, sizeof(int4) * work.size(), cudaMemcpyHostToDevice,
+                           b->stream));
+  HSB_CUDA(cudaMemcpyAsync(b->d_swptr, b->h_swptr, sizeof(int) * wptr.size(), cudaMemcpyHostToDevice,
+                           b->stream));
+  HSB_CUDA(cudaMemsetAsync(b->d_bar, 0, sizeof(unsigned) * 2 * b->n, b->stream));
+  HSB_CUDA(cudaEventRecord(b->ev[1], b->stream));
+  const TChip *chips_d = b->d_chips;
+  const int4 *work_d = b->d_swork;
+  const int *wptr_d = b->d_swptr;
+  long long *out = b->d_out;
+  const double *bpow = b->d_bpow;
+  long long nbtot = b->nbtotal;
+  long long max_attempts = 10000000;
+  int Kk = K;
+  double T = time_elapsed;
+  void *args[] = {&chips_d, &work_d, &wptr_d, &out, &T, &Kk, &bpow, &nbtot, &max_attempts};
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3((unsigned)(wptr.size() - 1));
+  cfg.blockDim = dim3(TB_THREADS);
+  cfg.dynamicSmemBytes = b->dyn;
+  cfg.stream = b->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  HSB_CUDA(cudaLaunchKernelExC(&cfg, tb_kernel(), args));
+  HSB_CUDA(cudaEventRecord(b->ev[2], b->stream));
+  HSB_CUDA(cudaMemcpyAsync(b->h_out, b->d_out, sizeof(long long) * TB_OUT * b->n, cudaMemcpyDeviceToHost,
+                           b->stream));
+  HSB_CUDA(cudaStreamSynchronize(b->stream));
+  float kms = 0.f;
+  cudaEventElapsedTime(&kms, b->ev[1], b->ev[2]);
+  st->launches += 1;
+  st->kernel_ms += kms;
+  for (int c : sub) {
+    hsb_dev_model *m = b->models[c];
+    FastWork *w = (FastWork *)m->fast;
+    const long long *o = b->h_out + (size_t)c * TB_OUT;
+    st->rk4_steps += o[0];
+    st->rk4_attempts += o[1];
+    const int cur = (int)o[6];
+    m->y = b->h_chips[c].y[cur];
+    w->ytemp = b->h_chips[c].y[cur ^ 1];
+    if (o[2] == 2) return set_error(HSB_E_CUDA, "batched transient: a chip barrier did not complete in time");
+    if (o[2] == 1) return set_error(HSB_E_NOCONV, "batched transient: RK4 attempt cap reached");
+    if (o[2] == 3) {   // the retries of a step outgrew the kernel: as in hsb_batch_transient_trace
+      double tt[2];
+      memcpy(tt, &o[4], sizeof(tt));
+      const int iv = (int)o[7];
+      st->fallbacks += 1;
+      for (int k = iv; k < K; k++) {
+        if ((rc = b2g(m, b->d_bpow + (long long)k * b->nbtotal + b->boff[c], m->pgrid, HSB_V_POWER))) return rc;
+        if (k == iv) {
+          if ((rc = rk4_stage_run(m, w, time_elapsed - tt[0], tt[1], st))) return rc;
+        } else {
+          void *wk = nullptr;
+          int fell = 0;
+          if ((rc = rk4_fast_interval_begin(m, time_elapsed, st, &wk, nullptr))) return rc;
+          if ((rc = cuda_check(cudaStreamSynchronize(m->stream), "fallback interval"))) return rc;
+          if ((rc = rk4_fast_interval_end(m, wk, time_elapsed, st, &fell))) return rc;
+        }
+      }
+      if ((rc = cuda_check(cudaStreamSynchronize(m->stream), "fallback intervals"))) return rc;
+    }
+  }
+  st->sim_time += time_elapsed * K;
+  return HSB_OK;
+}
+
+// boundaries of the chips' block-power vectors: chip c's row segment is
+// [off[c], off[c + 1]) of a row of hsb_batch_transient_trace's layout
+int hsb_batch_offsets(hsb_batch *b, long long *off) {
+  if (!b || !off) return set_error(HSB_E_ARG, "null argument");
+  for (int c = 0; c <= b->n; c++) off[c] = b->boff[c];
+  return HSB_OK;
 }
 
 // the autotuner's measurements: up to n candidates as (tile policy, split,

@@ -198,6 +198,16 @@ int  hsb_batch_set_schedule(hsb_batch *b, int policy, double split);
 int  hsb_batch_info(hsb_batch *b, int *grid, long long *cells, int *policy, double *split);
 /* accepted RK4 steps of each model in the last call (n entries) */
 int  hsb_batch_chip_steps(hsb_batch *b, long long *steps);
+/* at most `ctas` CTAs per launch (0: every co-resident CTA), so that other
+ * work keeps SMs while a batch runs */
+int  hsb_batch_set_ctas(hsb_batch *b, int ctas);
+/* one launch advancing only the listed models (n indices) by K intervals;
+ * block_powers has hsb_batch_transient_trace's layout, only the listed
+ * models' segments are read; blocks until done */
+int  hsb_batch_run_subset(hsb_batch *b, const int *chips, int n, const double *block_powers, int K,
+                          double time_elapsed, hsb_stats *st);
+/* where each model's block powers sit in a row: off[c] .. off[c + 1] (n + 1 entries) */
+int  hsb_batch_offsets(hsb_batch *b, long long *off);
 /* own-tile shape (rows x columns) of model c under the current schedule */
 int  hsb_batch_chip_tile(hsb_batch *b, int c, int *rows, int *cols);
 /* autotuner: when enabled, the next calls each run one candidate schedule

@@ -17,6 +17,7 @@ SuperLU (absent), is restated as the sparse system G T = P of
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import math
 import os
@@ -891,27 +892,49 @@ class _OrcModel(C.Structure):
 
 
 _olib = None
+LIB_X87 = os.path.join(HERE, "_build", "libgrid_oracle_x87.so")
 
 
 def olib():
     global _olib
     if _olib is None:
-        if not os.path.exists(LIB_PATH):
-            subprocess.run(["make", "-C", HERE, "restatement"], check=True, capture_output=True)
-        L = C.CDLL(LIB_PATH)
-        P = C.POINTER(_OrcModel)
-        D = C.POINTER(C.c_double)
-        L.orc_slope.argtypes = [P, D, D, D]
-        L.orc_rk4.argtypes = [P, D, D, D]
-        L.orc_rk4.restype = C.c_double
-        L.orc_compute_temp.argtypes = [P, D, D, C.c_double]
-        L.orc_compute_temp.restype = C.c_longlong
-        L.orc_steady.argtypes = [P, D, D, C.c_longlong]
-        L.orc_steady.restype = C.c_longlong
-        L.orc_gs_sweep.argtypes = [P, D, D]
-        L.orc_gs_sweep.restype = C.c_double
-        _olib = L
+        _olib = _load(LIB_PATH, "restatement")
     return _olib
+
+
+@contextlib.contextmanager
+def x87_rounding():
+    """Oracle calls made inside this block run the restatement compiled with
+    x87 80-bit intermediates: the same algorithm with different roundings.
+    The spread between the two builds is how far FP64 rounding alone moves a
+    result, the floor for comparing two FP64 evaluation orders on
+    ill-conditioned inputs (long intervals whose rejected attempts feed
+    k1 = f(t1) into the retry, RCutil.c:557-571)."""
+    global _olib
+    keep = _olib
+    _olib = _load(LIB_X87, "restatement-x87")
+    try:
+        yield
+    finally:
+        _olib = keep
+
+
+def _load(path, target):
+    if not os.path.exists(path):
+        subprocess.run(["make", "-C", HERE, target], check=True, capture_output=True)
+    L = C.CDLL(path)
+    P = C.POINTER(_OrcModel)
+    D = C.POINTER(C.c_double)
+    L.orc_slope.argtypes = [P, D, D, D]
+    L.orc_rk4.argtypes = [P, D, D, D]
+    L.orc_rk4.restype = C.c_double
+    L.orc_compute_temp.argtypes = [P, D, D, C.c_double]
+    L.orc_compute_temp.restype = C.c_longlong
+    L.orc_steady.argtypes = [P, D, D, C.c_longlong]
+    L.orc_steady.restype = C.c_longlong
+    L.orc_gs_sweep.argtypes = [P, D, D]
+    L.orc_gs_sweep.restype = C.c_double
+    return L
 
 
 def _d(a):

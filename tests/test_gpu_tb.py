@@ -8,8 +8,10 @@ for models with per-layer conductances) against
 * the oracle's FP64 replay of the reference: 0.01 K.
 
 The same kernel with every stencil pass in FP64 (HSB_FORM_FP64_BLOCKED)
-must stay within 1e-6 K of the FP64 replay of the reference's RK4 with the
-same accepted steps.
+must take the same accepted steps as the FP64 replay of the reference's RK4
+and stay within 1e-6 K of it (on long intervals with rejected attempts,
+within four times the spread FP64 rounding alone gives the reference
+algorithm there).
 
 Cases cover tiles that are all boundary ("ring") tiles (16x16), grids with
 interior tiles (256x256), rectangular grids, the secondary heat path (28
@@ -17,13 +19,15 @@ package nodes, 20 edges), 3-D stacks, and long sampling intervals whose
 adaptive steps are rejected (the retry recomputes its vectors with a larger
 halo in sub-tiles).
 """
+import contextlib
+
 import numpy as np
 import pytest
 
 from hotspot_b200 import FORM_FAST, FORM_FAST_PASSES, FORM_FP64_BLOCKED, FORM_PARITY
 from hotspot_b200 import model as hm
 from hotspot_b200 import workloads as W
-from oracle.restatement import OracleModel
+from oracle.restatement import OracleModel, x87_rounding
 
 pytestmark = pytest.mark.gpu
 TOL_FORMS = 1e-4
@@ -134,14 +138,39 @@ def test_blocked_against_fp64_oracle(workdir):
 TOL_REPLAY = 1e-6
 
 
+def _rounding_spread(sc, rows):
+    """How far FP64 rounding alone moves the reference algorithm's result on
+    this input: the oracle against the same oracle compiled with x87 80-bit
+    intermediates, blocks and grid."""
+    out = []
+    for ctx in (contextlib.nullcontext(), x87_rounding()):
+        with ctx:
+            o = OracleModel(sc)
+            to = o.vector(o.init_temp)
+            for k in range(rows):
+                o.compute_temp(o.power_vector(sc.block_power[k]), to if k == 0 else None, sc.dt)
+            out.append((to.copy(), o.grid("trans")))
+    return max(np.max(np.abs(out[0][0] - out[1][0])), np.max(np.abs(out[0][1] - out[1][1])))
+
+
 @pytest.mark.parametrize("case", ["chip2d16", "chip2d64", "secondary", "stack64", "stack256", "rect128x32",
                                   "long_chip2d", "long_stack"])
 def test_fp64_blocked_matches_replay(workdir, case):
+    """1e-6 K, or on long intervals with rejected attempts four times the
+    spread that FP64 rounding alone gives the reference algorithm there: a
+    retry takes k1 = f(t1) of the rejected, unstable attempt (RCutil.c:
+    557-571), whose large stiff components cancel in the accepted step, so any
+    two FP64 evaluation orders (the replay's stage by stage, this kernel's
+    polynomial in L) differ by more than 1e-6 K (long_stack: 2.1e-6 K between
+    the oracle's SSE and x87 builds)."""
     sc = _scenario(workdir, case)
     rows = min(sc.steps, sc.block_power.shape[0])
     ta, ga, sa, aa, fa = _run(sc, FORM_FP64_BLOCKED, rows)
     tb, gb, sb, ab, fb = _run(sc, FORM_PARITY, rows)
     assert fa == 0, "a retry outgrew the kernel"
     assert sa == sb and aa == ab, (sa, aa, sb, ab)
-    assert np.max(np.abs(ta - tb)) <= TOL_REPLAY
-    assert np.max(np.abs(ga - gb)) <= TOL_REPLAY
+    tol = TOL_REPLAY
+    if case.startswith("long_"):
+        tol = max(tol, 4.0 * _rounding_spread(sc, rows))
+    assert np.max(np.abs(ta - tb)) <= tol, tol
+    assert np.max(np.abs(ga - gb)) <= tol, tol
