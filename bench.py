@@ -64,6 +64,10 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="transient intervals of the fast form only (the case profiled with ncu)")
     ap.add_argument("--headline-only", action="store_true", help="skip the batched / microchannel / serving legs")
+    ap.add_argument("--legs", default="chip2d,batched,microchannel,serving",
+                    help="comma-separated legs to run after the headline")
+    ap.add_argument("--serving-batching", type=int, default=1,
+                    help="serve transients through the continuous batch engine (1) or the workers (0)")
     ap.add_argument("--profile-case", choices=["batch", "microchannel", "steady"], default=None,
                     help="small cases of the other kernels, for ncu captures (a few GB at most)")
     ap.add_argument("--chip2d-rows", type=int, default=1000, help="rows of the 2-D chip leg's trace")
@@ -494,6 +498,8 @@ def leg_serving(args):
                       replicas=args.serving_replicas, probe_rate=args.serving_probe_rate, probe_class=hp[0])
     calm = serving_mix(d, srv, seed=5, rate=args.serving_calm_rate, duration=args.serving_calm_seconds,
                        high_priority_classes=hp, reuse=mix, replicas=args.serving_replicas)
+    if args.serving_batching:
+        srv.set_batching(True)
     # every resident model (every member of every pool) serves one request before the clock starts
     warm = []
     for _, mi in mix.classes.items():
@@ -518,8 +524,16 @@ def leg_serving(args):
                 "latency_transient": latency_report([r for r in reqs if r.kind == 1]),
                 "latency_steady_256x256_4layers": latency_report(reqs, tag),
                 "service_ms_steady_256x256_4layers": float(np.median(svc)) if svc else None}
+    e0 = srv.batch_stats()
     srv.run(mix.requests)
+    e1 = srv.batch_stats()
     loaded = report(mix.requests, 2000.0 + args.serving_probe_rate, args.serving_seconds)
+    ticks = e1["ticks"] - e0["ticks"]
+    loaded["batch_engine"] = {
+        "ticks": ticks,
+        "requests_per_tick": ((e1["requests_per_tick"] * e1["ticks"] - e0["requests_per_tick"] * e0["ticks"]) / ticks
+                              if ticks else 0.0),
+        "request_intervals": e1["request_intervals"] - e0["request_intervals"]}
     srv.run(calm.requests)
     sustainable = report(calm.requests, args.serving_calm_rate, args.serving_calm_seconds)
     res = {"workload": "Poisson arrivals at 2000 req/s: 70% steady (sides 64..1024, 1..8 chip layers), 30% "
@@ -527,7 +541,10 @@ def leg_serving(args):
                        f"(256x256, 4 chip layers, steady) at {args.serving_probe_rate:g} req/s; "
                        f"{args.serving_replicas} resident models per class of side <= 256 (a pool), one above; "
                        "the SLO class in the high-priority class with 2 reserved workers; other requests pause "
-                       "between transient chunks and steady refinement passes while it runs",
+                       "between transient chunks and steady refinement passes while it runs; "
+                       + ("transients served by the continuous batch engine (every admitted transient of one "
+                          "interval length advanced together, a few intervals per launch; requests join and leave "
+                          "between launches)" if args.serving_batching else "transients on the workers"),
            "models": len(mix.models), "workers": workers, "offered_2000_req_per_s": loaded,
            "sustainable_rate": sustainable, "setup_s": setup_s}
     srv.close()
@@ -597,6 +614,7 @@ def run_ours(args):
     barrier()
     clk = clocks.stop()
     fast_state = m.grid("trans")
+    head_kernel = m.transient_kernel()
     if args.profile:
         print(json.dumps({"profile_case": True, "intervals": K, "device_ms": dev_ms,
                           "kernel_ms": ker_ms, "rk4_steps": steps_total}), flush=True)
@@ -654,9 +672,10 @@ def run_ours(args):
         # the FP64 forms on the same trace: the replay of the reference's own
         # operation order (bit-identical to it), and the temporally blocked
         # Krylov form with FP64 passes (within 1e-6 K of the replay)
-        from hotspot_b200 import FORM_FP64_BLOCKED
+        from hotspot_b200 import FORM_FAST_BLOCKED, FORM_FP64_BLOCKED
         plain = {}
-        for name, form in (("replay", FORM_PARITY), ("fp64_blocked", FORM_FP64_BLOCKED)):
+        for name, form in (("replay", FORM_PARITY), ("fp64_blocked", FORM_FP64_BLOCKED),
+                           ("fast_blocked", FORM_FAST_BLOCKED)):
             mp_ = hm.from_scenario(sc)
             mp_.set_solver(form)
             tp = mp_.vector(mp_.config.init_temp)
@@ -679,7 +698,7 @@ def run_ours(args):
                 plain[name]["steady_ms"] = mp_.stats()["device_ms"]
                 plain[name]["steady_grid"] = mp_.grid("steady")
             mp_.close()
-        rp, fb = plain["replay"], plain["fp64_blocked"]
+        rp, fb, tb = plain["replay"], plain["fp64_blocked"], plain["fast_blocked"]
         # the converged FP64 steady solution by sparse direct LU (the oracle's
         # restatement of the steady system, scipy splu)
         from oracle.restatement import OracleModel
@@ -697,8 +716,12 @@ def run_ours(args):
             "fp64_blocked": {"cell_steps_per_s": fb["rate"], "gpu_launches": fb["launches"],
                              "speedup_fast_vs_fp64_blocked_transient": value / (fb["rate"] * ws),
                              "max_dT_K_vs_replay": float(np.max(np.abs(fb["state"] - rp["state"]))),
-                             "what": "the same temporally blocked Krylov-form kernel as the fast form with every "
-                                     "stencil pass in FP64: the fastest all-FP64 transient here"},
+                             "what": "the temporally blocked Krylov-form kernel with every stencil pass in FP64: "
+                                     "the fastest all-FP64 transient here"},
+            "fast_blocked": {"cell_steps_per_s": tb["rate"], "gpu_launches": tb["launches"],
+                             "max_dT_K_vs_replay": float(np.max(np.abs(tb["state"] - rp["state"]))),
+                             "what": "the fast form's arithmetic on the temporally blocked kernel (the fast form's "
+                                     "kernel from 2^21 cells up; this chip is below that size)"},
             "max_dT_K": {"transient_fast_vs_fp64_replay": float(np.max(np.abs(fast_state - rp["state"]))),
                          "steady_fast_vs_fp64_replay": float(np.max(np.abs(steady_fast_grid - rp["steady_grid"]))),
                          "steady_fast_vs_fp64_direct": float(np.max(np.abs(steady_fast_grid - T_direct))),
@@ -720,7 +743,8 @@ def run_ours(args):
     # the kernel's own events; if the library could not time it, the whole interval
     kernel_timed = ker_ms > 0
     achieved = alg_bytes_launch / (((ker_ms if kernel_timed else dev_ms) / K) / 1e3) / 1e9
-    traffic = profiled_traffic("rk4_tb_kernel_stack256.md")
+    kname = {"passes": "rk4_krylov_kernel", "blocked": "rk4_tb_kernel"}.get(head_kernel, head_kernel)
+    traffic = profiled_traffic(f"{kname}_stack256.md")
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": K,
         "warmup": Wm, "ms_per_step": dev_ms_max / K, "higher_is_better": True, "scaling": "weak",
@@ -730,14 +754,14 @@ def run_ours(args):
                 "d2h_bytes_per_step": d2h},
         "steady_solves_per_s": {"fast": steady_fast, "unit": "solves/s",
                                 "fast_final_fp64_residual_W": steady_fast_residual},
-        "roofline": {"bound": "hbm", "kernel": "rk4_tb_kernel", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic,
                      "alg_bytes_per_launch": alg_bytes_launch,
                      "note": "one launch = one sampling interval; 108 B per cell-step algorithmic (the pass-by-"
-                             "pass form's FP32 stage fields + FP64 state r/w + FP32 power); the temporally blocked "
-                             "kernel keeps the passes in shared memory, and the 393k-cell state fits the 126 MB L2, "
-                             "so it is bound by latency and chip barriers, not HBM" +
+                             "pass form's FP32 stage fields + FP64 state r/w + FP32 power); the fast form runs the "
+                             "pass-by-pass kernel below 2^21 cells, and the 393k-cell working set fits the 126 MB "
+                             "L2, so the launch is bound by latency and grid barriers, not HBM" +
                              ("" if kernel_timed else "; kernel events unavailable: duration = the whole interval's "
                                                       "device time")},
         "gpu_launches": launches,
@@ -755,8 +779,11 @@ def run_ours(args):
                                 "sample": f"2 rows of the same workload x {cores} independent "
                                           "single-threaded replicas"}
     if ws == 1 and not args.headline_only:
+        legs = set(args.legs.split(","))
         for name, fn in (("chip2d", lambda: leg_chip2d(args, flush)), ("batched", lambda: leg_batched(args, flush)),
                          ("microchannel", lambda: leg_microchannel(args)), ("serving", lambda: leg_serving(args))):
+            if name not in legs:
+                continue
             try:
                 line[name] = fn()
             except Exception as e:      # a failed leg is reported, the headline still prints
@@ -778,7 +805,9 @@ def profile_case(args):
     if args.profile_case == "batch":
         from hotspot_b200.batch import Batch
         rng = np.random.default_rng(7)
-        specs = [(256, 8)] * 6 + [(128, 4)] * 6 + [(64, 2)] * 4
+        # 16 x 256x256x10 + 8 x 128x128x6 + 8 x 64x64x4: 11.4M cells, 180 MB
+        # of FP64 state and candidate buffers, above the 126 MB L2
+        specs = [(256, 8)] * 16 + [(128, 4)] * 8 + [(64, 2)] * 8
         scs = [W.scenario_random_chip(d, rng, f"p{i}", side=s, chip_layers=l, steps=8)
                for i, (s, l) in enumerate(specs)]
         models = []
@@ -789,7 +818,7 @@ def profile_case(args):
             m.compute_temp(m.power_vector(sc.block_power[0]), t, 0.0)
             models.append(m)
         bt = Batch(models)
-        bt.set_schedule(2, 1.0)
+        bt.set_schedule(0, 1.0)
         out = []
         for k in range(1, 4):
             st = bt.transient([m.power_vector(sc.block_power[k]) for sc, m in zip(scs, models)], scs[0].dt)

@@ -18,7 +18,7 @@ STR = 512
 EXTRA, EXTRA_SEC = 12, 16
 
 # solver forms / methods (hsb_device.h)
-FORM_PARITY, FORM_FAST, FORM_FAST_STAGES, FORM_FAST_PASSES, FORM_FP64_BLOCKED = 0, 1, 2, 3, 4
+FORM_PARITY, FORM_FAST, FORM_FAST_STAGES, FORM_FAST_PASSES, FORM_FP64_BLOCKED, FORM_FAST_BLOCKED = 0, 1, 2, 3, 4, 5
 STEADY_AUTO, STEADY_GS_REPLAY, STEADY_MG, STEADY_BICGSTAB = 0, 1, 2, 3
 
 
@@ -230,6 +230,7 @@ _SIGS = {
                                           C.POINTER(Stats)]),
     "hsb_dev_get_state": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "hsb_dev_workspaces": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "hsb_dev_transient_kernel": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "hsb_dev_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "hsb_dev_set_state": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "hsb_abi_sizes": (C.c_int, [C.POINTER(C.c_longlong), C.c_int]),
@@ -255,6 +256,9 @@ _SIGS = {
     "hsb_server_add_replica": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "hsb_server_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "hsb_server_set_priority": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "hsb_server_set_batching": (C.c_int, [C.c_void_p, C.c_int]),
+    "hsb_server_batch_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                         C.POINTER(C.c_longlong)]),
     "hsb_dev_set_priority": (C.c_int, [C.c_void_p, C.c_int]),
     "hsb_batch_tuning": (C.c_int, [C.c_void_p, _D, C.c_int]),
 }

@@ -47,6 +47,21 @@ class Batch:
         _check(lib().hsb_batch_transient_trace(self.ptr, _abi.dptr(flat), int(flat.shape[0]), dt, C.byref(st)))
         return st.as_dict()
 
+    def run_subset(self, chips, rows, dt: float) -> dict:
+        """Advance only the models ``chips`` (indices) by len(rows) intervals in
+        one launch; ``rows[k]`` is interval k's list of their block power
+        vectors, in the order of ``chips``."""
+        idx = np.ascontiguousarray(chips, dtype=np.int32)
+        flat = np.ascontiguousarray(np.stack([np.concatenate(r) for r in rows]), dtype=np.float64)
+        st = _abi.Stats()
+        _check(lib().hsb_batch_run_subset(self.ptr, idx.ctypes.data_as(C.POINTER(C.c_int)), int(idx.size),
+                                          _abi.dptr(flat), int(flat.shape[0]), dt, C.byref(st)))
+        return st.as_dict()
+
+    def set_ctas(self, ctas: int):
+        """At most ``ctas`` CTAs per launch (0: every co-resident CTA)."""
+        _check(lib().hsb_batch_set_ctas(self.ptr, int(ctas)))
+
     def set_schedule(self, policy: int, split: float = 1.0):
         """Tile policy (0, 1, 2; see hsb_batch_set_schedule) and CTA-group split."""
         _check(lib().hsb_batch_set_schedule(self.ptr, int(policy), float(split)))

@@ -568,12 +568,12 @@ static int fast_interval_graphed(hsb_dev_model *m, const double *block_power, do
   return HSB_OK;
 }
 
-// HSB_FORM_FAST_PASSES and HSB_FORM_FP64_BLOCKED are the fast form's
-// interval run by another kernel (pass by pass; all-FP64 blocked): record the
-// kernel choice on the model and return the form
+// HSB_FORM_FAST_PASSES, HSB_FORM_FP64_BLOCKED and HSB_FORM_FAST_BLOCKED are
+// the fast form's interval run by a named kernel (pass by pass; all-FP64
+// blocked; blocked): record the kernel choice on the model and return the form
 static int fast_form(hsb_dev_model *m, int form) {
-  if (form == HSB_FORM_FAST_PASSES || form == HSB_FORM_FP64_BLOCKED) {
-    m->fast_passes = form == HSB_FORM_FAST_PASSES ? 1 : 2;
+  if (form == HSB_FORM_FAST_PASSES || form == HSB_FORM_FP64_BLOCKED || form == HSB_FORM_FAST_BLOCKED) {
+    m->fast_passes = form == HSB_FORM_FAST_PASSES ? 1 : form == HSB_FORM_FP64_BLOCKED ? 2 : 3;
     return HSB_FORM_FAST;
   }
   if (form == HSB_FORM_FAST) m->fast_passes = 0;

@@ -141,10 +141,19 @@ namespace hsb {
 StencilArgs make_args(const hsb_dev_model *m, const LayerCoef *L, int nr, int nc);
 int set_error(int code, const std::string &msg);
 int cuda_check(cudaError_t e, const char *what);
+// HSB_OK on cudaSuccess, else the error recorded as cuda_check records it
+inline int cuda_ok(cudaError_t e, const char *what) { return e == cudaSuccess ? 0 : cuda_check(e, what); }
 // raise (never lower) a kernel's dynamic shared memory limit, thread-safe
 int raise_smem_limit(const void *fn, size_t bytes);
 
 // b2g / g2b on the device (temperature_grid.c:1888-2015)
+// host-to-device copy ordered on stream s, complete on return (a plain
+// cudaMemcpy from pageable memory is ordered on the legacy default stream
+// only, which non-blocking streams do not wait for)
+inline cudaError_t h2d_on(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
 int b2g(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type);
 int g2b(hsb_dev_model *m, const double *grid_dev, double *blk_dev);
 // the same on a given stream

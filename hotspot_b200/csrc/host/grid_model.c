@@ -1188,7 +1188,7 @@ int hsb_grid_set_state(grid_model_t *m, int which, const double *in)
 int hsb_grid_set_solver(grid_model_t *m, int form, int steady_method, double steady_tol, int max_iters)
 {
   if (form != HSB_FORM_PARITY && form != HSB_FORM_FAST && form != HSB_FORM_FAST_STAGES &&
-      form != HSB_FORM_FAST_PASSES && form != HSB_FORM_FP64_BLOCKED)
+      form != HSB_FORM_FAST_PASSES && form != HSB_FORM_FP64_BLOCKED && form != HSB_FORM_FAST_BLOCKED)
     return hsb_seterr(HSB_E_ARG, "unknown form %d\n", form);
   m->ext->opts.form = form;
   m->ext->opts.steady_method = steady_method;

@@ -1065,11 +1065,14 @@ static MgLevelDev dev_level(const hsb_dev_model *m, const MgLevel &L, int lvl) {
 static void free_mg(void *p);
 
 // workspace arrays start zeroed: no kernel of the solver depends on what an
-// earlier allocation left in the memory it reuses
+// earlier allocation left in the memory it reuses.  The zeroing is ordered
+// on the model's stream (a non-blocking stream does not wait for work on the
+// legacy default stream: a plain cudaMemset there could land after the
+// coefficients the solver's set-up kernels write)
 template <typename Tp>
-static cudaError_t mg_alloc(Tp **p, size_t bytes) {
+static cudaError_t mg_alloc(Tp **p, size_t bytes, cudaStream_t s) {
   cudaError_t e = cudaMalloc((void **)p, bytes);
-  if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);
+  if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, bytes, s);
   return e;
 }
 
@@ -1092,36 +1095,35 @@ static int mg_setup(hsb_dev_model *m, MgWork **out) {
   w->nlev = (int)w->lv.size();
   for (int l = 0; l < w->nlev; l++) {
     MgLevel &L = w->lv[l];
-    HSB_CUDA(mg_alloc(&L.gE, sizeof(float) * L.ncell));
-    HSB_CUDA(mg_alloc(&L.gS, sizeof(float) * L.ncell));
-    HSB_CUDA(mg_alloc(&L.gB, sizeof(float) * L.ncell));
-    HSB_CUDA(mg_alloc(&L.diag, sizeof(float) * L.ncell));
-    HSB_CUDA(mg_alloc(&L.gAmbL, sizeof(float) * HSB_MAX_LAYERS));
-    HSB_CUDA(mg_alloc(&L.gEdgeNS, sizeof(float) * HSB_MAX_LAYERS));
-    HSB_CUDA(mg_alloc(&L.gEdgeEW, sizeof(float) * HSB_MAX_LAYERS));
-    HSB_CUDA(mg_alloc(&L.x, sizeof(float) * L.n));
-    HSB_CUDA(mg_alloc(&L.f, sizeof(float) * L.n));
-    HSB_CUDA(mg_alloc(&L.r, sizeof(float) * L.n));
-    HSB_CUDA(mg_alloc(&L.pinv, sizeof(float) * NXP * NXP));
+    HSB_CUDA(mg_alloc(&L.gE, sizeof(float) * L.ncell, m->stream));
+    HSB_CUDA(mg_alloc(&L.gS, sizeof(float) * L.ncell, m->stream));
+    HSB_CUDA(mg_alloc(&L.gB, sizeof(float) * L.ncell, m->stream));
+    HSB_CUDA(mg_alloc(&L.diag, sizeof(float) * L.ncell, m->stream));
+    HSB_CUDA(mg_alloc(&L.gAmbL, sizeof(float) * HSB_MAX_LAYERS, m->stream));
+    HSB_CUDA(mg_alloc(&L.gEdgeNS, sizeof(float) * HSB_MAX_LAYERS, m->stream));
+    HSB_CUDA(mg_alloc(&L.gEdgeEW, sizeof(float) * HSB_MAX_LAYERS, m->stream));
+    HSB_CUDA(mg_alloc(&L.x, sizeof(float) * L.n, m->stream));
+    HSB_CUDA(mg_alloc(&L.f, sizeof(float) * L.n, m->stream));
+    HSB_CUDA(mg_alloc(&L.r, sizeof(float) * L.n, m->stream));
+    HSB_CUDA(mg_alloc(&L.pinv, sizeof(float) * NXP * NXP, m->stream));
   }
   const long long n0 = w->lv[0].n, ncell = m->ncell;
-  HSB_CUDA(mg_alloc(&w->gE64, sizeof(double) * ncell));
-  HSB_CUDA(mg_alloc(&w->gS64, sizeof(double) * ncell));
-  HSB_CUDA(mg_alloc(&w->gB64, sizeof(double) * ncell));
-  HSB_CUDA(mg_alloc(&w->gAmb64, sizeof(double) * (HSB_MAX_LAYERS + 3 * NXP + NXP * NXP)));
-  HSB_CUDA(mg_alloc(&w->gEdgeNS64, sizeof(double) * HSB_MAX_LAYERS));
-  HSB_CUDA(mg_alloc(&w->gEdgeEW64, sizeof(double) * HSB_MAX_LAYERS));
-  HSB_CUDA(mg_alloc(&w->r64, sizeof(double) * n0));
-  HSB_CUDA(mg_alloc(&w->b64, sizeof(double) * n0));
-  HSB_CUDA(mg_alloc(&w->p, sizeof(float) * n0));
-  HSB_CUDA(mg_alloc(&w->q, sizeof(float) * n0));
-  HSB_CUDA(mg_alloc(&w->z, sizeof(float) * n0));
-  HSB_CUDA(mg_alloc(&w->e, sizeof(float) * n0));
-  HSB_CUDA(mg_alloc(&w->rr, sizeof(float) * n0));
-  HSB_CUDA(mg_alloc(&w->red, sizeof(double) * 4096));
-  HSB_CUDA(mg_alloc(&w->d_ps, sizeof(PackSys)));
-  HSB_CUDA(mg_alloc(&w->dot_ticket, sizeof(unsigned)));
-  HSB_CUDA(cudaMemset(w->dot_ticket, 0, sizeof(unsigned)));
+  HSB_CUDA(mg_alloc(&w->gE64, sizeof(double) * ncell, m->stream));
+  HSB_CUDA(mg_alloc(&w->gS64, sizeof(double) * ncell, m->stream));
+  HSB_CUDA(mg_alloc(&w->gB64, sizeof(double) * ncell, m->stream));
+  HSB_CUDA(mg_alloc(&w->gAmb64, sizeof(double) * (HSB_MAX_LAYERS + 3 * NXP + NXP * NXP), m->stream));
+  HSB_CUDA(mg_alloc(&w->gEdgeNS64, sizeof(double) * HSB_MAX_LAYERS, m->stream));
+  HSB_CUDA(mg_alloc(&w->gEdgeEW64, sizeof(double) * HSB_MAX_LAYERS, m->stream));
+  HSB_CUDA(mg_alloc(&w->r64, sizeof(double) * n0, m->stream));
+  HSB_CUDA(mg_alloc(&w->b64, sizeof(double) * n0, m->stream));
+  HSB_CUDA(mg_alloc(&w->p, sizeof(float) * n0, m->stream));
+  HSB_CUDA(mg_alloc(&w->q, sizeof(float) * n0, m->stream));
+  HSB_CUDA(mg_alloc(&w->z, sizeof(float) * n0, m->stream));
+  HSB_CUDA(mg_alloc(&w->e, sizeof(float) * n0, m->stream));
+  HSB_CUDA(mg_alloc(&w->rr, sizeof(float) * n0, m->stream));
+  HSB_CUDA(mg_alloc(&w->red, sizeof(double) * 4096, m->stream));
+  HSB_CUDA(mg_alloc(&w->d_ps, sizeof(PackSys), m->stream));
+  HSB_CUDA(mg_alloc(&w->dot_ticket, sizeof(unsigned), m->stream));
   if (w->lv[0].plane >= (1LL << 31) - MGT) return set_error(HSB_E_ARG, "multigrid: more than 2^31 columns per layer");
 
   HSB_CUDA(cudaMallocHost(&w->h_red, sizeof(double) * 8));
@@ -1235,7 +1237,7 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
     float inv32[NXP * NXP];
     for (int a = 0; a < NXP; a++)
       for (int o = 0; o < NXP; o++) inv32[a * NXP + o] = (float)M[a][NXP + o];
-    HSB_CUDA(cudaMemcpy(L.pinv, inv32, sizeof(inv32), cudaMemcpyHostToDevice));
+    HSB_CUDA(h2d_on(L.pinv, inv32, sizeof(inv32), m->stream));
   }
   double pack64[HSB_MAX_LAYERS + 3 * NXP + NXP * NXP];
   memcpy(pack64, gamb, sizeof(double) * HSB_MAX_LAYERS);
@@ -1358,7 +1360,7 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
         for (long long r = 0; r < n; r++)
           for (long long c = 0; c < n; c++) inv[(size_t)r * n + c] = at(r, n + c);
         HSB_CUDA(cudaMalloc(&w->cinv, sizeof(double) * n * n));
-        HSB_CUDA(cudaMemcpy(w->cinv, inv.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice));
+        HSB_CUDA(h2d_on(w->cinv, inv.data(), sizeof(double) * n * n, m->stream));
         w->cn = (int)n;
       }
     }

@@ -145,19 +145,20 @@ static int batch_tiles(hsb_batch *b) {
     int rc;
     if ((rc = tb_fill_chip(m, r, y0, y1, w->pf, w->t1, oi, oj, false, b->cap, &C))) return rc;
     C.bar = b->d_bar + 2 * c;
-    C.boff = b->boff[c];
     b->dyn = std::max(b->dyn, tb_dyn_smem(m->nl, oi, oj, false, b->cap));
   }
   if (b->dyn + tb_static_smem() > b->cap) return set_error(HSB_E_ARG, "batch tiles do not fit shared memory");
-  HSB_CUDA(cudaMemcpy(b->d_chips, b->h_chips.data(), sizeof(TChip) * b->n, cudaMemcpyHostToDevice));
+  HSB_CUDA(h2d_on(b->d_chips, b->h_chips.data(), sizeof(TChip) * b->n, b->stream));
   return raise_smem_limit(tb_kernel(), b->dyn);
 }
 
 // CTA work lists of the chips in `chips` over G CTAs: a chip worth more than
 // a CTA's fair share gets a group of CTAs (chip-local barriers), the rest are
 // packed onto single CTAs, longest first onto the least loaded
-static void batch_lists(const hsb_batch *b, const std::vector<int> &chips, int G, std::vector<int4> &work,
-                        std::vector<int> &wptr) {
+// work item: (chip, rank in its CTA group, group size, offset of the chip's
+// block powers in a row of the launch's power rows); off[k] for chips[k]
+static void batch_lists(const hsb_batch *b, const std::vector<int> &chips, const std::vector<long long> &off, int G,
+                        std::vector<int4> &work, std::vector<int> &wptr) {
   const int n = (int)chips.size();
   // work of a chip: its tiles x the work of a tile x layers
   std::vector<double> wk(n);
@@ -208,7 +209,7 @@ static void batch_lists(const hsb_batch *b, const std::vector<int> &chips, int G
   for (int k : order)
     if (g[k] >= 2)
       for (int r = 0; r < g[k]; r++) {
-        lists.push_back({make_int4(chips[k], r, g[k], 0)});
+        lists.push_back({make_int4(chips[k], r, g[k], (int)off[k])});
         load.push_back(wk[k] / g[k]);
       }
   const int base = (int)lists.size();
@@ -222,7 +223,7 @@ static void batch_lists(const hsb_batch *b, const std::vector<int> &chips, int G
     int best = base;
     for (int q = base; q < (int)lists.size(); q++)
       if (load[q] < load[best]) best = q;
-    lists[best].push_back(make_int4(chips[k], 0, 1, 0));
+    lists[best].push_back(make_int4(chips[k], 0, 1, (int)off[k]));
     load[best] += wk[k];
   }
   work.clear();
@@ -250,18 +251,22 @@ static int batch_schedule(hsb_batch *b) {
   if ((rc = batch_tiles(b))) return rc;
   if ((rc = batch_ctas(b, &G))) return rc;
   std::vector<int> all(b->n);
-  for (int c = 0; c < b->n; c++) all[c] = c;
+  std::vector<long long> off(b->n);
+  for (int c = 0; c < b->n; c++) {
+    all[c] = c;
+    off[c] = b->boff[c];
+  }
   std::vector<int4> work;
   std::vector<int> wptr;
-  batch_lists(b, all, G, work, wptr);
+  batch_lists(b, all, off, G, work, wptr);
   if (b->d_work) cudaFree(b->d_work);
   if (b->d_wptr) cudaFree(b->d_wptr);
   b->d_work = nullptr;
   b->d_wptr = nullptr;
   HSB_CUDA(cudaMalloc(&b->d_work, sizeof(int4) * (work.size() + 1)));
   HSB_CUDA(cudaMalloc(&b->d_wptr, sizeof(int) * wptr.size()));
-  HSB_CUDA(cudaMemcpy(b->d_work, work.data(), sizeof(int4) * work.size(), cudaMemcpyHostToDevice));
-  HSB_CUDA(cudaMemcpy(b->d_wptr, wptr.data(), sizeof(int) * wptr.size(), cudaMemcpyHostToDevice));
+  HSB_CUDA(h2d_on(b->d_work, work.data(), sizeof(int4) * work.size(), b->stream));
+  HSB_CUDA(h2d_on(b->d_wptr, wptr.data(), sizeof(int) * wptr.size(), b->stream));
   b->grid = (int)wptr.size() - 1;
   b->version++;
   return HSB_OK;
@@ -399,8 +404,9 @@ int hsb_batch_create(hsb_batch **out, hsb_dev_model *const *models, int n) {
     b->boff[c + 1] = b->boff[c] + m->total_n_blocks + m->nx;
   }
   b->nbtotal = b->boff[n];
+  if (b->nbtotal >= (1LL << 31)) return fail(set_error(HSB_E_ARG, "batch block vectors exceed 2^31 entries"));
   memset(b->h_out, 0, sizeof(long long) * TB_OUT * n);
-  if (cudaMemcpy(b->d_out, b->h_out, sizeof(long long) * TB_OUT * n, cudaMemcpyHostToDevice) != cudaSuccess)
+  if (h2d_on(b->d_out, b->h_out, sizeof(long long) * TB_OUT * n, b->stream) != cudaSuccess)
     return fail(set_error(HSB_E_CUDA, "batch outputs"));
   if ((rc = batch_schedule(b))) return fail(rc);
   if ((rc = batch_bpow(b, 1))) return fail(rc);
@@ -545,15 +551,15 @@ int hsb_batch_transient_trace(hsb_batch *b, const double *block_powers, int K, d
           void *work = nullptr;
           int fell = 0;
           rc = rk4_fast_interval_begin(m, time_elapsed, st, &work, nullptr);
-          if (!rc) rc = cuda_check(cudaStreamSynchronize(m->stream), "fallback interval");
+          if (!rc) rc = cuda_ok(cudaStreamSynchronize(m->stream), "fallback interval");
           if (!rc) rc = rk4_fast_interval_end(m, work, time_elapsed, st, &fell);
         }
       }
-      if (!rc) rc = cuda_check(cudaStreamSynchronize(m->stream), "fallback intervals");
+      if (!rc) rc = cuda_ok(cudaStreamSynchronize(m->stream), "fallback intervals");
       // the single-model path may have swapped the buffers
       long long now = m->y == b->h_chips[c].y[0] ? 0 : 1;
       b->h_out[(size_t)c * TB_OUT + 6] = now;
-      if (!rc && cudaMemcpy(b->d_out + (size_t)c * TB_OUT + 6, &now, sizeof(now), cudaMemcpyHostToDevice) !=
+      if (!rc && h2d_on(b->d_out + (size_t)c * TB_OUT + 6, &now, sizeof(now), b->stream) !=
                      cudaSuccess)
         rc = set_error(HSB_E_CUDA, "batch state index");
     }
@@ -597,14 +603,20 @@ int hsb_batch_run_subset(hsb_batch *b, const int *chips, int n, const double *bl
   if (!st) st = &local;
   cudaSetDevice(b->device);
   int rc, G;
-  for (int k = 0; k < n; k++)
+  std::vector<char> seen(b->n, 0);
+  for (int k = 0; k < n; k++) {
     if (chips[k] < 0 || chips[k] >= b->n) return set_error(HSB_E_ARG, "chip index out of range");
+    if (seen[chips[k]]++) return set_error(HSB_E_ARG, "a chip is listed twice");
+  }
   if ((rc = batch_bpow(b, K))) return rc;
   if ((rc = batch_ctas(b, &G))) return rc;
   std::vector<int> sub(chips, chips + n);
+  std::vector<long long> off(n + 1, 0);   // packed rows: the listed chips' vectors in list order
+  for (int k = 0; k < n; k++) off[k + 1] = off[k] + (b->boff[sub[k] + 1] - b->boff[sub[k]]);
+  const long long nbt = off[n];
   std::vector<int4> work;
   std::vector<int> wptr;
-  batch_lists(b, sub, G, work, wptr);
+  batch_lists(b, sub, off, G, work, wptr);
   const int need = (int)std::max(work.size(), wptr.size()) + 1;
   if (need > b->scap) {
     void *p[] = {b->d_swork, b->d_swptr};
@@ -626,12 +638,7 @@ int hsb_batch_run_subset(hsb_batch *b, const int *chips, int n, const double *bl
   }
   memcpy(b->h_swork, work.data(), sizeof(int4) * work.size());
   memcpy(b->h_swptr, wptr.data(), sizeof(int) * wptr.size());
-  // the listed chips' block powers of every interval, and their state buffers
-  for (int k = 0; k < K; k++)
-    for (int c : sub) {
-      const long long o = (long long)k * b->nbtotal + b->boff[c];
-      memcpy(b->h_bpow + o, block_powers + o, sizeof(double) * (b->boff[c + 1] - b->boff[c]));
-    }
+  memcpy(b->h_bpow, block_powers, sizeof(double) * nbt * K);
   for (int c : sub) {
     hsb_dev_model *m = b->models[c];
     const long long cur = m->y == b->h_chips[c].y[0] ? 0 : 1;
@@ -641,8 +648,7 @@ int hsb_batch_run_subset(hsb_batch *b, const int *chips, int n, const double *bl
   }
   HSB_CUDA(cudaMemcpyAsync(b->d_out, b->h_out, sizeof(long long) * TB_OUT * b->n, cudaMemcpyHostToDevice,
                            b->stream));
-  HSB_CUDA(cudaMemcpyAsync(b->d_bpow, b->h_bpow, sizeof(double) * b->nbtotal * K, cudaMemcpyHostToDevice,
-                           b->stream));
+  HSB_CUDA(cudaMemcpyAsync(b->d_bpow, b->h_bpow, sizeof(double) * nbt * K, cudaMemcpyHostToDevice, b->stream));
   HSB_CUDA(cudaMemcpyAsync(b->d_swork, b->h_swork, sizeof(int4) * work.size(), cudaMemcpyHostToDevice,
                            b->stream));
   HSB_CUDA(cudaMemcpyAsync(b->d_swptr, b->h_swptr, sizeof(int) * wptr.size(), cudaMemcpyHostToDevice,
@@ -654,7 +660,7 @@ int hsb_batch_run_subset(hsb_batch *b, const int *chips, int n, const double *bl
   const int *wptr_d = b->d_swptr;
   long long *out = b->d_out;
   const double *bpow = b->d_bpow;
-  long long nbtot = b->nbtotal;
+  long long nbtot = nbt;
   long long max_attempts = 10000000;
   int Kk = K;
   double T = time_elapsed;
@@ -679,7 +685,8 @@ int hsb_batch_run_subset(hsb_batch *b, const int *chips, int n, const double *bl
   cudaEventElapsedTime(&kms, b->ev[1], b->ev[2]);
   st->launches += 1;
   st->kernel_ms += kms;
-  for (int c : sub) {
+  for (int q = 0; q < n; q++) {
+    const int c = sub[q];
     hsb_dev_model *m = b->models[c];
     FastWork *w = (FastWork *)m->fast;
     const long long *o = b->h_out + (size_t)c * TB_OUT;
@@ -696,18 +703,18 @@ int hsb_batch_run_subset(hsb_batch *b, const int *chips, int n, const double *bl
       const int iv = (int)o[7];
       st->fallbacks += 1;
       for (int k = iv; k < K; k++) {
-        if ((rc = b2g(m, b->d_bpow + (long long)k * b->nbtotal + b->boff[c], m->pgrid, HSB_V_POWER))) return rc;
+        if ((rc = b2g(m, b->d_bpow + (long long)k * nbt + off[q], m->pgrid, HSB_V_POWER))) return rc;
         if (k == iv) {
           if ((rc = rk4_stage_run(m, w, time_elapsed - tt[0], tt[1], st))) return rc;
         } else {
           void *wk = nullptr;
           int fell = 0;
           if ((rc = rk4_fast_interval_begin(m, time_elapsed, st, &wk, nullptr))) return rc;
-          if ((rc = cuda_check(cudaStreamSynchronize(m->stream), "fallback interval"))) return rc;
+          if ((rc = cuda_ok(cudaStreamSynchronize(m->stream), "fallback interval"))) return rc;
           if ((rc = rk4_fast_interval_end(m, wk, time_elapsed, st, &fell))) return rc;
         }
       }
-      if ((rc = cuda_check(cudaStreamSynchronize(m->stream), "fallback intervals"))) return rc;
+      if ((rc = cuda_ok(cudaStreamSynchronize(m->stream), "fallback intervals"))) return rc;
     }
   }
   st->sim_time += time_elapsed * K;

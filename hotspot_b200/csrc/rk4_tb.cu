@@ -84,10 +84,11 @@ struct TSh {
   double wred[TB_WARPS];
   Coef E, D, F1, K, E1, D1, F11;
   double ps[PMAX];
-  V xs[NXMAX];                         // package inputs of the pass (in the cells' arithmetic)
+  V xs[2][NXMAX];                      // package inputs of pass m in xs[m & 1] (in the cells' arithmetic)
   double gmax, pmax, hprev;
   int lost;
   int dE, dD, eLo, sep, SI, SJ;        // the attempt's plan
+  int SEG;                             // phase 2: band segment length (0: on the sub-tiles)
 };
 
 // ---------------------------------------------------------------------------
@@ -125,78 +126,91 @@ template <> __device__ __forceinline__ const float *tb_power_of<float>(const TCh
 template <> __device__ __forceinline__ const double *tb_power_of<double>(const TChip &C) { return C.pd; }
 
 // ---------------------------------------------------------------------------
-// one stencil pass over the region rectangle [m+1, RI-m-1) x [m+1, RJ-m-1):
+// one stencil pass over the region rectangle [ra, rb) x [ca, cb) of an
+// RI x RJ box whose cell (0, 0) is grid cell (gi0, gj0):
 // P0: dst = V_0 = (p + L y) / C from the state deviations in src;
-// else dst = h L src.  Package inputs from sh.xs (BND: grid-boundary cells
+// else dst = h L src.  Package inputs from xs (BND: grid-boundary cells
 // present in the region).  The operation order per cell is rk4_krylov.cu's.
+// The rectangle's columns are dealt to the CTA's threads in row-major order
+// (consecutive threads take consecutive columns of a row), so every thread
+// gets the same number of columns to within one whatever the rectangle's
+// shape.
 // ---------------------------------------------------------------------------
 template <typename V, int NL, bool BND, bool P0>
-__device__ __forceinline__ void tb_pass(const TChip &C, const TSh<V> &sh, const V *__restrict__ src,
-                                        V *__restrict__ dst, int RI, int RJ, int m, int gi0, int gj0, V hf) {
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+__device__ __forceinline__ void tb_pass(const TChip &C, const TSh<V> &sh, const V *__restrict__ xs,
+                                        const V *__restrict__ src, V *__restrict__ dst, int RI, int RJ, int ra,
+                                        int rb, int ca, int cb, int gi0, int gj0, V hf) {
   const int LP = RI * RJ;
-  const int ra = m + 1, rb = RI - m - 1, ca = m + 1, cb = RJ - m - 1;
+  const int nrow = rb - ra, ncol = cb - ca;
+  if (nrow <= 0 || ncol <= 0) return;
+  const int tot = nrow * ncol;
   const int nr = C.nr, nc = C.nc;
-  for (int r = ra + w; r < rb; r += TB_WARPS) {
-    const int gi = gi0 + r;
-    if (BND && (unsigned)gi >= (unsigned)nr) continue;
-    for (int c = ca + lane; c < cb; c += 32) {
-      const int gj = gj0 + c;
-      if (BND && (unsigned)gj >= (unsigned)nc) continue;
-      const V *p = src + r * RJ + c;
-      V *o = dst + r * RJ + c;
-      const bool hN = !BND || gi > 0, hS = !BND || gi < nr - 1, hW = !BND || gj > 0, hE = !BND || gj < nc - 1;
-      const V *pw = nullptr;
-      if constexpr (P0) pw = tb_power_of<V>(C) + (long long)gi * nc + gj;
-      V up = 0, cur = p[0], gup = 0;
+  int rr = (int)threadIdx.x / ncol, cc = (int)threadIdx.x - rr * ncol;
+  const int dr = TB_THREADS / ncol, dc = TB_THREADS - dr * ncol;
+  for (int k = threadIdx.x; k < tot; k += TB_THREADS) {
+    const int r = ra + rr, c = ca + cc;
+    cc += dc;
+    rr += dr;
+    if (cc >= ncol) {
+      cc -= ncol;
+      rr++;
+    }
+    const int gi = gi0 + r, gj = gj0 + c;
+    if (BND && ((unsigned)gi >= (unsigned)nr || (unsigned)gj >= (unsigned)nc)) continue;
+    const V *p = src + r * RJ + c;
+    V *o = dst + r * RJ + c;
+    const bool hN = !BND || gi > 0, hS = !BND || gi < nr - 1, hW = !BND || gj > 0, hE = !BND || gj < nc - 1;
+    const V *pw = nullptr;
+    if constexpr (P0) pw = tb_power_of<V>(C) + (long long)gi * nc + gj;
+    V up = 0, cur = p[0], gup = 0;
 #pragma unroll
-      for (int n = 0; n < NL; n++) {
-        const V *pn = p + n * LP;
-        V gNS, gEW, gDn, invC, gEdgeNS, gEdgeEW, gAmb;
-        int nb;
-        if constexpr (sizeof(V) == 4) {   // two vector loads of the FP32 table
-          const float4 L4 = *reinterpret_cast<const float4 *>(&sh.L[n]);          // gNS, gEW, gDn, invC
-          const float4 E4 = *reinterpret_cast<const float4 *>(&sh.L[n].gEdgeNS);  // gEdgeNS, gEdgeEW, gAmb, nbase
-          gNS = L4.x; gEW = L4.y; gDn = L4.z; invC = L4.w;
-          gEdgeNS = E4.x; gEdgeEW = E4.y; gAmb = E4.z;
-          nb = __float_as_int(E4.w);
-        } else {
-          gNS = sh.L[n].gNS; gEW = sh.L[n].gEW; gDn = sh.L[n].gDn; invC = sh.L[n].invC;
-          gEdgeNS = sh.L[n].gEdgeNS; gEdgeEW = sh.L[n].gEdgeEW; gAmb = sh.L[n].gAmb;
-          nb = sh.L[n].nbase;
-        }
-        const V dn = n < NL - 1 ? pn[LP] : V(0);
-        V s = 0;
-        if (hN) s += gNS * (pn[-RJ] - cur);
-        if (hS) s += gNS * (pn[RJ] - cur);
-        if (hE) s += gEW * (pn[1] - cur);
-        if (hW) s += gEW * (pn[-1] - cur);
-        if (n > 0) s += gup * (up - cur);
-        if (n < NL - 1) s += gDn * (dn - cur);
-        s -= gAmb * cur;                         // sink / PCB to ambient (0 elsewhere)
-        if (BND) {
-          if (nb >= 0) {
-            if (gi == 0) s += gEdgeNS * (sh.xs[nb + 2] - cur);
-            if (gi == nr - 1) s += gEdgeNS * (sh.xs[nb + 3] - cur);
-            if (gj == nc - 1) s += gEdgeEW * (sh.xs[nb + 1] - cur);
-            if (gj == 0) s += gEdgeEW * (sh.xs[nb + 0] - cur);
-          }
-        }
-        if constexpr (P0) o[n * LP] = (__ldg(pw + (long long)n * C.plane) + s) * invC;
-        else o[n * LP] = s * (invC * hf);
-        gup = gDn;
-        up = cur;
-        cur = dn;
+    for (int n = 0; n < NL; n++) {
+      const V *pn = p + n * LP;
+      V gNS, gEW, gDn, invC, gEdgeNS, gEdgeEW, gAmb;
+      int nb;
+      if constexpr (sizeof(V) == 4) {   // two vector loads of the FP32 table
+        const float4 L4 = *reinterpret_cast<const float4 *>(&sh.L[n]);          // gNS, gEW, gDn, invC
+        const float4 E4 = *reinterpret_cast<const float4 *>(&sh.L[n].gEdgeNS);  // gEdgeNS, gEdgeEW, gAmb, nbase
+        gNS = L4.x; gEW = L4.y; gDn = L4.z; invC = L4.w;
+        gEdgeNS = E4.x; gEdgeEW = E4.y; gAmb = E4.z;
+        nb = __float_as_int(E4.w);
+      } else {
+        gNS = sh.L[n].gNS; gEW = sh.L[n].gEW; gDn = sh.L[n].gDn; invC = sh.L[n].invC;
+        gEdgeNS = sh.L[n].gEdgeNS; gEdgeEW = sh.L[n].gEdgeEW; gAmb = sh.L[n].gAmb;
+        nb = sh.L[n].nbase;
       }
+      const V dn = n < NL - 1 ? pn[LP] : V(0);
+      V s = 0;
+      if (hN) s += gNS * (pn[-RJ] - cur);
+      if (hS) s += gNS * (pn[RJ] - cur);
+      if (hE) s += gEW * (pn[1] - cur);
+      if (hW) s += gEW * (pn[-1] - cur);
+      if (n > 0) s += gup * (up - cur);
+      if (n < NL - 1) s += gDn * (dn - cur);
+      s -= gAmb * cur;                         // sink / PCB to ambient (0 elsewhere)
+      if (BND) {
+        if (nb >= 0) {
+          if (gi == 0) s += gEdgeNS * (xs[nb + 2] - cur);
+          if (gi == nr - 1) s += gEdgeNS * (xs[nb + 3] - cur);
+          if (gj == nc - 1) s += gEdgeEW * (xs[nb + 1] - cur);
+          if (gj == 0) s += gEdgeEW * (xs[nb + 0] - cur);
+        }
+      }
+      if constexpr (P0) o[n * LP] = (__ldg(pw + (long long)n * C.plane) + s) * invC;
+      else o[n * LP] = s * (invC * hf);
+      gup = gDn;
+      up = cur;
+      cur = dn;
     }
   }
 }
 
 template <typename V, int NL, bool P0>
-__device__ __forceinline__ void tb_pass_any(bool bnd, const TChip &C, const TSh<V> &sh, const V *src, V *dst,
-                                            int RI, int RJ, int m, int gi0, int gj0, V hf) {
-  if (bnd) tb_pass<V, NL, true, P0>(C, sh, src, dst, RI, RJ, m, gi0, gj0, hf);
-  else tb_pass<V, NL, false, P0>(C, sh, src, dst, RI, RJ, m, gi0, gj0, hf);
+__device__ __forceinline__ void tb_pass_any(bool bnd, const TChip &C, const TSh<V> &sh, const V *xs, const V *src,
+                                            V *dst, int RI, int RJ, int ra, int rb, int ca, int cb, int gi0, int gj0,
+                                            V hf) {
+  if (bnd) tb_pass<V, NL, true, P0>(C, sh, xs, src, dst, RI, RJ, ra, rb, ca, cb, gi0, gj0, hf);
+  else tb_pass<V, NL, false, P0>(C, sh, xs, src, dst, RI, RJ, ra, rb, ca, cb, gi0, gj0, hf);
 }
 
 // the sides of the grid a sub-tile's own cells lie on: bit 0 N, 1 S, 2 W, 3 E
@@ -232,14 +246,21 @@ __device__ __forceinline__ void tb_edge_sums(const TChip &C, TSh<V> &sh, const V
   }
 }
 
-// One sub-tile: load the state box, run passes 0 .. dE.  phase 1 (A):
-// package input only through V_0; OUT: finish the own cells (candidate
-// state, error); SUMS: edge sums into sh.es.  phase 2 (V): package input
-// sh.Vp through every pass; OUT always.
+// a cell the package reaches within an attempt: B_m (below) is zero more
+// than m - 1 cells from the grid's edge, so every B_m of an attempt of degree
+// dE is zero at in-plane distance dE and beyond
+__device__ __forceinline__ bool tb_band(const TChip &C, int gi, int gj, int dE) {
+  return min(min(gi, C.nr - 1 - gi), min(gj, C.nc - 1 - gj)) < dE;
+}
+
+// One sub-tile, phase 1: load the state box, run passes 0 .. dE of the A
+// part (package input through V_0 only: A_0 = V_0, A_m = h L_cc A_{m-1});
+// SUMS: edge sums into sh.es.  Own cells out of the package's reach finish
+// (candidate state, error); the others get the A part of their increment in
+// the candidate state and of their error sum in C.ea, finished by tb_bbox.
 template <typename V, int NL>
 __device__ void tb_subtile(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, const double *__restrict__ yb,
-                           double *__restrict__ yn, int i0, int j0, bool phase2, bool out, bool sums,
-                           double h, double &errl) {
+                           double *__restrict__ yn, int i0, int j0, bool sums, double h, double &errl) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int dE = sh.dE, dD = sh.dD, eLo = sh.eLo, H = dE + 1;
   const int SI = sh.SI, SJ = sh.SJ;
@@ -254,12 +275,13 @@ __device__ void tb_subtile(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, const d
   // own cells of this thread: slot s -> own index tid + s * TB_THREADS
   int q[S];
   long long g[S];
-  bool ok[S];
+  bool ok[S], bd[S];
 #pragma unroll
   for (int s = 0; s < S; s++) {
     const int idx = tid + s * TB_THREADS;
     const int oi = idx / SJ, oj = idx - (idx / SJ) * SJ;
-    ok[s] = out && idx < SI * SJ && i0 + oi < nr && j0 + oj < nc;
+    ok[s] = idx < SI * SJ && i0 + oi < nr && j0 + oj < nc;
+    bd[s] = tb_band(C, i0 + oi, j0 + oj, dE);
     q[s] = (oi + H) * RJ + (oj + H);
     g[s] = (long long)(i0 + oi) * nc + (j0 + oj);
   }
@@ -283,68 +305,184 @@ __device__ void tb_subtile(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, const d
       for (int n = 0; n < NL; n++) buf0[n * LP + r * RJ + c] = (V)(__ldcg(py + (long long)n * C.plane) - amb);
     }
   }
-  if (tid < C.nx) sh.xs[tid] = (V)(sh.yp[tid] - amb);
+  if (tid < C.nx) sh.xs[0][tid] = (V)(sh.yp[tid] - amb);
   __syncthreads();
   if (sums) tb_edge_sums<V>(C, sh, nullptr, yb, 0, RI, RJ, H, i0, j0, SI, SJ, sides);
 
+  // One CTA barrier per pass.  After the barrier that ends pass m, a thread
+  // reads pass m's output (own cells, edge sums) and goes on to pass m + 1,
+  // which writes the buffer pass m read: every thread finished reading it
+  // before that barrier.  Package inputs are double-buffered for the same
+  // reason: pass m + 1's are written before the barrier that ends pass m.
   V *src = buf0, *dst = buf1;
   const V hf = (V)h;
   for (int m = 0; m <= dE; m++) {
-    if (m == 0) tb_pass_any<V, NL, true>(bnd, C, sh, src, dst, RI, RJ, 0, gi0, gj0, V(1));
-    else tb_pass_any<V, NL, false>(bnd, C, sh, src, dst, RI, RJ, m, gi0, gj0, hf);
+    if (m == 0) tb_pass_any<V, NL, true>(bnd, C, sh, sh.xs[0], src, dst, RI, RJ, 1, RI - 1, 1, RJ - 1, gi0, gj0, V(1));
+    else
+      tb_pass_any<V, NL, false>(bnd, C, sh, sh.xs[m & 1], src, dst, RI, RJ, m + 1, RI - m - 1, m + 1, RJ - m - 1, gi0,
+                                gj0, hf);
+    // the next pass's package input: none after V_0
+    if (tid < C.nx) sh.xs[(m + 1) & 1][tid] = V(0);
     __syncthreads();
-    // the next pass's package inputs (phase 1: none after V_0)
-    if (tid < C.nx) sh.xs[tid] = phase2 ? (V)sh.Vp[m][tid] : V(0);
-    if (out) {
-      const double cd = m <= dD ? sh.D.c[m] : 0.0, ce = m >= eLo ? sh.E.c[m] : 0.0;
-      if (sep) {
-        const double cf = m <= dD ? cd : ce;
-        if (cf != 0.0) {
+    const double cd = m <= dD ? sh.D.c[m] : 0.0, ce = m >= eLo ? sh.E.c[m] : 0.0;
+    if (sep) {
+      const double cf = m <= dD ? cd : ce;
+      if (cf != 0.0) {
 #pragma unroll
-          for (int s = 0; s < S; s++)
-            if (ok[s])
+        for (int s = 0; s < S; s++)
+          if (ok[s])
 #pragma unroll
-              for (int n = 0; n < NL; n++) acc[s][n] += cf * (double)dst[n * LP + q[s]];
-        }
-        if (m == dD) {   // the increment is complete: the candidate state, then the error sums
-#pragma unroll
-          for (int s = 0; s < S; s++)
-            if (ok[s])
-#pragma unroll
-              for (int n = 0; n < NL; n++) {
-                const long long cc = (long long)n * C.plane + g[s];
-                yn[cc] = __ldcg(yb + cc) + acc[s][n];
-                acc[s][n] = 0.0;
-              }
-        }
-      } else {   // overlapping increment and error terms (a retry): the increment in the candidate state
+            for (int n = 0; n < NL; n++) acc[s][n] += cf * (double)dst[n * LP + q[s]];
+      }
+      if (m == dD) {   // the increment is complete: the candidate state, then the error sums
 #pragma unroll
         for (int s = 0; s < S; s++)
           if (ok[s])
 #pragma unroll
             for (int n = 0; n < NL; n++) {
-              const double v = (double)dst[n * LP + q[s]];
-              if (m <= dD) {
-                const long long cc = (long long)n * C.plane + g[s];
-                yn[cc] = (m == 0 ? __ldcg(yb + cc) : yn[cc]) + cd * v;
-              }
-              acc[s][n] += ce * v;
+              const long long cc = (long long)n * C.plane + g[s];
+              yn[cc] = __ldcg(yb + cc) + acc[s][n];
+              acc[s][n] = 0.0;
             }
       }
+    } else {   // overlapping increment and error terms (a retry): the increment in the candidate state
+#pragma unroll
+      for (int s = 0; s < S; s++)
+        if (ok[s])
+#pragma unroll
+          for (int n = 0; n < NL; n++) {
+            const double v = (double)dst[n * LP + q[s]];
+            if (m <= dD) {
+              const long long cc = (long long)n * C.plane + g[s];
+              yn[cc] = (m == 0 ? __ldcg(yb + cc) : yn[cc]) + cd * v;
+            }
+            acc[s][n] += ce * v;
+          }
     }
     if (sums && m < dE) tb_edge_sums<V>(C, sh, dst, yb, m + 1, RI, RJ, H, i0, j0, SI, SJ, sides);
     V *t = src;
     src = dst;
     dst = t;
+  }
+  __syncthreads();   // the last pass's output is read; the buffers are free for the next sub-tile
+#pragma unroll
+  for (int s = 0; s < S; s++)
+    if (ok[s])
+#pragma unroll
+      for (int n = 0; n < NL; n++) {
+        if (bd[s]) C.ea[(long long)n * C.plane + g[s]] = acc[s][n];
+        else errl = fmax(errl, fabs(acc[s][n]));
+      }
+}
+
+// Phase 2 on one box: the package part B of V_1 .. V_dE, B_0 = 0 and
+// B_m = h (L_cc B_{m-1} + L_cp V^p_{m-1}), over the box [gi0, gi0 + RI) x
+// [gj0, gj0 + RJ) holding the own rectangle [i0, i0 + SI) x [j0, j0 + SJ).
+// Box sides on the grid's edge (fN, fS, fW, fE) are fixed; the others shrink
+// by one cell per pass, and lie dE + 1 cells beyond the own rectangle.  Own
+// cells the package reaches finish: the increment gets sum D_m B_m on top of
+// its A part, the error |E.A + E.B| enters the norm.
+template <typename V, int NL>
+__device__ void tb_bbox(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, double *__restrict__ yn, int i0, int j0,
+                        int SI, int SJ, int gi0, int gj0, int RI, int RJ, bool fN, bool fS, bool fW, bool fE,
+                        double h, double &errl) {
+  const int tid = threadIdx.x;
+  const int dE = sh.dE, dD = sh.dD, eLo = sh.eLo;
+  const int LP = RI * RJ;
+  const int nr = C.nr, nc = C.nc;
+  const bool bnd = gi0 < 1 || gj0 < 1 || gi0 + RI > nr - 1 || gj0 + RJ > nc - 1;
+  const bool sep = sh.sep != 0;
+  constexpr int S = tb_slots<V, NL>();
+  int q[S];
+  long long g[S];
+  bool ok[S];
+#pragma unroll
+  for (int s = 0; s < S; s++) {
+    const int idx = tid + s * TB_THREADS;
+    const int oi = idx / SJ, oj = idx - (idx / SJ) * SJ;
+    const int gi = i0 + oi, gj = j0 + oj;
+    ok[s] = idx < SI * SJ && gi < nr && gj < nc && tb_band(C, gi, gj, dE);
+    q[s] = (gi - gi0) * RJ + (gj - gj0);
+    g[s] = (long long)gi * nc + gj;
+  }
+  double acc[S][NL];
+#pragma unroll
+  for (int s = 0; s < S; s++)
+#pragma unroll
+    for (int n = 0; n < NL; n++) acc[s][n] = 0.0;
+  for (int k = tid; k < NL * LP; k += TB_THREADS) buf0[k] = V(0);   // B_0
+  if (tid < C.nx) sh.xs[1][tid] = (V)sh.Vp[0][tid];                 // pass 1's package input
+  __syncthreads();
+  V *src = buf0, *dst = buf1;
+  const V hf = (V)h;
+  for (int m = 1; m <= dE; m++) {
+    tb_pass_any<V, NL, false>(bnd, C, sh, sh.xs[m & 1], src, dst, RI, RJ, fN ? 0 : m + 1, fS ? RI : RI - m - 1,
+                              fW ? 0 : m + 1, fE ? RJ : RJ - m - 1, gi0, gj0, hf);
+    if (tid < C.nx && m < dE) sh.xs[(m + 1) & 1][tid] = (V)sh.Vp[m][tid];
     __syncthreads();
-  }
-  if (out) {
+    const double cd = m <= dD ? sh.D.c[m] : 0.0, ce = m >= eLo ? sh.E.c[m] : 0.0;
+    if (sep) {
+      const double cf = m <= dD ? cd : ce;
+      if (cf != 0.0) {
 #pragma unroll
-    for (int s = 0; s < S; s++)
-      if (ok[s])
+        for (int s = 0; s < S; s++)
+          if (ok[s])
 #pragma unroll
-        for (int n = 0; n < NL; n++) errl = fmax(errl, fabs(acc[s][n]));
+            for (int n = 0; n < NL; n++) acc[s][n] += cf * (double)dst[n * LP + q[s]];
+      }
+      if (m == dD) {
+#pragma unroll
+        for (int s = 0; s < S; s++)
+          if (ok[s])
+#pragma unroll
+            for (int n = 0; n < NL; n++) {
+              const long long cc = (long long)n * C.plane + g[s];
+              yn[cc] = __ldcg(yn + cc) + acc[s][n];   // written by another CTA in phase 1: read from L2
+              acc[s][n] = 0.0;
+            }
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < S; s++)
+        if (ok[s])
+#pragma unroll
+          for (int n = 0; n < NL; n++) {
+            const double v = (double)dst[n * LP + q[s]];
+            if (m <= dD) {
+              const long long cc = (long long)n * C.plane + g[s];
+              yn[cc] = __ldcg(yn + cc) + cd * v;
+            }
+            acc[s][n] += ce * v;
+          }
+    }
+    V *t = src;
+    src = dst;
+    dst = t;
   }
+  __syncthreads();
+#pragma unroll
+  for (int s = 0; s < S; s++)
+    if (ok[s])
+#pragma unroll
+      for (int n = 0; n < NL; n++) {
+        const long long cc = (long long)n * C.plane + g[s];
+        errl = fmax(errl, fabs(__ldcg(C.ea + cc) + acc[s][n]));
+      }
+}
+
+// a box for phase 2: the own rectangle [i0, i0 + SI) x [j0, j0 + SJ) with
+// dE + 1 cells of halo, clipped to the grid (clipped sides fixed)
+template <typename V, int NL>
+__device__ __forceinline__ void tb_bbox_own(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, double *yn, int i0, int j0,
+                                            int SI, int SJ, double h, double &errl) {
+  const int H = sh.dE + 1;
+  int lo_i = i0 - H, hi_i = i0 + SI + H, lo_j = j0 - H, hi_j = j0 + SJ + H;
+  const bool fN = lo_i <= 0, fS = hi_i >= C.nr, fW = lo_j <= 0, fE = hi_j >= C.nc;
+  if (fN) lo_i = 0;
+  if (fS) hi_i = C.nr;
+  if (fW) lo_j = 0;
+  if (fE) hi_j = C.nc;
+  tb_bbox<V, NL>(C, sh, buf0, buf1, yn, i0, j0, SI, SJ, lo_i, lo_j, hi_i - lo_i, hi_j - lo_j, fN, fS, fW, fE, h, errl);
 }
 
 // the package recursion: V^p_0 .. V^p_dE from the chip's edge sums of y and
@@ -402,7 +540,7 @@ __device__ __noinline__ void tb_package(const TChip &C, TSh<V> &sh, double h) {
 // the attempt's coefficients (thread 0); returns 0, or 3 when the degree is
 // beyond what a sub-tile of this chip can hold
 template <typename V>
-__device__ __noinline__ int tb_plan(const TChip &C, TSh<V> &sh, double h, bool first) {
+__device__ __noinline__ int tb_plan(const TChip &C, TSh<V> &sh, double h, bool first, int size) {
   if (first) {
     for (int q = 0; q < PMAX; q++) sh.ps[q] = h;
     sh.E.n = sh.E1.n;
@@ -435,6 +573,16 @@ __device__ __noinline__ int tb_plan(const TChip &C, TSh<V> &sh, double h, bool f
   // sub-tile: the own tile, halved until its box fits the buffers and its
   // own cells fit the threads' accumulator slots
   const int H = dE + 1, slots = tb_slots_rt(sizeof(V) == 8, C.nl);
+  // phase 2's band segments: a box of 2 dE + 1 cells across the band and
+  // SEG + 2 H along it; about one segment per CTA of the chip, at least 8 long
+  {
+    int fit = C.rcap / (2 * dE + 1) - 2 * H;
+    if (dE > 0 && fit > TB_THREADS * slots / dE) fit = TB_THREADS * slots / dE;
+    const int perim = 2 * C.nc + 2 * max(0, C.nr - 2 * dE);
+    int seg = max(8, (perim + size - 1) / size);
+    if (seg > fit) seg = fit;
+    sh.SEG = seg >= 4 ? seg : 0;
+  }
   for (int SJ = C.oj; SJ >= 8; SJ >>= 1)
     for (int SI = C.oi; SI >= 1; SI >>= 1)
       if ((SI + 2 * H) * (SJ + 2 * H) <= C.rcap && SI * SJ <= TB_THREADS * slots) {
@@ -447,8 +595,9 @@ __device__ __noinline__ int tb_plan(const TChip &C, TSh<V> &sh, double h, bool f
 
 // grid power of interval iv for this CTA's tiles, in the kernel's type
 template <typename V>
-__device__ void tb_power(const TChip &C, int rank, int size, int K, int iv, const double *bpow, long long nbtot) {
-  const double *b = K > 0 ? bpow + (long long)iv * nbtot + C.boff : nullptr;
+__device__ void tb_power(const TChip &C, int rank, int size, int K, int iv, const double *bpow, long long nbtot,
+                         long long boff) {
+  const double *b = K > 0 ? bpow + (long long)iv * nbtot + boff : nullptr;
   const bool last = K > 0 && iv == K - 1;
   for (int t = rank; t < C.ntiles; t += size) {
     const int i0 = (t / C.ntj) * C.oi, j0 = (t % C.ntj) * C.oj;
@@ -476,7 +625,7 @@ __device__ void tb_power(const TChip &C, int rank, int size, int K, int iv, cons
 // group of `size` CTAs of which this is `rank`
 template <typename V, int NL>
 __device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh<V> &sh, V *dyn, double T, int K,
-                        const double *bpow, long long nbtot, long long max_attempts) {
+                        const double *bpow, long long nbtot, long long boff, long long max_attempts) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int nx = C.nx;
   V *buf0 = dyn, *buf1 = dyn + (size_t)C.rcap * NL;
@@ -495,7 +644,7 @@ __device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh<
   int iv = 0;
   if (rank == 0 && tid < 3) C.err[tid] = 0ull;
   for (iv = 0; iv < nint && !status && !sh.lost; iv++) {
-    tb_power<V>(C, rank, size, K, iv, bpow, nbtot);
+    tb_power<V>(C, rank, size, K, iv, bpow, nbtot, boff);
     tsync(C, size, gen, sh);
     t = 0.0;
     new_h = 1e-7;
@@ -505,7 +654,7 @@ __device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh<
       double mx = 0.0;
       for (;;) {
         h = new_h;
-        if (tid == 0) status = tb_plan(C, sh, h, first);
+        if (tid == 0) status = tb_plan(C, sh, h, first, size);
         if (tid == 0) sh.wred[0] = (double)status;
         __syncthreads();
         status = (int)sh.wred[0];
@@ -528,10 +677,8 @@ __device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh<
             for (int sj = 0; sj < C.oj; sj += SJ) {
               const int i0 = ti0 + si, j0 = tj0 + sj;
               if (i0 >= C.nr || j0 >= C.nc) continue;
-              const bool ring = i0 < dE || j0 < dE || i0 + SI > C.nr - dE || j0 + SJ > C.nc - dE;
               const bool sums = tb_sides(C, i0, j0, SI, SJ) != 0;
-              if (!ring || sums)
-                tb_subtile<V, NL>(C, sh, buf0, buf1, yb, yn, i0, j0, false, !ring, sums, h, errl);
+              tb_subtile<V, NL>(C, sh, buf0, buf1, yb, yn, i0, j0, sums, h, errl);
             }
           if (tsides) {   // this tile's partial edge sums
             const int ti = tt / C.ntj, tj = tt % C.ntj;
@@ -561,16 +708,43 @@ __device__ void tb_chip(const TChip &C, int rank, int size, long long *out, TSh<
         if (w == 0) tb_package<V>(C, sh, h);
         if (rank == 0 && tid == 0) C.err[(a + 1) % 3] = 0ull;
         __syncthreads();
-        // ---- phase 2: V on the tiles within dE cells of the boundary
-        for (int tt = rank; tt < C.ntiles && !sh.lost; tt += size) {
-          const int ti0 = (tt / C.ntj) * C.oi, tj0 = (tt % C.ntj) * C.oj;
-          for (int si = 0; si < C.oi; si += SI)
-            for (int sj = 0; sj < C.oj; sj += SJ) {
-              const int i0 = ti0 + si, j0 = tj0 + sj;
-              if (i0 >= C.nr || j0 >= C.nc) continue;
-              const bool ring = i0 < dE || j0 < dE || i0 + SI > C.nr - dE || j0 + SJ > C.nc - dE;
-              if (ring) tb_subtile<V, NL>(C, sh, buf0, buf1, yb, yn, i0, j0, true, true, false, h, errl);
+        // ---- phase 2: the package part B on the band within dE cells of
+        // the grid's edge, in segments dealt over the chip's CTAs (the four
+        // strips: N and S full width, W and E between them); or, when no
+        // segment box fits the buffers, on the sub-tiles that reach the band
+        if (sh.SEG > 0) {
+          const int SEG = sh.SEG, nr = C.nr, nc = C.nc;
+          const int b = min(dE, nr), sS = max(b, nr - dE), wc = min(dE, nc), eC = max(wc, nc - dE);
+          const int nN = (nc + SEG - 1) / SEG, nS = sS < nr ? nN : 0;
+          const int nW = sS > b ? (sS - b + SEG - 1) / SEG : 0, nE = eC < nc ? nW : 0;
+          for (int sg = rank; sg < nN + nS + nW + nE && !sh.lost; sg += size) {
+            int i0, j0, si, sj;
+            if (sg < nN + nS) {
+              const int k = sg < nN ? sg : sg - nN;
+              j0 = k * SEG;
+              sj = min(SEG, nc - j0);
+              i0 = sg < nN ? 0 : sS;
+              si = sg < nN ? b : nr - sS;
+            } else {
+              const int k = sg - nN - nS, kk = k < nW ? k : k - nW;
+              i0 = b + kk * SEG;
+              si = min(SEG, sS - i0);
+              j0 = k < nW ? 0 : eC;
+              sj = k < nW ? wc : nc - eC;
             }
+            tb_bbox_own<V, NL>(C, sh, buf0, buf1, yn, i0, j0, si, sj, h, errl);
+          }
+        } else {
+          for (int tt = rank; tt < C.ntiles && !sh.lost; tt += size) {
+            const int ti0 = (tt / C.ntj) * C.oi, tj0 = (tt % C.ntj) * C.oj;
+            for (int si = 0; si < C.oi; si += SI)
+              for (int sj = 0; sj < C.oj; sj += SJ) {
+                const int i0 = ti0 + si, j0 = tj0 + sj;
+                if (i0 >= C.nr || j0 >= C.nc) continue;
+                const bool reach = i0 < dE || j0 < dE || i0 + SI > C.nr - dE || j0 + SJ > C.nc - dE;
+                if (reach) tb_bbox_own<V, NL>(C, sh, buf0, buf1, yn, i0, j0, SI, SJ, h, errl);
+              }
+          }
         }
         // ---- the error norm: cells (all CTAs of the chip) and package nodes
         for (int o = 16; o > 0; o >>= 1) errl = fmax(errl, __shfl_down_sync(0xffffffffu, errl, o));
@@ -683,7 +857,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
     long long *o = out + (long long)it.x * TB_OUT;
     switch (C.nl) {
 #define TB_CASE(n) \
-  case n: tb_chip<V, n>(C, it.y, it.z, o, sh, tdyn, T, K, bpow, nbtot, max_attempts); break;
+  case n: tb_chip<V, n>(C, it.y, it.z, o, sh, tdyn, T, K, bpow, nbtot, it.w, max_attempts); break;
       TB_CASE(3) TB_CASE(4) TB_CASE(5) TB_CASE(6) TB_CASE(7) TB_CASE(8) TB_CASE(9) TB_CASE(10) TB_CASE(11)
       TB_CASE(12)
 #undef TB_CASE
@@ -945,7 +1119,6 @@ int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1,
   C->pf = pf;
   C->pd = pd;
   C->pgrid = m->pgrid;
-  C->boff = 0;
   C->b2g_ptr = m->b2g_ptr;
   C->b2g_blk = m->b2g_blk;
   C->b2g_occ = m->b2g_occ;
@@ -956,6 +1129,7 @@ int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1,
   C->pk = r->pk;
   C->er = r->er;
   C->part = r->part;
+  C->ea = r->ea;
   C->err = r->err;
   C->bar = r->bar;
   C->ncell = m->ncell;
@@ -983,7 +1157,7 @@ int tb_fill_chip(hsb_dev_model *m, TbRes *r, const double *y0, const double *y1,
 
 void tb_res_free(TbRes *r) {
   if (!r) return;
-  void *d[] = {r->L, r->Ld, r->part, r->err, r->bar, r->d_chip};   // pk is the fast workspace's; er the cache's
+  void *d[] = {r->L, r->Ld, r->part, r->ea, r->err, r->bar, r->d_chip};   // pk is the fast workspace's; er the cache's
   for (void *p : d)
     if (p) cudaFree(p);
   delete r;
@@ -1016,6 +1190,7 @@ int tb_res_prepare(hsb_dev_model *m, TbRes **out, const PackF *pk_dev) {
     HSB_CUDA(cudaMalloc(&r->L, sizeof(TLayer) * TB_NLMAX));
     HSB_CUDA(cudaMalloc(&r->Ld, sizeof(TLayerD) * TB_NLMAX));
     HSB_CUDA(cudaMalloc(&r->part, sizeof(double) * (TB_DMAX + 1) * NEDGE * r->segmax));
+    HSB_CUDA(cudaMalloc(&r->ea, sizeof(double) * m->ncell));
     HSB_CUDA(cudaMalloc(&r->err, sizeof(unsigned long long) * 4));
     HSB_CUDA(cudaMalloc(&r->bar, sizeof(unsigned) * 2));
     HSB_CUDA(cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, m->stream));

@@ -39,7 +39,6 @@ struct TChip {
   float *pf;                        // FP32 grid power (FP32 kernel)
   double *pd;                       // FP64 grid power (FP64 kernel; a scratch vector of ncell doubles)
   double *pgrid;                    // FP64 grid power (K = 0: source; K > 0: the last interval's, written)
-  long long boff;                   // K > 0: this chip's block powers of interval k at bpow + k * nbtot + boff
   const int *b2g_ptr, *b2g_blk;
   const double *b2g_occ, *b2g_area;
   double cell_area;
@@ -48,6 +47,7 @@ struct TChip {
   const PackF *pk;
   const double *er;                 // [TB_JMAX][ne][ne] edge responses
   double *part;                     // [TB_DMAX + 1][NEDGE][segmax] per-tile edge sums
+  double *ea;                       // [ncell] error sums of the A part at cells the package reaches
   unsigned long long *err;          // [3] rotating error-norm slots
   unsigned *bar;                    // [2] chip barrier: arrivals, generation
   long long ncell, plane;
@@ -66,6 +66,7 @@ struct TbRes {
   PackF *pk;
   double *er;
   double *part;
+  double *ea;
   unsigned long long *err;
   unsigned *bar;
   TChip *d_chip;                    // [variant * 2 + role]: FP32 / FP64 kernel; state in the first buffer / second

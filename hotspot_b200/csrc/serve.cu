@@ -30,9 +30,21 @@
 // reached a yield point (at most DRAIN_MS later), so it runs on a drained
 // device instead of interleaving with their kernels.
 //
+// Continuous batching (hsb_server_set_batching): the fast-form models whose
+// layers the temporally blocked kernel takes are gathered into one batch
+// (hsb_batch), and their transient requests are served by a batch engine
+// instead of the workers.  The engine advances every admitted transient of
+// one interval length together, a few intervals per launch (a tick, about
+// TICK_CELL_INTERVALS cell-intervals): between ticks it admits the requests
+// that have arrived onto idle pool members (loading their initial
+// temperatures) and retires the finished ones (reading their block
+// temperatures), so requests join and leave a running batch without waiting
+// for each other.  Steady requests keep running on the workers meanwhile.
+//
 // Each request's result depends only on its model and inputs: the kernels
-// are deterministic and models share no mutable device state, so a result
-// is the same alone and in any mix.
+// are deterministic, models share no mutable device state and a chip's
+// result does not depend on which CTAs advance it or on how its intervals
+// are split over launches, so a result is the same alone and in any mix.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -43,6 +55,7 @@
 #include <vector>
 
 #include "dev_model.cuh"
+#include "rk4_tb.cuh"
 
 // worker threads reserved for high-priority requests
 #define HIGH_SLOTS 2
@@ -51,6 +64,9 @@
 // longest wait of a priority request for background work to reach a yield point
 #define DRAIN_MS 4.0
 #define CHUNK_MAX_INTERVALS 64
+// cell-intervals per launch of the batch engine, and its interval cap
+#define TICK_CELL_INTERVALS (1LL << 22)
+#define TICK_MAX_INTERVALS 16
 
 struct hsb_server {
   int workers = 1;
@@ -63,8 +79,18 @@ struct hsb_server {
     bool busy = false;
     int high = 0;        // priority class
     int cls = 0;         // the pool: index of the first model registered for this class
+    int slot = -1;       // index in the batch, -1: not batched
   };
   std::vector<Model> models;
+  // continuous batching of transients
+  int batching = 0;
+  hsb_batch *batch = nullptr;
+  int batch_built = -1;        // models registered when the batch was built
+  std::vector<long long> boff;  // the batch's block-vector offsets
+  long long ticks = 0, tick_requests = 0, tick_intervals = 0;
+  ~hsb_server() {
+    if (batch) hsb_batch_destroy(batch);
+  }
 };
 
 using namespace hsb;
@@ -128,6 +154,72 @@ int hsb_server_set_priority(hsb_server *s, int model, int high) {
   return HSB_OK;
 }
 
+int hsb_server_set_batching(hsb_server *s, int on) {
+  if (!s) return set_error(HSB_E_ARG, "null server");
+  s->batching = on ? 1 : 0;
+  if (!on && s->batch) {
+    hsb_batch_destroy(s->batch);
+    s->batch = nullptr;
+    s->batch_built = -1;
+    for (auto &M : s->models) M.slot = -1;
+  }
+  return HSB_OK;
+}
+
+int hsb_server_batch_stats(hsb_server *s, long long *ticks, long long *request_ticks, long long *request_intervals) {
+  if (!s) return set_error(HSB_E_ARG, "null server");
+  if (ticks) *ticks = s->ticks;
+  if (request_ticks) *request_ticks = s->tick_requests;
+  if (request_intervals) *request_intervals = s->tick_intervals;
+  return HSB_OK;
+}
+
+// (re)build the batch over the registered fast-form models the temporally
+// blocked kernel takes
+static int build_batch(hsb_server *s) {
+  if (s->batch && s->batch_built == (int)s->models.size()) return HSB_OK;
+  if (s->batch) hsb_batch_destroy(s->batch);
+  s->batch = nullptr;
+  std::vector<hsb_dev_model *> ms;
+  for (auto &M : s->models) {
+    M.slot = -1;
+    if ((M.opts.form == HSB_FORM_FAST || M.opts.form == HSB_FORM_FAST_BLOCKED) && tb_eligible(M.m)) {
+      M.slot = (int)ms.size();
+      ms.push_back(M.m);
+    }
+  }
+  s->batch_built = (int)s->models.size();
+  if (ms.empty()) return HSB_OK;
+  int rc = hsb_batch_create(&s->batch, ms.data(), (int)ms.size());
+  if (rc) {
+    s->batch = nullptr;
+    for (auto &M : s->models) M.slot = -1;
+    return rc;
+  }
+  s->boff.assign(ms.size() + 1, 0);
+  return hsb_batch_offsets(s->batch, s->boff.data());
+}
+
+// the initial block temperatures of a transient into the model's state
+static int load_temps(hsb_dev_model *m, const double *block_temp) {
+  const size_t nb = (size_t)m->total_n_blocks + m->nx;
+  if (cudaSetDevice(m->device) != cudaSuccess) return set_error(HSB_E_CUDA, "cudaSetDevice");
+  HSB_CUDA(cudaMemcpyAsync(m->blk_in + nb, block_temp, sizeof(double) * nb, cudaMemcpyHostToDevice, m->stream));
+  int rc = b2g(m, m->blk_in + nb, m->y, HSB_V_TEMP);
+  if (rc) return rc;
+  return cuda_ok(cudaStreamSynchronize(m->stream), "initial temperatures");
+}
+
+// the block temperatures of the model's state
+static int read_temps(hsb_dev_model *m, double *block_temp) {
+  const size_t nb = (size_t)m->total_n_blocks + m->nx;
+  if (cudaSetDevice(m->device) != cudaSuccess) return set_error(HSB_E_CUDA, "cudaSetDevice");
+  int rc = g2b(m, m->y, m->blk_out);
+  if (rc) return rc;
+  HSB_CUDA(cudaMemcpyAsync(block_temp, m->blk_out, sizeof(double) * nb, cudaMemcpyDeviceToHost, m->stream));
+  return cuda_ok(cudaStreamSynchronize(m->stream), "block temperatures");
+}
+
 // the pause of background requests while high-priority ones run
 struct Gate {
   std::mutex *mu;
@@ -184,11 +276,24 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
   for (int k = 0; k < n; k++)
     if (reqs[k].model < 0 || reqs[k].model >= (int)s->models.size())
       return set_error(HSB_E_ARG, "request names an unknown model");
+  if (s->batching) {
+    const int rc = build_batch(s);
+    if (rc) return rc;
+  }
+  // transients the batch engine serves: a batched, normal-priority pool
+  std::vector<char> isb(n, 0);
+  int n_engine = 0;
+  for (int k = 0; k < n; k++) {
+    const hsb_server::Model &M = s->models[reqs[k].model];
+    isb[k] = s->batch && reqs[k].kind == HSB_REQ_TRANSIENT && reqs[k].steps >= 1 && M.slot >= 0 && !M.high;
+    n_engine += isb[k];
+  }
   std::mutex mu;
   std::condition_variable cv;
   std::vector<int> state(n, 0);   // 0 pending, 1 running, 2 done
   std::vector<int> served_by(n, -1);
   int done = 0, running = 0, running_high = 0, running_low = 0, paused_low = 0;
+  int engine_on = 0;              // the engine holds admitted requests
   bool any_high = false;   // a high-priority request is in this run
   for (int k = 0; k < n; k++) any_high = any_high || s->models[reqs[k].model].high;
   Gate gate{&mu, &cv, &running_high, &paused_low};
@@ -210,7 +315,7 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
       size_t free_b = 0, total_b = 0;
       bool mem_known = false;
       for (int k = 0; k < n; k++) {
-        if (state[k] != 0) continue;
+        if (state[k] != 0 || isb[k]) continue;
         const hsb_request &r = reqs[k];
         if (r.arrival > t) {
           next_arrival = std::min(next_arrival, r.arrival);
@@ -261,17 +366,22 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
           best = k;
       }
       if (best < 0 && running == 0 && next_arrival >= 1e300) {
-        // nothing runs, nothing more arrives: what is left waits on memory
-        // that no request will free -- fail those requests
+        // nothing runs, nothing more arrives: what is left for the workers
+        // waits on memory that no request will free -- fail those requests
+        bool failed_some = false;
         for (int k = 0; k < n; k++)
-          if (state[k] == 0 && reqs[k].arrival <= t) {
+          if (state[k] == 0 && !isb[k] && reqs[k].arrival <= t) {
             reqs[k].status = set_error(HSB_E_NOMEM, "request not admitted: not enough free device memory");
             reqs[k].start = reqs[k].finish = t;
             state[k] = 2;
             done++;
+            failed_some = true;
           }
-        cv.notify_all();
-        continue;
+        if (failed_some) {
+          cv.notify_all();
+          continue;
+        }
+        // nothing of the workers' is left: wait for the batch engine's requests
       }
       if (best < 0) {
         if (next_arrival < 1e300)
@@ -294,7 +404,7 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
         // running background request reaches its next yield point within
         // one chunk or iteration (bounded wait, DRAIN_MS at most)
         const auto until = clk::now() + std::chrono::microseconds((long long)(DRAIN_MS * 1000));
-        while (paused_low < running_low && clk::now() < until) cv.wait_until(lk, until);
+        while (paused_low < running_low + engine_on && clk::now() < until) cv.wait_until(lk, until);
       }
       lk.unlock();
       const int rc = run_request(M, &r, (any_high && !high) ? &gate : nullptr);
@@ -311,9 +421,160 @@ int hsb_server_run(hsb_server *s, hsb_request *reqs, int n) {
       cv.notify_all();
     }
   };
+  // the batch engine: admit, advance one tick, retire
+  auto engine = [&]() {
+    std::vector<int> act, fresh, grp, chips;
+    std::vector<int> prog(n, 0);
+    std::vector<double> rows;
+    std::unique_lock<std::mutex> lk(mu);
+    int eng_done = 0;
+    for (;;) {
+      if (eng_done == n_engine) return;
+      const double t = now();
+      double next_arrival = 1e300;
+      for (int k = 0; k < n; k++) {
+        if (!isb[k] || state[k] != 0) continue;
+        const hsb_request &r = reqs[k];
+        if (r.arrival > t) {
+          next_arrival = std::min(next_arrival, r.arrival);
+          continue;
+        }
+        // an idle batched member of the pool; a transient that continues
+        // the named model's state waits for that model
+        const int cls = s->models[r.model].cls;
+        const bool any = r.temp_in != nullptr;
+        int pick = -1;
+        for (int q = any ? cls : r.model; q < (int)s->models.size(); q++) {
+          const hsb_server::Model &Q = s->models[q];
+          if (Q.cls == cls && !Q.busy && Q.slot >= 0) {
+            pick = q;
+            break;
+          }
+          if (!any) break;
+        }
+        if (pick < 0) continue;
+        served_by[k] = pick;
+        s->models[pick].busy = true;
+        state[k] = 1;
+        running++;
+        reqs[k].start = t;
+        reqs[k].worker = -1;
+        act.push_back(k);
+        fresh.push_back(k);
+      }
+      engine_on = act.empty() ? 0 : 1;
+      if (act.empty()) {
+        if (next_arrival < 1e300)
+          cv.wait_until(lk, t0 + std::chrono::duration_cast<clk::duration>(std::chrono::duration<double>(next_arrival)));
+        else
+          cv.wait(lk);
+        continue;
+      }
+      if (running_high > 0) {   // a priority request runs: pause between ticks
+        ++paused_low;
+        cv.notify_all();
+        while (running_high > 0) cv.wait_for(lk, std::chrono::milliseconds(10));
+        --paused_low;
+        continue;
+      }
+      // one tick over the admitted requests of the first one's interval length
+      const double dt = reqs[act[0]].dt;
+      grp.clear();
+      chips.clear();
+      long long cells = 0;
+      int rem = 1 << 30;
+      for (int k : act)
+        if (reqs[k].dt == dt) {
+          grp.push_back(k);
+          const hsb_server::Model &M = s->models[served_by[k]];
+          chips.push_back(M.slot);
+          cells += M.m->ncell;
+          rem = std::min(rem, reqs[k].steps - prog[k]);
+        }
+      int K = (int)std::max(1LL, std::min<long long>(TICK_MAX_INTERVALS, TICK_CELL_INTERVALS / std::max(1LL, cells)));
+      K = std::min(K, rem);
+      std::vector<int> load(fresh);
+      fresh.clear();
+      lk.unlock();
+      int rc = HSB_OK;
+      std::vector<int> failed;
+      for (int k : load)   // initial temperatures of the requests admitted at this tick
+        if (reqs[k].temp_in) {
+          const int r2 = load_temps(s->models[served_by[k]].m, reqs[k].temp_in);
+          if (r2) {
+            reqs[k].status = r2;
+            failed.push_back(k);
+          }
+        }
+      if (!failed.empty()) rc = HSB_E_CUDA;
+      if (rc == HSB_OK) {   // K rows of the group's block vectors, packed in group order
+        size_t nbt = 0;
+        for (int c : chips) nbt += (size_t)(s->boff[c + 1] - s->boff[c]);
+        rows.resize((size_t)K * nbt);
+        size_t o = 0;
+        for (size_t q = 0; q < grp.size(); q++) {
+          const hsb_request &r = reqs[grp[q]];
+          const size_t nb = (size_t)(s->boff[chips[q] + 1] - s->boff[chips[q]]);
+          for (int i = 0; i < K; i++)
+            memcpy(rows.data() + (size_t)i * nbt + o, r.power + (size_t)(prog[grp[q]] + i) * nb, sizeof(double) * nb);
+          o += nb;
+        }
+        hsb_stats st;
+        memset(&st, 0, sizeof(st));
+        rc = hsb_batch_run_subset(s->batch, chips.data(), (int)chips.size(), rows.data(), K, dt, &st);
+      }
+      std::vector<int> fin;
+      for (int k : grp) {
+        const bool last = prog[k] + K >= reqs[k].steps;
+        if (rc == HSB_OK && last) {
+          const int r2 = read_temps(s->models[served_by[k]].m, reqs[k].out);
+          reqs[k].status = r2;
+          fin.push_back(k);
+        } else if (rc != HSB_OK) {
+          if (std::find(failed.begin(), failed.end(), k) == failed.end()) reqs[k].status = rc;
+          fin.push_back(k);
+        }
+      }
+      lk.lock();
+      if (rc == HSB_OK) {
+        s->ticks++;
+        s->tick_requests += (long long)grp.size();
+        s->tick_intervals += (long long)grp.size() * K;
+      }
+      for (int k : grp) prog[k] += K;
+      if (rc != HSB_OK && first_error.empty()) first_error = hsb_dev_last_error();
+      for (int k : fin) {
+        hsb_request &r = reqs[k];
+        r.finish = now();
+        if (r.status != HSB_OK && first_error.empty()) first_error = hsb_dev_last_error();
+        hsb_server::Model &M = s->models[served_by[k]];
+        if (r.status == HSB_OK) M.warm = true;
+        M.busy = false;
+        state[k] = 2;
+        running--;
+        done++;
+        eng_done++;
+        act.erase(std::find(act.begin(), act.end(), k));
+      }
+      // a request that failed while loading its temperatures, outside the tick's group
+      for (int k : failed)
+        if (state[k] == 1) {
+          reqs[k].finish = now();
+          s->models[served_by[k]].busy = false;
+          state[k] = 2;
+          running--;
+          done++;
+          eng_done++;
+          act.erase(std::find(act.begin(), act.end(), k));
+        }
+      engine_on = act.empty() ? 0 : 1;
+      cv.notify_all();
+    }
+  };
   std::vector<std::thread> pool;
   const int threads = s->workers + (any_high ? HIGH_SLOTS : 0);
   for (int w = 0; w < threads; w++) pool.emplace_back(worker, w);
+  if (n_engine) pool.emplace_back(engine);
   for (auto &th : pool) th.join();
   int failed = 0;
   for (int k = 0; k < n; k++)

@@ -924,7 +924,8 @@ static int bc_setup(hsb_dev_model *m, BcWork **out) {
       cudaMallocHost(&w->h_red, sizeof(double) * 16) != cudaSuccess)
     return fail(set_error(HSB_E_NOMEM, "BiCGStab reductions"));
   w->status = (int *)(w->red + RED_STATUS);
-  if (cudaMemset(w->status, 0, sizeof(int)) != cudaSuccess) return fail(set_error(HSB_E_CUDA, "BiCGStab status"));
+  if (cudaMemsetAsync(w->status, 0, sizeof(int), m->stream) != cudaSuccess)
+    return fail(set_error(HSB_E_CUDA, "BiCGStab status"));
   // plane solve: chunks of R rows, as many planes per CTA as fit ~200 KB
   w->R = m->nr % 16 == 0 ? 16 : m->nr % 8 == 0 ? 8 : m->nr % 4 == 0 ? 4 : m->nr % 2 == 0 ? 2 : 1;
   const size_t per = bc_solve_smem(nl, w->R, 1);
@@ -1010,7 +1011,7 @@ static int bc_build(hsb_dev_model *m, BcWork *w) {
     float inv32[BNX * BNX];
     for (int a = 0; a < BNX; a++)
       for (int b = 0; b < BNX; b++) inv32[a * BNX + b] = (float)M[a][BNX + b];
-    HSB_CUDA(cudaMemcpy(w->lv[k].pinv, inv32, sizeof(inv32), cudaMemcpyHostToDevice));
+    HSB_CUDA(h2d_on(w->lv[k].pinv, inv32, sizeof(inv32), m->stream));
   }
   // the edge conductances go to the device with the FP64 build (scratch in r64)
   double ge[2 * BC_MAX_NL];

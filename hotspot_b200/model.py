@@ -207,6 +207,14 @@ class RCModel:
         if lib().hsb_dev_set_tile(lib().hsb_grid_device(self.ptr), int(rows), int(cols)) != 0:
             raise _abi.HotspotError(lib().hsb_dev_last_error().decode(errors="replace").strip())
 
+    def transient_kernel(self) -> str:
+        """The kernel the fast transient runs for this model: "blocked",
+        "blocked_fp64", "passes", or "" before its first fast interval."""
+        k = C.c_int()
+        if lib().hsb_dev_transient_kernel(lib().hsb_grid_device(self.ptr), C.byref(k)) != 0:
+            raise _abi.HotspotError(lib().hsb_dev_last_error().decode(errors="replace").strip())
+        return {0: "", 1: "blocked", 2: "blocked_fp64", 3: "passes"}[k.value]
+
     def stats(self) -> dict:
         s = _abi.Stats()
         check(lib().hsb_grid_get_stats(self.ptr, C.byref(s)))

@@ -45,6 +45,7 @@ class Request:
     start: float = 0.0
     finish: float = 0.0
     status: int = 0
+    worker: int = 0                   # written by the server; -1: the batch engine
 
     @property
     def latency(self) -> float:
@@ -81,6 +82,20 @@ class Server:
         """Dispatch this model's requests first and run them on a high-priority stream."""
         _check(lib().hsb_server_set_priority(self.ptr, int(model), int(bool(high))))
 
+    def set_batching(self, on: bool = True):
+        """Serve the transients of fast-form models through the continuous batch
+        engine: one launch per tick advances every admitted transient of one
+        interval length; requests join and leave between ticks."""
+        _check(lib().hsb_server_set_batching(self.ptr, int(bool(on))))
+
+    def batch_stats(self) -> dict:
+        """Engine counters: ticks (launches), mean requests advanced per tick,
+        request-intervals advanced."""
+        t, rt, ri = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        _check(lib().hsb_server_batch_stats(self.ptr, C.byref(t), C.byref(rt), C.byref(ri)))
+        return {"ticks": t.value, "requests_per_tick": rt.value / t.value if t.value else 0.0,
+                "request_intervals": ri.value}
+
     def run(self, requests: list[Request]):
         n = len(requests)
         arr = (_abi.Request * n)()
@@ -102,6 +117,7 @@ class Server:
         rc = lib().hsb_server_run(self.ptr, arr, n)
         for k, r in enumerate(requests):
             r.start, r.finish, r.status = arr[k].start, arr[k].finish, arr[k].status
+            r.worker = arr[k].worker       # -1: served by the batch engine
         _check(rc)
         return requests
 

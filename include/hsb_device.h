@@ -45,6 +45,9 @@ extern "C" {
 #define HSB_FORM_FP64_BLOCKED 4 /* transient: the temporally blocked Krylov form with every
                                    stencil pass in FP64 (per-layer models of 3..12 layers),
                                    within 1e-6 K of the FP64 replay; steady as HSB_FORM_PARITY */
+#define HSB_FORM_FAST_BLOCKED 5 /* the fast transient on the temporally blocked kernel
+                                   whatever the model's size (HSB_FORM_FAST takes it from
+                                   2^21 cells up, the pass-by-pass kernel below) */
 
 /* steady methods */
 #define HSB_STEADY_AUTO       0  /* GS replay for FORM_PARITY; MG-PCG (or BiCGStab with advection) for FORM_FAST */
@@ -202,8 +205,8 @@ int  hsb_batch_chip_steps(hsb_batch *b, long long *steps);
  * work keeps SMs while a batch runs */
 int  hsb_batch_set_ctas(hsb_batch *b, int ctas);
 /* one launch advancing only the listed models (n indices) by K intervals;
- * block_powers has hsb_batch_transient_trace's layout, only the listed
- * models' segments are read; blocks until done */
+ * block_powers: K rows, each the listed models' block vectors one after
+ * another in list order; blocks until done */
 int  hsb_batch_run_subset(hsb_batch *b, const int *chips, int n, const double *block_powers, int K,
                           double time_elapsed, hsb_stats *st);
 /* where each model's block powers sit in a row: off[c] .. off[c + 1] (n + 1 entries) */
@@ -262,6 +265,17 @@ int  hsb_server_run(hsb_server *s, hsb_request *reqs, int n);
 /* priority class of a registered model: its requests are dispatched before
  * normal ones and its kernels run on a high-priority stream (high = 1) */
 int  hsb_server_set_priority(hsb_server *s, int model, int high);
+/* continuous batching (on = 1): transient requests of normal-priority
+ * fast-form models that the temporally blocked kernel takes are served by a
+ * batch engine -- one launch advances every admitted transient of one
+ * interval length by a few intervals (a tick); requests join and leave the
+ * batch between ticks.  The batch is built at the next hsb_server_run over
+ * the models registered then. */
+int  hsb_server_set_batching(hsb_server *s, int on);
+/* engine counters since the server was created: ticks (launches), the sum
+ * over ticks of the requests each advanced, and of requests x intervals */
+int  hsb_server_batch_stats(hsb_server *s, long long *ticks, long long *request_ticks,
+                            long long *request_intervals);
 
 /* run the model's work on a high-priority (high = 1) or normal stream; call
  * with no work of the model in flight */
@@ -282,6 +296,13 @@ int hsb_dev_set_tile(hsb_dev_model *m, int rows, int cols);
 #define HSB_WS_MG             2
 #define HSB_WS_BICGSTAB       4
 int hsb_dev_workspaces(const hsb_dev_model *m, int *mask);
+
+/* the kernel the fast transient form runs for this model (set at its first
+ * fast interval): 0 none yet, or HSB_TK_* */
+#define HSB_TK_BLOCKED      1   /* temporally blocked, FP32 passes */
+#define HSB_TK_BLOCKED_FP64 2   /* temporally blocked, FP64 passes */
+#define HSB_TK_PASSES       3   /* one grid-wide pass per Krylov vector */
+int hsb_dev_transient_kernel(const hsb_dev_model *m, int *kind);
 
 /* which: 0 = transient state (last_trans), 1 = steady state (last_steady);
  * n = nl*nr*nc + n_extra doubles */

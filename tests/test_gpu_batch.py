@@ -8,7 +8,7 @@ intervals run one per call or K per launch."""
 import numpy as np
 import pytest
 
-from hotspot_b200 import FORM_FAST
+from hotspot_b200 import FORM_FAST_BLOCKED
 from hotspot_b200 import model as hm
 from hotspot_b200 import workloads as W
 from hotspot_b200.batch import Batch
@@ -39,7 +39,7 @@ def _models(scs):
     for sc in scs:
         for lst in (single, batched):
             m = hm.from_scenario(sc)
-            m.set_solver(FORM_FAST)
+            m.set_solver(FORM_FAST_BLOCKED)
             t = m.vector(m.config.init_temp)
             m.compute_temp(m.power_vector(sc.block_power[0]), t, 0.0)
             lst.append(m)
@@ -125,4 +125,38 @@ def test_batch_autotuner(workdir):
     assert len(tun) == 9 and all(t["ms_per_gcell_step"] > 0 for t in tun)
     best = min(tun, key=lambda t: t["ms_per_gcell_step"])
     assert info["policy"] == best["policy"] and info["split"] == best["split"]
+    assert max(errs) <= TOL, errs
+
+
+def test_batch_subset_launches(workdir):
+    """Launches over a subset of the models, a few intervals each (the ticks of
+    the serving batch engine): the listed chips match the single-model form
+    on the same tiles (same steps, 1e-9 K) and the others keep their state
+    bit for bit."""
+    scs = _chips(workdir, [("stack3d", 128), ("chip2d", 32), ("random", 64), ("chip2d", 64), ("secondary", 32)])
+    single, batched = _models(scs)
+    bt = Batch(batched)
+    bt.set_ctas(40)                    # fewer CTAs than the device holds: groups shrink
+    for c, a in enumerate(single):
+        a.set_tile(*bt.tile(c))
+    done = [0] * len(scs)
+    for chips, K in [([2, 0], 3), ([1, 3, 4], 2), ([4, 0, 2, 1, 3], 1), ([3], 2)]:
+        before = {c: batched[c].grid("trans") for c in range(len(scs)) if c not in chips}
+        rows = [[batched[c].power_vector(scs[c].block_power[1 + done[c] + j]) for c in chips] for j in range(K)]
+        st = bt.run_subset(chips, rows, scs[0].dt)
+        assert st["launches"] == 1
+        steps = bt.chip_steps()
+        for c in chips:
+            s1 = 0
+            for j in range(K):
+                single[c].compute_temp(single[c].power_vector(scs[c].block_power[1 + done[c] + j]), None, scs[c].dt)
+                s1 += single[c].stats()["rk4_steps"]
+            assert steps[c] == s1, (c, steps[c], s1)
+            done[c] += K
+        for c, g in before.items():
+            assert np.array_equal(batched[c].grid("trans"), g), c
+    errs = [float(np.max(np.abs(a.grid("trans") - b.grid("trans")))) for a, b in zip(single, batched)]
+    bt.close()
+    for m in single + batched:
+        m.close()
     assert max(errs) <= TOL, errs

@@ -125,3 +125,64 @@ def test_pool_members_serve_one_class(workdir):
     srv.close()
     for mm in members:
         mm.close()
+
+
+def test_batched_transients_join_and_leave(workdir):
+    """Continuous batching: transients of several classes and pool members,
+    two interval lengths, arriving over time, advanced by the batch engine a
+    tick at a time while steady requests run on the workers.  Each result
+    equals the same request served alone (through the engine, bit for bit:
+    a chip's result does not depend on its batch mates, its CTAs or its
+    launch boundaries); requests shared ticks; a transient's result stays
+    within 0.01 K of the oracle's FP64 replay."""
+    rng = np.random.default_rng(95)
+    scs = [W.scenario_random_chip(workdir, rng, "ta", side=64, chip_layers=2, steps=0),
+           W.scenario_random_chip(workdir, rng, "tb", side=128, chip_layers=3, steps=0),
+           W.scenario_random_chip(workdir, rng, "tc", side=32, chip_layers=5, steps=0),
+           W.scenario_random_chip(workdir, rng, "sd", side=128, chip_layers=2, steps=0)]
+    models = [hm.from_scenario(sc) for sc in scs]
+    srv = Server(workers=3)
+    idx = [srv.add_model(m, _abi.FORM_FAST, 1e-6) for m in models]
+    reps = [hm.from_scenario(scs[0]) for _ in range(2)]
+    for r in reps:
+        srv.add_replica(idx[0], r)
+    srv.set_batching(True)
+    r2 = np.random.default_rng(96)
+    reqs, t = [], 0.0
+    for k in range(18):
+        t += r2.exponential(1.0 / 3000.0)
+        mi = 2 if k == 0 else int(r2.integers(0, 4))
+        m = models[mi]
+        nblk = sum(m.layer_units[l] for l in range(m.n_layers) if m.layer_power[l])
+        if mi == 3:
+            reqs.append(Request(mi, _abi.REQ_STEADY, m.power_vector(r2.uniform(0.5, 20.0, nblk)), t, tag="s"))
+            continue
+        steps = int(r2.integers(5, 60))
+        dt = 3.333e-6 if k % 3 else 1e-5
+        trace = W.ar1_power(r2, r2.uniform(0.5, 20.0, nblk), steps)
+        p = np.stack([m.power_vector(trace[s]) for s in range(steps)])
+        reqs.append(Request(mi, _abi.REQ_TRANSIENT, p, t, temp_in=m.vector(m.config.init_temp), steps=steps, dt=dt,
+                            tag=f"t{mi}"))
+    alone = [Request(r.model, r.kind, r.power, 0.0, r.temp_in, r.steps, r.dt, r.tag) for r in reqs]
+    for r in alone:
+        srv.run([r])
+    st0 = srv.batch_stats()
+    srv.run(reqs)
+    st1 = srv.batch_stats()
+    for a, b in zip(alone, reqs):
+        assert a.status == 0 and b.status == 0
+        assert np.array_equal(a.out, b.out), (a.tag, np.max(np.abs(a.out - b.out)))
+        assert (b.worker == -1) == (b.kind == _abi.REQ_TRANSIENT), (b.tag, b.worker)
+    ticks = st1["ticks"] - st0["ticks"]
+    shared = (st1["requests_per_tick"] * st1["ticks"] - st0["requests_per_tick"] * st0["ticks"]) / ticks
+    assert shared > 1.0, shared            # mean requests advanced per tick in the mixed run
+    # one transient against the oracle's FP64 replay of the reference
+    r = next(r for r in reqs if r.kind == _abi.REQ_TRANSIENT and r.model == 2)
+    o = OracleModel(scs[2])
+    to = np.array(r.temp_in, dtype=np.float64)
+    for k in range(r.steps):
+        o.compute_temp(r.power[k].copy(), to if k == 0 else None, r.dt)
+    assert np.max(np.abs(r.out - to)) <= 0.01
+    srv.close()
+    for m in models + reps:
+        m.close()

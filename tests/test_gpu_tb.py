@@ -1,5 +1,5 @@
-"""The temporally blocked fast transient (the default kernel of HSB_FORM_FAST
-for models with per-layer conductances) against
+"""The temporally blocked fast transient (HSB_FORM_FAST_BLOCKED; the kernel of
+HSB_FORM_FAST for models of 2^21 cells and more) against
 
 * the same arithmetic run one grid-wide pass per Krylov vector
   (HSB_FORM_FAST_PASSES): the same accepted steps and attempts, block and
@@ -24,7 +24,7 @@ import contextlib
 import numpy as np
 import pytest
 
-from hotspot_b200 import FORM_FAST, FORM_FAST_PASSES, FORM_FP64_BLOCKED, FORM_PARITY
+from hotspot_b200 import FORM_FAST_BLOCKED, FORM_FAST_PASSES, FORM_FP64_BLOCKED, FORM_PARITY
 from hotspot_b200 import model as hm
 from hotspot_b200 import workloads as W
 from oracle.restatement import OracleModel, x87_rounding
@@ -91,7 +91,7 @@ CASES = ["chip2d16", "chip2d64", "rect32x64", "rect128x32", "secondary", "stack6
 def test_blocked_matches_pass_by_pass(workdir, case):
     sc = _scenario(workdir, case)
     rows = min(sc.steps, sc.block_power.shape[0])
-    ta, ga, sa, aa, fa = _run(sc, FORM_FAST, rows)
+    ta, ga, sa, aa, fa = _run(sc, FORM_FAST_BLOCKED, rows)
     tb, gb, sb, ab, fb = _run(sc, FORM_FAST_PASSES, rows)
     assert fa == 0 and fb == 0, "a retry outgrew the kernel"
     if case.startswith("long"):
@@ -116,7 +116,7 @@ def test_blocked_against_fp64_replay(workdir, case):
     path, by the reference's golden vectors)."""
     sc = _scenario(workdir, case)
     rows = min(sc.steps, sc.block_power.shape[0], 4)
-    ta, ga, *_ = _run(sc, FORM_FAST, rows)
+    ta, ga, *_ = _run(sc, FORM_FAST_BLOCKED, rows)
     tr, gr, *_ = _run(sc, FORM_PARITY, rows)
     assert np.max(np.abs(ta - tr)) <= TOL_FP64
     assert np.max(np.abs(ga - gr)) <= TOL_FP64
@@ -126,7 +126,7 @@ def test_blocked_against_fp64_oracle(workdir):
     """The same against the oracle's restatement on the CPU (primary path)."""
     sc = _scenario(workdir, "stack64")
     rows = 4
-    ta, ga, *_ = _run(sc, FORM_FAST, rows)
+    ta, ga, *_ = _run(sc, FORM_FAST_BLOCKED, rows)
     o = OracleModel(sc)
     to = o.vector(o.init_temp)
     for k in range(rows):
@@ -174,3 +174,27 @@ def test_fp64_blocked_matches_replay(workdir, case):
         tol = max(tol, 4.0 * _rounding_spread(sc, rows))
     assert np.max(np.abs(ta - tb)) <= tol, tol
     assert np.max(np.abs(ga - gb)) <= tol, tol
+
+
+def test_fast_form_picks_kernel_by_size(workdir):
+    """HSB_FORM_FAST runs the pass-by-pass kernel below 2^21 cells and the
+    blocked kernel from there up; there its result is the explicit blocked
+    form's, bit for bit."""
+    from hotspot_b200 import FORM_FAST
+    small = W.scenario_chip2d(workdir, seed=97, grid=64, steps=2)
+    m = hm.from_scenario(small)
+    m.set_solver(FORM_FAST)
+    m.compute_temp(m.power_vector(small.block_power[0]), m.vector(m.config.init_temp), small.dt)
+    assert m.transient_kernel() == "passes"
+    m.close()
+    big = W.scenario_random_chip(workdir, np.random.default_rng(98), "big", side=512, chip_layers=6, steps=2)
+    grids = []
+    for form in (FORM_FAST, FORM_FAST_BLOCKED):
+        m = hm.from_scenario(big)
+        assert m.n_cells >= 1 << 21
+        m.set_solver(form)
+        m.compute_temp(m.power_vector(big.block_power[0]), m.vector(m.config.init_temp), big.dt)
+        assert m.transient_kernel() == "blocked"
+        grids.append(m.grid("trans"))
+        m.close()
+    assert np.array_equal(grids[0], grids[1])
