@@ -210,6 +210,7 @@ _SIGS = {
     "hsb_grid_populate_C": (C.c_int, [_GM, C.POINTER(Flp)]),
     "hsb_grid_compute_temp": (C.c_int, [_GM, _D, _D, C.c_double]),
     "hsb_grid_steady": (C.c_int, [_GM, _D, _D]),
+    "hsb_grid_steady_leakage": (C.c_int, [_GM, _D, _D, C.POINTER(C.c_int)]),
     "hsb_grid_device": (C.c_void_p, [_GM]),
     "hsb_read_flp": (C.POINTER(Flp), [C.c_char_p]),
     "hsb_free_flp_public": (None, [C.POINTER(Flp)]),
@@ -231,6 +232,7 @@ _SIGS = {
     "hsb_dev_get_state": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "hsb_dev_workspaces": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "hsb_dev_transient_kernel": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "hsb_dev_steady_leakage": (C.c_int, [C.c_void_p, _D, _D, _D, _D, C.c_void_p, C.POINTER(C.c_int), C.c_void_p]),
     "hsb_dev_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "hsb_dev_set_state": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "hsb_abi_sizes": (C.c_int, [C.POINTER(C.c_longlong), C.c_int]),

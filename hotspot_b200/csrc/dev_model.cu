@@ -700,25 +700,18 @@ int hsb_dev_transient_trace(hsb_dev_model *m, const double *block_powers, int K,
   return HSB_OK;
 }
 
-int hsb_dev_steady(hsb_dev_model *m, const double *block_power, double *block_temp_out,
-                   const hsb_solver_opts *o, hsb_stats *st) {
-  if (!m || !block_power) return set_error(HSB_E_ARG, "null argument");
-  if (!m->b2g_ptr) return set_error(HSB_E_ARG, "block-grid maps not set");
-  const size_t nb = (size_t)m->total_n_blocks + m->nx;
-  hsb_stats local;
-  if (!st) st = &local;
-  hsb_solver_opts def = {HSB_FORM_PARITY, HSB_STEADY_AUTO, 0.0, 0};
-  if (!o) o = &def;
-  cudaEventRecord(m->ev[0], m->stream);
+}  // extern "C"
+
+// the steady solve from the block powers in m->blk_in (device) to the grid
+// state m->ys and the block temperatures in m->blk_out (device)
+int hsb::steady_core(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
   int rc;
-  HSB_CUDA(cudaMemcpyAsync(m->blk_in, block_power, sizeof(double) * nb, cudaMemcpyHostToDevice,
-                           m->stream));
   if ((rc = b2g(m, m->blk_in, m->pgrid, HSB_V_POWER))) return rc;
   st->launches += 1;
   int method = o->steady_method;
   if (method == HSB_STEADY_AUTO) {
     if (m->uchan_mask) method = HSB_STEADY_BICGSTAB;
-    else if (o->form != HSB_FORM_PARITY && o->form != HSB_FORM_FP64_BLOCKED && m->nx == HSB_EXTRA)
+    else if (o->form != HSB_FORM_PARITY && o->form != HSB_FORM_FP64_BLOCKED)
       method = HSB_STEADY_MG;
     else method = HSB_STEADY_GS_REPLAY;
   }
@@ -732,12 +725,30 @@ int hsb_dev_steady(hsb_dev_model *m, const double *block_power, double *block_te
     default: rc = set_error(HSB_E_ARG, "unknown steady method");
   }
   if (rc) return rc;
-  if (block_temp_out) {
-    if ((rc = g2b(m, m->ys, m->blk_out))) return rc;
-    st->launches += 1;
+  if ((rc = g2b(m, m->ys, m->blk_out))) return rc;
+  st->launches += 1;
+  return HSB_OK;
+}
+
+extern "C" {
+
+int hsb_dev_steady(hsb_dev_model *m, const double *block_power, double *block_temp_out,
+                   const hsb_solver_opts *o, hsb_stats *st) {
+  if (!m || !block_power) return set_error(HSB_E_ARG, "null argument");
+  if (!m->b2g_ptr) return set_error(HSB_E_ARG, "block-grid maps not set");
+  const size_t nb = (size_t)m->total_n_blocks + m->nx;
+  hsb_stats local;
+  if (!st) st = &local;
+  hsb_solver_opts def = {HSB_FORM_PARITY, HSB_STEADY_AUTO, 0.0, 0};
+  if (!o) o = &def;
+  cudaEventRecord(m->ev[0], m->stream);
+  int rc;
+  HSB_CUDA(cudaMemcpyAsync(m->blk_in, block_power, sizeof(double) * nb, cudaMemcpyHostToDevice,
+                           m->stream));
+  if ((rc = steady_core(m, o, st))) return rc;
+  if (block_temp_out)
     HSB_CUDA(cudaMemcpyAsync(block_temp_out, m->blk_out, sizeof(double) * nb,
                              cudaMemcpyDeviceToHost, m->stream));
-  }
   cudaEventRecord(m->ev[1], m->stream);
   HSB_CUDA(cudaStreamSynchronize(m->stream));
   float ms = 0;

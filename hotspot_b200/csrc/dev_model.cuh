@@ -155,6 +155,9 @@ inline cudaError_t h2d_on(void *dst, const void *src, size_t bytes, cudaStream_t
   return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
 }
 int b2g(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type);
+// the steady solve from the block powers in m->blk_in to m->ys and the block
+// temperatures in m->blk_out, all on the device
+int steady_core(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st);
 int g2b(hsb_dev_model *m, const double *grid_dev, double *blk_dev);
 // the same on a given stream
 int b2g_on(hsb_dev_model *m, const double *blk_dev, double *grid_dev, int type, cudaStream_t s);

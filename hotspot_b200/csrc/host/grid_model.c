@@ -988,6 +988,34 @@ int hsb_grid_steady(grid_model_t *m, double *power, double *temp)
   return HSB_OK;
 }
 
+int hsb_grid_steady_leakage(grid_model_t *m, double *power, double *temp, int *iterations)
+{
+  int k, j, base, rc;
+  double *dims;
+  if (!m->r_ready) return hsb_seterr(HSB_E_ARG, "R model not ready\n");
+  if (m->config.leakage_mode)
+    return hsb_seterr(HSB_E_ARG, "HotLeakage currently is not implemented in this release of HotSpot\n");
+  /* the power blocks' heights and widths (0: a block of a layer without power) */
+  dims = calloc(2 * (size_t)m->total_n_blocks, sizeof(double));
+  if (!dims) return hsb_seterr(HSB_E_NOMEM, "memory allocation error\n");
+  for (k = 0, base = 0; k < m->n_layers; k++) {
+    if (m->layers[k].has_power)
+      for (j = 0; j < m->layers[k].flp->n_units; j++) {
+        dims[base + j] = m->layers[k].flp->units[j].height;
+        dims[m->total_n_blocks + base + j] = m->layers[k].flp->units[j].width;
+      }
+    base += m->layers[k].flp->n_units;
+  }
+  zero_internal_power(m, power);
+  memset(&m->ext->last, 0, sizeof(hsb_stats));
+  rc = hsb_dev_steady_leakage(m->dev, power, dims, dims + m->total_n_blocks, temp, &m->ext->opts, iterations,
+                              &m->ext->last);
+  free(dims);
+  if (rc) return hsb_seterr(rc, "%s\n", hsb_dev_last_error());
+  m->ext->host_steady_valid = 0;
+  return HSB_OK;
+}
+
 /* ------------------------------------------------------------------------ */
 /* exported: temperature_grid.h interface                                    */
 /* ------------------------------------------------------------------------ */

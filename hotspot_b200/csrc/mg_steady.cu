@@ -29,7 +29,7 @@
 namespace hsb {
 
 #define MGT 256
-#define NXP 12
+#define NXP (HSB_EXTRA + HSB_EXTRA_SEC)   // package nodes of either path; the primary path's unused ones are inert
 #ifndef MG_SWEEPS
 #define MG_SWEEPS 1  // smoothing sweeps before and after each coarse-grid correction
 #endif
@@ -54,9 +54,9 @@ struct MgLevelDev {
   const float *diag;
   const float *gAmbL;          // per layer ambient conductance per cell
   const float *gEdgeNS, *gEdgeEW;  // per layer edge conductance per cell
-  int spidx, hsidx;
+  int el[5];                   // layers of the edge groups: sink, spreader, PCB, solder, substrate (-1 absent)
   float scale;                 // 2^level: edge conductances per coarse cell
-  const float *pinv;           // 12 x 12 inverse of the package block
+  const float *pinv;           // NXP x NXP inverse of the package block
 };
 
 struct MgLevel {
@@ -64,7 +64,7 @@ struct MgLevel {
   long long plane, ncell, n;
   float *gE, *gS, *gB, *diag, *gAmbL, *gEdgeNS, *gEdgeEW;
   float *x, *f, *r;
-  float *pinv;                 // 12 x 12 inverse of the package block at this level
+  float *pinv;                 // NXP x NXP inverse of the package block at this level
 };
 
 struct MgWork {
@@ -102,11 +102,16 @@ struct MgWork {
 // ---------------------------------------------------------------------------
 // operator application helpers
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int edge_node(int layer, int side, int spidx, int hsidx) {
-  // side 0 N, 1 S, 2 W, 3 E
-  if (layer == hsidx) return side == 0 ? HSB_SINK_C_N : side == 1 ? HSB_SINK_C_S : side == 2 ? HSB_SINK_C_W : HSB_SINK_C_E;
-  if (layer == spidx) return side == 0 ? HSB_SP_N : side == 1 ? HSB_SP_S : side == 2 ? HSB_SP_W : HSB_SP_E;
+// the package node an edge of a layer couples to (side 0 N, 1 S, 2 W, 3 E):
+// each edge group's nodes are numbered W, E, N, S from its W node
+__host__ __device__ __forceinline__ int edge_node(int layer, int side, const int *el) {
+  const int wnode[5] = {HSB_SINK_C_W, HSB_SP_W, HSB_PCB_C_W, HSB_SOLDER_W, HSB_SUB_W};
+  for (int g = 0; g < 5; g++)
+    if (layer == el[g]) return wnode[g] + ((side + 2) & 3);
   return -1;
+}
+__host__ __device__ __forceinline__ bool edge_layer(int layer, const int *el) {
+  return layer == el[0] || layer == el[1] || layer == el[2] || layer == el[3] || layer == el[4];
 }
 
 // y = A x on level L (cells; the package rows by apply_pack_rows),
@@ -140,11 +145,11 @@ __global__ void mg_apply_cells(MgLevelDev L, const float *__restrict__ x, float 
   if (n < L.nl - 1) s += L.gB[c] * (xc - x[c + L.plane]);
   if (n > 0) s += L.gB[c - L.plane] * (xc - x[c - L.plane]);
   const float *xp = x + L.ncell;
-  if (n == L.spidx || n == L.hsidx) {
-    if (i == 0) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 0, L.spidx, L.hsidx)]);
-    if (i == L.nr - 1) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 1, L.spidx, L.hsidx)]);
-    if (j == 0) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 2, L.spidx, L.hsidx)]);
-    if (j == L.nc - 1) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 3, L.spidx, L.hsidx)]);
+  if (edge_layer(n, L.el)) {
+    if (i == 0) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 0, L.el)]);
+    if (i == L.nr - 1) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 1, L.el)]);
+    if (j == 0) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 2, L.el)]);
+    if (j == L.nc - 1) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 3, L.el)]);
   }
   y[c] = mode ? f[c] - s : s;
 }
@@ -195,11 +200,11 @@ __device__ __forceinline__ void zline_col(const MgLevelDev &L, float *__restrict
     if (j > 0) rhs += L.gE[c - 1] * x[c - 1];
     if (i < L.nr - 1) rhs += L.gS[c] * x[c + L.nc];
     if (i > 0) rhs += L.gS[c - L.nc] * x[c - L.nc];
-    if (n == L.spidx || n == L.hsidx) {
-      if (i == 0) rhs += L.gEdgeNS[n] * xp[edge_node(n, 0, L.spidx, L.hsidx)];
-      if (i == L.nr - 1) rhs += L.gEdgeNS[n] * xp[edge_node(n, 1, L.spidx, L.hsidx)];
-      if (j == 0) rhs += L.gEdgeEW[n] * xp[edge_node(n, 2, L.spidx, L.hsidx)];
-      if (j == L.nc - 1) rhs += L.gEdgeEW[n] * xp[edge_node(n, 3, L.spidx, L.hsidx)];
+    if (edge_layer(n, L.el)) {
+      if (i == 0) rhs += L.gEdgeNS[n] * xp[edge_node(n, 0, L.el)];
+      if (i == L.nr - 1) rhs += L.gEdgeNS[n] * xp[edge_node(n, 1, L.el)];
+      if (j == 0) rhs += L.gEdgeEW[n] * xp[edge_node(n, 2, L.el)];
+      if (j == L.nc - 1) rhs += L.gEdgeEW[n] * xp[edge_node(n, 3, L.el)];
     }
     const float a = n > 0 ? -L.gB[c - L.plane] : 0.f;   // sub-diagonal
     const float cc = n < nl - 1 ? -L.gB[c] : 0.f;        // super-diagonal
@@ -252,11 +257,11 @@ __device__ __forceinline__ void zline_colT(const MgLevelDev &L, float *x, const 
         r += wS * x[c + dS];
         r += wN * x[c - dN];
       }
-      if (!ZERO && (n == L.spidx || n == L.hsidx)) {
-        if (i == 0) r += L.gEdgeNS[n] * xp[edge_node(n, 0, L.spidx, L.hsidx)];
-        if (i == nr - 1) r += L.gEdgeNS[n] * xp[edge_node(n, 1, L.spidx, L.hsidx)];
-        if (j == 0) r += L.gEdgeEW[n] * xp[edge_node(n, 2, L.spidx, L.hsidx)];
-        if (j == nc - 1) r += L.gEdgeEW[n] * xp[edge_node(n, 3, L.spidx, L.hsidx)];
+      if (!ZERO && edge_layer(n, L.el)) {
+        if (i == 0) r += L.gEdgeNS[n] * xp[edge_node(n, 0, L.el)];
+        if (i == nr - 1) r += L.gEdgeNS[n] * xp[edge_node(n, 1, L.el)];
+        if (j == 0) r += L.gEdgeEW[n] * xp[edge_node(n, 2, L.el)];
+        if (j == nc - 1) r += L.gEdgeEW[n] * xp[edge_node(n, 3, L.el)];
       }
       rhs[n] = r;
       gb[n] = n < nl - 1 ? L.gB[c] : 0.f;
@@ -611,11 +616,11 @@ __device__ __noinline__ void fz_resid(const MgLevelDev &L, const PackSys *ps, co
     if (i > 0) s += L.gS[c - L.nc] * (xc - x[c - L.nc]);
     if (n < L.nl - 1) s += L.gB[c] * (xc - x[c + L.plane]);
     if (n > 0) s += L.gB[c - L.plane] * (xc - x[c - L.plane]);
-    if (n == L.spidx || n == L.hsidx) {
-      if (i == 0) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 0, L.spidx, L.hsidx)]);
-      if (i == L.nr - 1) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 1, L.spidx, L.hsidx)]);
-      if (j == 0) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 2, L.spidx, L.hsidx)]);
-      if (j == L.nc - 1) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 3, L.spidx, L.hsidx)]);
+    if (edge_layer(n, L.el)) {
+      if (i == 0) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 0, L.el)]);
+      if (i == L.nr - 1) s += L.gEdgeNS[n] * (xc - xp[edge_node(n, 1, L.el)]);
+      if (j == 0) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 2, L.el)]);
+      if (j == L.nc - 1) s += L.gEdgeEW[n] * (xc - xp[edge_node(n, 3, L.el)]);
     }
     r[c] = f[c] - s;
   }
@@ -820,7 +825,7 @@ __global__ void mg_diag(MgLevelDev L, float *__restrict__ diag) {
   if (i > 0) d += L.gS[c - L.nc];
   if (n < L.nl - 1) d += L.gB[c];
   if (n > 0) d += L.gB[c - L.plane];
-  if (n == L.spidx || n == L.hsidx) {
+  if (edge_layer(n, L.el)) {
     if (i == 0) d += L.gEdgeNS[n];
     if (i == L.nr - 1) d += L.gEdgeNS[n];
     if (j == 0) d += L.gEdgeEW[n];
@@ -889,12 +894,15 @@ __global__ void pack_residual64(const hsb::StencilArgs S, const PackSys *__restr
     if (lane == 0) esum[k] = s;
   }
   __syncthreads();
-  if (threadIdx.x < NXP) {
+  if (threadIdx.x < NXP) {   // the model's nodes; the state has no entries for inert ones (residual 0)
     const int k = threadIdx.x;
-    const double *x = T + S.ncell;
-    double s = ge64[k] * esum[k] + gamb64[k] * x[k];
-    for (int o = 0; o < NXP; o++) s += link64[k * NXP + o] * (x[k] - x[o]);
-    const double res = b[S.ncell + k] - s;
+    double res = 0.0;
+    if (k < S.nx) {
+      const double *x = T + S.ncell;
+      double s = ge64[k] * esum[k] + gamb64[k] * x[k];
+      for (int o = 0; o < S.nx; o++) s += link64[k * NXP + o] * (x[k] - x[o]);
+      res = b[S.ncell + k] - s;
+    }
     r[S.ncell + k] = res;
     r32[S.ncell + k] = (float)res;
     atomicMax(maxbits, (unsigned long long)__double_as_longlong(fabs(res)));
@@ -1050,13 +1058,23 @@ __global__ void d2f(const double *__restrict__ a, float *__restrict__ b, long lo
 // ---------------------------------------------------------------------------
 static inline unsigned nb(long long n) { return (unsigned)((n + MGT - 1) / MGT); }
 
+// the layers of the edge groups (sink, spreader, PCB, solder, substrate), -1 absent
+static void edge_layers(const hsb_dev_model *m, int el[5]) {
+  for (int g = 0; g < 5; g++) el[g] = -1;
+  for (int n = 0; n < m->nl; n++) {
+    const int k = m->hostL0[n].kind;
+    const int g = k == LK_SINK ? 0 : k == LK_SPREADER ? 1 : k == LK_PCB ? 2 : k == LK_SOLDER ? 3 : k == LK_SUB ? 4 : -1;
+    if (g >= 0) el[g] = n;
+  }
+}
+
 static MgLevelDev dev_level(const hsb_dev_model *m, const MgLevel &L, int lvl) {
   MgLevelDev d;
   d.nr = L.nr; d.nc = L.nc; d.nl = m->nl;
   d.plane = L.plane; d.ncell = L.ncell;
   d.gE = L.gE; d.gS = L.gS; d.gB = L.gB; d.diag = L.diag;
   d.gAmbL = L.gAmbL; d.gEdgeNS = L.gEdgeNS; d.gEdgeEW = L.gEdgeEW;
-  d.spidx = m->spidx; d.hsidx = m->hsidx;
+  edge_layers(m, d.el);
   d.scale = (float)(1 << lvl);
   d.pinv = L.pinv;
   return d;
@@ -1158,24 +1176,37 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
   // FP64 fine faces
   if (m->field) field_faces64<<<nb(m->ncell), MGT, 0, m->stream>>>(S, w->gE64, w->gS64, w->gB64);
   else uniform_faces64<<<nb(m->ncell), MGT, 0, m->stream>>>(S, w->gE64, w->gS64, w->gB64);
-  // per-layer ambient and edge conductances (FP64 and per level FP32)
+  // per-layer ambient and edge conductances (FP64 and per level FP32): the
+  // sink's and, on the secondary path, the PCB's cells to ambient; the edge
+  // cells of every edge group's layer to its package nodes
   double gamb[HSB_MAX_LAYERS] = {0}, gens[HSB_MAX_LAYERS] = {0}, geew[HSB_MAX_LAYERS] = {0};
+  int el[5];
+  edge_layers(m, el);
   for (int n = 0; n < nl; n++) {
     const LayerCoef &c = m->hostL0[n];
-    if (c.kind == LK_SINK) gamb[n] = 1.0 / c.ramb;
-    if (c.kind == LK_SINK || c.kind == LK_SPREADER) {
+    if (c.ramb != 0.0) gamb[n] = 1.0 / c.ramb;
+    if (edge_layer(n, el)) {
       gens[n] = 1.0 / c.edgeNS;
       geew[n] = 1.0 / c.edgeEW;
     }
   }
-  // package system
+  // package system: the steady package equations of temperature_grid.c:
+  // 2123-2379 (primary nodes, and the secondary path's PCB, solder and
+  // substrate nodes), one row per node; nodes the model does not have are
+  // inert (unit diagonal, no coupling, zero right-hand side)
   PackSys ps;
   memset(&ps, 0, sizeof(ps));
   double link64[NXP * NXP] = {0}, gamb_p[NXP] = {0}, ge_p[NXP] = {0};
   for (int k = 0; k < NXP; k++) ps.elayer[k] = -1;
+  for (int k = m->nx; k < NXP; k++) gamb_p[k] = 1.0;
   auto link = [&](int a, int b, double r) {
     link64[a * NXP + b] += 1.0 / r;
     link64[b * NXP + a] += 1.0 / r;
+  };
+  auto edge = [&](int node, int layer, int side) {
+    ps.elayer[node] = layer;
+    ps.eside[node] = side;
+    ge_p[node] = side < 2 ? gens[layer] : geew[layer];
   };
   const int nodesC[4] = {HSB_SINK_C_N, HSB_SINK_C_S, HSB_SINK_C_W, HSB_SINK_C_E};
   const int nodesO[4] = {HSB_SINK_N, HSB_SINK_S, HSB_SINK_W, HSB_SINK_E};
@@ -1186,12 +1217,25 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
     link(nodesO[s], nodesC[s], (y ? pk.r_hs2_y : pk.r_hs2_x) + pk.r_hs);
     gamb_p[nodesC[s]] = 1.0 / (y ? pk.r_hs_c_per_y + pk.r_amb_c_per_y : pk.r_hs_c_per_x + pk.r_amb_c_per_x);
     link(nodesC[s], nodesS[s], y ? pk.r_sp_per_y : pk.r_sp_per_x);
-    ps.elayer[nodesC[s]] = m->hsidx;
-    ps.eside[nodesC[s]] = s;
-    ge_p[nodesC[s]] = y ? gens[m->hsidx] : geew[m->hsidx];
-    ps.elayer[nodesS[s]] = m->spidx;
-    ps.eside[nodesS[s]] = s;
-    ge_p[nodesS[s]] = y ? gens[m->spidx] : geew[m->spidx];
+    edge(nodesC[s], m->hsidx, s);
+    edge(nodesS[s], m->spidx, s);
+  }
+  if (m->nx > HSB_EXTRA) {   // temperature_grid.c:2228-2379
+    const int pO[4] = {HSB_PCB_N, HSB_PCB_S, HSB_PCB_W, HSB_PCB_E};
+    const int pC[4] = {HSB_PCB_C_N, HSB_PCB_C_S, HSB_PCB_C_W, HSB_PCB_C_E};
+    const int sO[4] = {HSB_SOLDER_N, HSB_SOLDER_S, HSB_SOLDER_W, HSB_SOLDER_E};
+    const int bO[4] = {HSB_SUB_N, HSB_SUB_S, HSB_SUB_W, HSB_SUB_E};
+    for (int s = 0; s < 4; s++) {
+      const bool y = s < 2;
+      gamb_p[pO[s]] = 1.0 / pk.r_amb_sec_per;
+      link(pO[s], pC[s], (y ? pk.r_pcb2_y : pk.r_pcb2_x) + pk.r_pcb);
+      gamb_p[pC[s]] = 1.0 / (y ? pk.r_amb_sec_c_per_y : pk.r_amb_sec_c_per_x);
+      link(pC[s], sO[s], y ? pk.r_pcb_c_per_y : pk.r_pcb_c_per_x);
+      link(sO[s], bO[s], y ? pk.r_solder_per_y : pk.r_solder_per_x);
+      edge(pC[s], el[2], s);
+      edge(sO[s], el[3], s);
+      edge(bO[s], el[4], s);
+    }
   }
   for (int k = 0; k < NXP; k++) {
     ps.gamb[k] = (float)gamb_p[k];
@@ -1295,11 +1339,9 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
       std::vector<double> A((size_t)n * 2 * n, 0.0);   // [A | I], Gauss-Jordan in place
       auto at = [&](long long r, long long c) -> double & { return A[(size_t)r * 2 * n + c]; };
       const long long N = C.ncell, pl = C.plane;
-      auto node_of = [&](int layer, int side) -> int {
-        if (layer == m->hsidx) return side == 0 ? HSB_SINK_C_N : side == 1 ? HSB_SINK_C_S : side == 2 ? HSB_SINK_C_W : HSB_SINK_C_E;
-        if (layer == m->spidx) return side == 0 ? HSB_SP_N : side == 1 ? HSB_SP_S : side == 2 ? HSB_SP_W : HSB_SP_E;
-        return -1;
-      };
+      int el[5];
+      edge_layers(m, el);
+      auto node_of = [&](int layer, int side) -> int { return edge_node(layer, side, el); };
       for (long long c = 0; c < N; c++) {
         const int ln = (int)(c / pl);
         const long long q = c - ln * pl;
@@ -1311,7 +1353,7 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
         if (i > 0) at(c, c - C.nc) -= gS[c - C.nc];
         if (ln < nl - 1) at(c, c + pl) -= gB[c];
         if (ln > 0) at(c, c - pl) -= gB[c - pl];
-        if (ln == m->spidx || ln == m->hsidx) {
+        if (edge_layer(ln, el)) {
           const float gn = (float)(gens[ln] * scale), gw = (float)(geew[ln] * scale);
           if (i == 0) at(c, N + node_of(ln, 0)) -= gn;
           if (i == C.nr - 1) at(c, N + node_of(ln, 1)) -= gn;
@@ -1487,7 +1529,7 @@ static int dot(hsb_dev_model *m, MgWork *w, const float *a, const float *b, long
 }
 
 int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
-  if (m->nx != HSB_EXTRA) return set_error(HSB_E_ARG, "the multigrid steady solver models the primary heat path only");
+
   if (m->uchan_mask) return set_error(HSB_E_ARG, "advection makes the system non-symmetric: use BiCGStab");
   MgWork *w = (MgWork *)m->mg;
   int rc;

@@ -186,6 +186,26 @@ class RCModel:
         f = self.ptr.contents.layers[l].flp.contents
         return [f.units[u].name.decode() for u in range(f.n_units)]
 
+    def block_dims(self) -> tuple[np.ndarray, np.ndarray]:
+        """Height and width (m) of every block; 0 for blocks of layers without power."""
+        h, w = np.zeros(self.total_n_blocks), np.zeros(self.total_n_blocks)
+        base = 0
+        for l in range(self.n_layers):
+            f = self.ptr.contents.layers[l].flp.contents
+            if self.layer_power[l]:
+                for u in range(f.n_units):
+                    h[base + u], w[base + u] = f.units[u].height, f.units[u].width
+            base += self.layer_units[l]
+        return h, w
+
+    def steady_leakage(self, power: np.ndarray, temp: np.ndarray) -> int:
+        """The temperature-leakage fixed point of the steady solve on the device
+        (steady_state_temp with leakage_used); temp: start in, result out.
+        Returns the number of steady solves."""
+        it = C.c_int()
+        check(lib().hsb_grid_steady_leakage(self.ptr, dptr(power), dptr(temp), C.byref(it)))
+        return it.value
+
     def power_vector(self, row) -> np.ndarray:
         """Scatter one trace row (power layers' blocks, floorplan order) into a block vector."""
         p = self.vector()

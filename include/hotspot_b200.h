@@ -123,6 +123,13 @@ int hsb_grid_populate_R(grid_model_t *model, flp_t *flp);
 int hsb_grid_populate_C(grid_model_t *model, flp_t *flp);
 int hsb_grid_compute_temp(grid_model_t *model, double *power, double *temp, double time_elapsed);
 int hsb_grid_steady(grid_model_t *model, double *power, double *temp);
+/* the temperature-leakage fixed point of steady_state_temp with leakage_used
+ * (temperature.c:706-746; calc_leakage, temperature.c:910-927) with the
+ * block vectors on the device between iterations: temp holds the starting
+ * temperatures and receives the result; *iterations (may be NULL) the
+ * steady solves it took.  HSB_E_NOCONV on thermal runaway or when the loop
+ * does not converge, as the reference's fatal() cases */
+int hsb_grid_steady_leakage(grid_model_t *model, double *power, double *temp, int *iterations);
 /* the device model behind a grid model (for the batch and serving layers) */
 struct hsb_dev_model *hsb_grid_device(grid_model_t *model);
 /* floorplan reader with flp.c's format (read_flp, flp.c:1175), for callers

@@ -289,6 +289,14 @@ int hsb_dev_set_priority(hsb_dev_model *m, int high);
  * FP64 sums over grid edges does. */
 int hsb_dev_set_tile(hsb_dev_model *m, int rows, int cols);
 
+/* the temperature-leakage fixed point of the steady solve (temperature.c:
+ * 706-746) on the device: height/width of each of the total_n_blocks blocks
+ * (0 for blocks of layers without power), block_temp in: starting
+ * temperatures, out: the result; *iterations: steady solves taken */
+int hsb_dev_steady_leakage(hsb_dev_model *m, const double *block_power, const double *height,
+                           const double *width, double *block_temp, const hsb_solver_opts *o,
+                           int *iterations, hsb_stats *st);
+
 /* which of the model's solver workspaces exist (no counterpart in the
  * reference): the fast transient, MG-PCG and BiCGStab solvers allocate
  * theirs on their first call; *mask = OR of HSB_WS_* */

@@ -202,3 +202,37 @@ def test_forms_alternate_on_one_model(workdir):
         assert np.max(np.abs(t - to)) <= TOL, k
     assert np.max(np.abs(m.grid("trans") - o.grid("trans"))) <= TOL
     m.close()
+
+
+def test_mg_steady_secondary_path(workdir):
+    """The MG-PCG steady solve on the secondary heat path (substrate, solder
+    and PCB layers, 28 package nodes; the steady package equations of
+    temperature_grid.c:2228-2379) against the reference's own steady result
+    (golden vectors of the reference build, which stops within 1e-3 K of the
+    fixed point) and, on a 64x64 chip, against the FP64 replay of the
+    reference's Gauss-Seidel: 0.01 K, with a converged FP64 residual."""
+    from test_gpu_parity import _golden
+    sc, n, g = _golden(workdir, "secondary_16")
+    m = hm.from_scenario(sc)
+    m.set_solver(FORM_FAST)
+    s = m.vector()
+    m.steady(g["steady_power"].copy(), s)
+    assert np.max(np.abs(s - g["steady"])) <= TOL
+    assert np.max(np.abs(m.grid("steady") - g["grid_steady"])) <= TOL
+    assert m.stats()["refinements"] >= 1
+    m.close()
+    sc = W.scenario_chip2d(workdir, seed=23, grid=64, steps=2)
+    sc.config["model_secondary"] = "1"
+    out = []
+    for form in (FORM_FAST, None):
+        m = hm.from_scenario(sc)
+        if form is not None:
+            m.set_solver(form)
+        p = m.power_vector(sc.block_power.mean(0))
+        s = m.vector()
+        m.steady(p.copy(), s)
+        out.append((s, m.grid("steady"), m.stats()))
+        m.close()
+    (sf, gf, stf), (sr, gr, _) = out
+    assert np.max(np.abs(sf - sr)) <= TOL and np.max(np.abs(gf - gr)) <= TOL
+    assert stf["residual"] < 1e-6
