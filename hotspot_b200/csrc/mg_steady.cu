@@ -29,7 +29,7 @@
 namespace hsb {
 
 #define MGT 256
-#define NXP (HSB_EXTRA + HSB_EXTRA_SEC)   // package nodes of either path; the primary path's unused ones are inert
+#define NXP (HSB_EXTRA + HSB_EXTRA_SEC)   // package node slots of either path; the primary path uses 12
 #ifndef MG_SWEEPS
 #define MG_SWEEPS 1  // smoothing sweeps before and after each coarse-grid correction
 #endif
@@ -45,6 +45,7 @@ struct PackSys {               // the 12 package nodes' equations
   float gamb[NXP];             // conductance to ambient
   int elayer[NXP], eside[NXP]; // attached edge: layer, side (0 N,1 S,2 W,3 E), -1 none
   float ge0[NXP];              // per-cell edge conductance at level 0
+  int nx;                      // the model's nodes (12 or 28); the solves touch only these
 };
 
 struct MgLevelDev {
@@ -161,7 +162,7 @@ __device__ void apply_pack_rows(const MgLevelDev &L, const PackSys *__restrict__
   __shared__ float esum[NXP];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const float *xp = x + L.ncell;
-  for (int k = w; k < NXP; k += blockDim.x >> 5) {
+  for (int k = w; k < ps->nx; k += blockDim.x >> 5) {
     float s = 0.f;
     const int layer = ps->elayer[k], side = ps->eside[k];
     if (layer >= 0) {
@@ -176,11 +177,11 @@ __device__ void apply_pack_rows(const MgLevelDev &L, const PackSys *__restrict__
     if (lane == 0) esum[k] = s;
   }
   __syncthreads();
-  if (threadIdx.x < NXP) {
+  if (threadIdx.x < ps->nx) {
     const int k = threadIdx.x;
     const float ge = ps->ge0[k] * L.scale;
     float s = ge * esum[k] + ps->gamb[k] * xp[k];
-    for (int o = 0; o < NXP; o++) s += ps->link[k][o] * (xp[k] - xp[o]);
+    for (int o = 0; o < ps->nx; o++) s += ps->link[k][o] * (xp[k] - xp[o]);
     y[L.ncell + k] = mode ? f[L.ncell + k] - s : s;
   }
 }
@@ -330,7 +331,7 @@ __global__ void mg_pack_solve(MgLevelDev L, const PackSys *__restrict__ ps, floa
                               const float *__restrict__ f) {
   __shared__ float esum[NXP], rhs[NXP];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int k = w; k < NXP; k += blockDim.x >> 5) {
+  for (int k = w; k < ps->nx; k += blockDim.x >> 5) {
     float s = 0.f;
     const int layer = ps->elayer[k], side = ps->eside[k];
     if (layer >= 0) {
@@ -344,16 +345,16 @@ __global__ void mg_pack_solve(MgLevelDev L, const PackSys *__restrict__ ps, floa
     if (lane == 0) esum[k] = s;
   }
   __syncthreads();
-  if (threadIdx.x < NXP) {
+  if (threadIdx.x < ps->nx) {
     const int k = threadIdx.x;
     rhs[k] = f[L.ncell + k] + ps->ge0[k] * L.scale * esum[k];
   }
   __syncthreads();
-  if (threadIdx.x < NXP) {
+  if (threadIdx.x < ps->nx) {
     const int k = threadIdx.x;
     float s = 0.f;
 #pragma unroll
-    for (int o = 0; o < NXP; o++) s += L.pinv[k * NXP + o] * rhs[o];
+    for (int o = 0; o < ps->nx; o++) s += L.pinv[k * NXP + o] * rhs[o];
     x[L.ncell + k] = s;
   }
 }
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(1024) mg_coarse_solve(MgLevelDev L, const Pack
     __syncthreads();
   };
   auto pk = [&]() {
-    for (int k = w; k < NXP; k += blockDim.x >> 5) {
+    for (int k = w; k < ps->nx; k += blockDim.x >> 5) {
       float sm = 0.f;
       const int layer = ps->elayer[k], side = ps->eside[k];
       if (layer >= 0) {
@@ -388,11 +389,11 @@ __global__ void __launch_bounds__(1024) mg_coarse_solve(MgLevelDev L, const Pack
       if (lane == 0) esum[k] = sm;
     }
     __syncthreads();
-    if (threadIdx.x < NXP) rhs[threadIdx.x] = f[L.ncell + threadIdx.x] + ps->ge0[threadIdx.x] * L.scale * esum[threadIdx.x];
+    if (threadIdx.x < ps->nx) rhs[threadIdx.x] = f[L.ncell + threadIdx.x] + ps->ge0[threadIdx.x] * L.scale * esum[threadIdx.x];
     __syncthreads();
-    if (threadIdx.x < NXP) {
+    if (threadIdx.x < ps->nx) {
       float v = 0.f;
-      for (int o = 0; o < NXP; o++) v += L.pinv[threadIdx.x * NXP + o] * rhs[o];
+      for (int o = 0; o < ps->nx; o++) v += L.pinv[threadIdx.x * NXP + o] * rhs[o];
       x[L.ncell + threadIdx.x] = v;
     }
     __syncthreads();
@@ -572,7 +573,7 @@ __device__ __noinline__ void fz_pk(const MgLevelDev &L, const PackSys *ps, float
                                    float *prhs) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int w = tid >> 5, lane = tid & 31, nw = nt >> 5;
-  for (int k = w; k < NXP; k += nw) {
+  for (int k = w; k < ps->nx; k += nw) {
     float sm = 0.f;
     const int layer = ps->elayer[k], side = ps->eside[k];
     if (layer >= 0) {
@@ -586,12 +587,12 @@ __device__ __noinline__ void fz_pk(const MgLevelDev &L, const PackSys *ps, float
     if (lane == 0) esum[k] = sm;
   }
   __syncthreads();
-  if (tid < NXP) prhs[tid] = f[L.ncell + tid] + ps->ge0[tid] * L.scale * esum[tid];
+  if (tid < ps->nx) prhs[tid] = f[L.ncell + tid] + ps->ge0[tid] * L.scale * esum[tid];
   __syncthreads();
-  if (tid < NXP) {
+  if (tid < ps->nx) {
     float v = 0.f;
 #pragma unroll
-    for (int o = 0; o < NXP; o++) v += L.pinv[tid * NXP + o] * prhs[o];
+    for (int o = 0; o < ps->nx; o++) v += L.pinv[tid * NXP + o] * prhs[o];
     x[L.ncell + tid] = v;
   }
   __syncthreads();
@@ -624,7 +625,7 @@ __device__ __noinline__ void fz_resid(const MgLevelDev &L, const PackSys *ps, co
     }
     r[c] = f[c] - s;
   }
-  for (int k = w; k < NXP; k += nw) {
+  for (int k = w; k < ps->nx; k += nw) {
     float sm = 0.f;
     const int layer = ps->elayer[k], side = ps->eside[k];
     if (layer >= 0) {
@@ -639,11 +640,11 @@ __device__ __noinline__ void fz_resid(const MgLevelDev &L, const PackSys *ps, co
     if (lane == 0) esum[k] = sm;
   }
   __syncthreads();
-  if (tid < NXP) {
+  if (tid < ps->nx) {
     const int k = tid;
     const float ge = ps->ge0[k] * L.scale;
     float s = ge * esum[k] + ps->gamb[k] * xp[k];
-    for (int o = 0; o < NXP; o++) s += ps->link[k][o] * (xp[k] - xp[o]);
+    for (int o = 0; o < ps->nx; o++) s += ps->link[k][o] * (xp[k] - xp[o]);
     r[L.ncell + k] = f[L.ncell + k] - s;
   }
   __syncthreads();
@@ -857,12 +858,16 @@ __global__ void fine_residual64(const hsb::StencilArgs S, const double *__restri
     if (n > 0) s += gB[c - S.plane] * (Tc - T[c - S.plane]);
     const double *x = T + S.ncell;
     const hsb::LayerCoef &Ln = S.L[n];
-    if (Ln.kind == hsb::LK_SPREADER || Ln.kind == hsb::LK_SINK) {
-      const int sp = Ln.kind == hsb::LK_SPREADER;
-      if (i == 0) s += gENS[n] * (Tc - x[sp ? HSB_SP_N : HSB_SINK_C_N]);
-      if (i == S.nr - 1) s += gENS[n] * (Tc - x[sp ? HSB_SP_S : HSB_SINK_C_S]);
-      if (j == 0) s += gEEW[n] * (Tc - x[sp ? HSB_SP_W : HSB_SINK_C_W]);
-      if (j == S.nc - 1) s += gEEW[n] * (Tc - x[sp ? HSB_SP_E : HSB_SINK_C_E]);
+    // the edge group's W node (its nodes are W, E, N, S)
+    const int k = Ln.kind;
+    const int wn = k == hsb::LK_SINK ? HSB_SINK_C_W : k == hsb::LK_SPREADER ? HSB_SP_W
+                   : k == hsb::LK_PCB ? HSB_PCB_C_W : k == hsb::LK_SOLDER ? HSB_SOLDER_W
+                   : k == hsb::LK_SUB ? HSB_SUB_W : -1;
+    if (wn >= 0) {
+      if (i == 0) s += gENS[n] * (Tc - x[wn + 2]);
+      if (i == S.nr - 1) s += gENS[n] * (Tc - x[wn + 3]);
+      if (j == 0) s += gEEW[n] * (Tc - x[wn + 0]);
+      if (j == S.nc - 1) s += gEEW[n] * (Tc - x[wn + 1]);
     }
     res = b[c] - s;
     r[c] = res;
@@ -880,7 +885,7 @@ __global__ void pack_residual64(const hsb::StencilArgs S, const PackSys *__restr
                                 float *__restrict__ r32, unsigned long long *maxbits) {
   __shared__ double esum[NXP];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int k = w; k < NXP; k += blockDim.x >> 5) {
+  for (int k = w; k < S.nx; k += blockDim.x >> 5) {
     double s = 0.0;
     const int layer = ps->elayer[k], side = ps->eside[k];
     if (layer >= 0) {
@@ -1184,7 +1189,7 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
   edge_layers(m, el);
   for (int n = 0; n < nl; n++) {
     const LayerCoef &c = m->hostL0[n];
-    if (c.ramb != 0.0) gamb[n] = 1.0 / c.ramb;
+    if (c.kind == LK_SINK || c.kind == LK_PCB) gamb[n] = 1.0 / c.ramb;   // ramb is rz on the other layers
     if (edge_layer(n, el)) {
       gens[n] = 1.0 / c.edgeNS;
       geew[n] = 1.0 / c.edgeEW;
@@ -1237,6 +1242,7 @@ static int mg_build(hsb_dev_model *m, MgWork *w) {
       edge(bO[s], el[4], s);
     }
   }
+  ps.nx = m->nx;
   for (int k = 0; k < NXP; k++) {
     ps.gamb[k] = (float)gamb_p[k];
     ps.ge0[k] = (float)ge_p[k];

@@ -65,7 +65,7 @@
 #define DRAIN_MS 4.0
 #define CHUNK_MAX_INTERVALS 64
 // cell-intervals per launch of the batch engine, and its interval cap
-#define TICK_CELL_INTERVALS (1LL << 22)
+#define TICK_CELL_INTERVALS (1LL << 21)
 #define TICK_MAX_INTERVALS 16
 
 struct hsb_server {

@@ -41,8 +41,9 @@ def test_leakage_loop_on_device(workdir, case):
         m = hm.from_scenario(sc)
         if form is not None:
             m.set_solver(form)
-        p = m.power_vector(sc.block_power.mean(0))
-        t0 = m.vector(m.config.init_temp)
+        # a start at ambient, so the first solve is a rise and the loop takes several
+        p = m.power_vector(0.5 * sc.block_power.mean(0))
+        t0 = m.vector(m.config.ambient)
         t_dev = t0.copy()
         n_dev = m.steady_leakage(p.copy(), t_dev)
         t_host, n_host = _host_loop(m, p.copy(), t0)
