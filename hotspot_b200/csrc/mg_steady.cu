@@ -177,12 +177,16 @@ __device__ void apply_pack_rows(const MgLevelDev &L, const PackSys *__restrict__
     if (lane == 0) esum[k] = s;
   }
   __syncthreads();
-  if (threadIdx.x < ps->nx) {
+  if (threadIdx.x < NXP) {   // the slots the model has no node for stay zero
     const int k = threadIdx.x;
-    const float ge = ps->ge0[k] * L.scale;
-    float s = ge * esum[k] + ps->gamb[k] * xp[k];
-    for (int o = 0; o < ps->nx; o++) s += ps->link[k][o] * (xp[k] - xp[o]);
-    y[L.ncell + k] = mode ? f[L.ncell + k] - s : s;
+    float v = 0.f;
+    if (k < ps->nx) {
+      const float ge = ps->ge0[k] * L.scale;
+      float s = ge * esum[k] + ps->gamb[k] * xp[k];
+      for (int o = 0; o < ps->nx; o++) s += ps->link[k][o] * (xp[k] - xp[o]);
+      v = mode ? f[L.ncell + k] - s : s;
+    }
+    y[L.ncell + k] = v;
   }
 }
 
@@ -350,11 +354,11 @@ __global__ void mg_pack_solve(MgLevelDev L, const PackSys *__restrict__ ps, floa
     rhs[k] = f[L.ncell + k] + ps->ge0[k] * L.scale * esum[k];
   }
   __syncthreads();
-  if (threadIdx.x < ps->nx) {
+  if (threadIdx.x < NXP) {
     const int k = threadIdx.x;
     float s = 0.f;
-#pragma unroll
-    for (int o = 0; o < ps->nx; o++) s += L.pinv[k * NXP + o] * rhs[o];
+    if (k < ps->nx)
+      for (int o = 0; o < ps->nx; o++) s += L.pinv[k * NXP + o] * rhs[o];
     x[L.ncell + k] = s;
   }
 }
@@ -391,9 +395,10 @@ __global__ void __launch_bounds__(1024) mg_coarse_solve(MgLevelDev L, const Pack
     __syncthreads();
     if (threadIdx.x < ps->nx) rhs[threadIdx.x] = f[L.ncell + threadIdx.x] + ps->ge0[threadIdx.x] * L.scale * esum[threadIdx.x];
     __syncthreads();
-    if (threadIdx.x < ps->nx) {
+    if (threadIdx.x < NXP) {
       float v = 0.f;
-      for (int o = 0; o < ps->nx; o++) v += L.pinv[threadIdx.x * NXP + o] * rhs[o];
+      if ((int)threadIdx.x < ps->nx)
+        for (int o = 0; o < ps->nx; o++) v += L.pinv[threadIdx.x * NXP + o] * rhs[o];
       x[L.ncell + threadIdx.x] = v;
     }
     __syncthreads();
@@ -589,10 +594,10 @@ __device__ __noinline__ void fz_pk(const MgLevelDev &L, const PackSys *ps, float
   __syncthreads();
   if (tid < ps->nx) prhs[tid] = f[L.ncell + tid] + ps->ge0[tid] * L.scale * esum[tid];
   __syncthreads();
-  if (tid < ps->nx) {
+  if (tid < NXP) {   // the slots the model has no node for stay zero
     float v = 0.f;
-#pragma unroll
-    for (int o = 0; o < ps->nx; o++) v += L.pinv[tid * NXP + o] * prhs[o];
+    if (tid < ps->nx)
+      for (int o = 0; o < ps->nx; o++) v += L.pinv[tid * NXP + o] * prhs[o];
     x[L.ncell + tid] = v;
   }
   __syncthreads();
@@ -640,12 +645,16 @@ __device__ __noinline__ void fz_resid(const MgLevelDev &L, const PackSys *ps, co
     if (lane == 0) esum[k] = sm;
   }
   __syncthreads();
-  if (tid < ps->nx) {
+  if (tid < NXP) {   // the slots the model has no node for stay zero (shared memory is not)
     const int k = tid;
-    const float ge = ps->ge0[k] * L.scale;
-    float s = ge * esum[k] + ps->gamb[k] * xp[k];
-    for (int o = 0; o < ps->nx; o++) s += ps->link[k][o] * (xp[k] - xp[o]);
-    r[L.ncell + k] = f[L.ncell + k] - s;
+    float v = 0.f;
+    if (k < ps->nx) {
+      const float ge = ps->ge0[k] * L.scale;
+      float s = ge * esum[k] + ps->gamb[k] * xp[k];
+      for (int o = 0; o < ps->nx; o++) s += ps->link[k][o] * (xp[k] - xp[o]);
+      v = f[L.ncell + k] - s;
+    }
+    r[L.ncell + k] = v;
   }
   __syncthreads();
 }

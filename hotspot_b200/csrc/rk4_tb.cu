@@ -131,26 +131,11 @@ template <> __device__ __forceinline__ const double *tb_power_of<double>(const T
 // P0: dst = V_0 = (p + L y) / C from the state deviations in src;
 // else dst = h L src.  Package inputs from xs (BND: grid-boundary cells
 // present in the region).  The operation order per cell is rk4_krylov.cu's.
-// A thread takes two horizontally adjacent cells (a pair) of a row: they
-// share the layer constants, the index arithmetic and the loads of each
-// other's centre value (the E neighbour of the first is the second, the W
-// neighbour of the second the first).  The pairs are dealt to the CTA's
-// threads in row-major order, so every thread gets the same number of pairs
-// to within one whatever the rectangle's shape.
+// The rectangle's columns are dealt to the CTA's threads in row-major order
+// (consecutive threads take consecutive columns of a row), so every thread
+// gets the same number of columns to within one whatever the rectangle's
+// shape.
 // ---------------------------------------------------------------------------
-template <typename V, int NL, bool BND>
-__device__ __forceinline__ void tb_cell_edges(const TChip &C, const V *__restrict__ xs, int nb, int gi, int gj,
-                                              V gEdgeNS, V gEdgeEW, V cur, V &s) {
-  if (BND) {
-    if (nb >= 0) {
-      if (gi == 0) s += gEdgeNS * (xs[nb + 2] - cur);
-      if (gi == C.nr - 1) s += gEdgeNS * (xs[nb + 3] - cur);
-      if (gj == C.nc - 1) s += gEdgeEW * (xs[nb + 1] - cur);
-      if (gj == 0) s += gEdgeEW * (xs[nb + 0] - cur);
-    }
-  }
-}
-
 template <typename V, int NL, bool BND, bool P0>
 __device__ __forceinline__ void tb_pass(const TChip &C, const TSh<V> &sh, const V *__restrict__ xs,
                                         const V *__restrict__ src, V *__restrict__ dst, int RI, int RJ, int ra,
@@ -158,36 +143,26 @@ __device__ __forceinline__ void tb_pass(const TChip &C, const TSh<V> &sh, const 
   const int LP = RI * RJ;
   const int nrow = rb - ra, ncol = cb - ca;
   if (nrow <= 0 || ncol <= 0) return;
-  const int npr = (ncol + 1) >> 1;   // pairs per row (the last one single when ncol is odd)
-  const int tot = nrow * npr;
+  const int tot = nrow * ncol;
   const int nr = C.nr, nc = C.nc;
-  int rr = (int)threadIdx.x / npr, cc = (int)threadIdx.x - rr * npr;
-  const int dr = TB_THREADS / npr, dc = TB_THREADS - dr * npr;
+  int rr = (int)threadIdx.x / ncol, cc = (int)threadIdx.x - rr * ncol;
+  const int dr = TB_THREADS / ncol, dc = TB_THREADS - dr * ncol;
   for (int k = threadIdx.x; k < tot; k += TB_THREADS) {
-    const int r = ra + rr, c = ca + 2 * cc;
+    const int r = ra + rr, c = ca + cc;
     cc += dc;
     rr += dr;
-    if (cc >= npr) {
-      cc -= npr;
+    if (cc >= ncol) {
+      cc -= ncol;
       rr++;
     }
     const int gi = gi0 + r, gj = gj0 + c;
-    bool okA = true, okB = c + 1 < cb;
-    if (BND) {
-      const bool rowok = (unsigned)gi < (unsigned)nr;
-      okA = rowok && (unsigned)gj < (unsigned)nc;
-      okB = okB && rowok && (unsigned)(gj + 1) < (unsigned)nc;
-      if (!okA && !okB) continue;
-    }
+    if (BND && ((unsigned)gi >= (unsigned)nr || (unsigned)gj >= (unsigned)nc)) continue;
     const V *p = src + r * RJ + c;
     V *o = dst + r * RJ + c;
-    const bool hN = !BND || gi > 0, hS = !BND || gi < nr - 1;
-    const bool hWa = !BND || gj > 0, hEa = !BND || gj < nc - 1;
-    const bool hWb = !BND || gj + 1 > 0, hEb = !BND || gj + 1 < nc - 1;
+    const bool hN = !BND || gi > 0, hS = !BND || gi < nr - 1, hW = !BND || gj > 0, hE = !BND || gj < nc - 1;
     const V *pw = nullptr;
     if constexpr (P0) pw = tb_power_of<V>(C) + (long long)gi * nc + gj;
-    V upA = 0, upB = 0, gup = 0;
-    V curA = okA ? p[0] : V(0), curB = okB ? p[1] : V(0);
+    V up = 0, cur = p[0], gup = 0;
 #pragma unroll
     for (int n = 0; n < NL; n++) {
       const V *pn = p + n * LP;
@@ -204,41 +179,28 @@ __device__ __forceinline__ void tb_pass(const TChip &C, const TSh<V> &sh, const 
         gEdgeNS = sh.L[n].gEdgeNS; gEdgeEW = sh.L[n].gEdgeEW; gAmb = sh.L[n].gAmb;
         nb = sh.L[n].nbase;
       }
-      const V sc = invC * hf;
-      V dnA = 0, dnB = 0;
-      if (okA) {
-        dnA = n < NL - 1 ? pn[LP] : V(0);
-        V s = 0;
-        if (hN) s += gNS * (pn[-RJ] - curA);
-        if (hS) s += gNS * (pn[RJ] - curA);
-        if (hEa) s += gEW * ((okB ? curB : pn[1]) - curA);
-        if (hWa) s += gEW * (pn[-1] - curA);
-        if (n > 0) s += gup * (upA - curA);
-        if (n < NL - 1) s += gDn * (dnA - curA);
-        s -= gAmb * curA;                        // sink / PCB to ambient (0 elsewhere)
-        tb_cell_edges<V, NL, BND>(C, xs, nb, gi, gj, gEdgeNS, gEdgeEW, curA, s);
-        if constexpr (P0) o[n * LP] = (__ldg(pw + (long long)n * C.plane) + s) * invC;
-        else o[n * LP] = s * sc;
+      const V dn = n < NL - 1 ? pn[LP] : V(0);
+      V s = 0;
+      if (hN) s += gNS * (pn[-RJ] - cur);
+      if (hS) s += gNS * (pn[RJ] - cur);
+      if (hE) s += gEW * (pn[1] - cur);
+      if (hW) s += gEW * (pn[-1] - cur);
+      if (n > 0) s += gup * (up - cur);
+      if (n < NL - 1) s += gDn * (dn - cur);
+      s -= gAmb * cur;                         // sink / PCB to ambient (0 elsewhere)
+      if (BND) {
+        if (nb >= 0) {
+          if (gi == 0) s += gEdgeNS * (xs[nb + 2] - cur);
+          if (gi == nr - 1) s += gEdgeNS * (xs[nb + 3] - cur);
+          if (gj == nc - 1) s += gEdgeEW * (xs[nb + 1] - cur);
+          if (gj == 0) s += gEdgeEW * (xs[nb + 0] - cur);
+        }
       }
-      if (okB) {
-        dnB = n < NL - 1 ? pn[LP + 1] : V(0);
-        V s = 0;
-        if (hN) s += gNS * (pn[1 - RJ] - curB);
-        if (hS) s += gNS * (pn[1 + RJ] - curB);
-        if (hEb) s += gEW * (pn[2] - curB);
-        if (hWb) s += gEW * ((okA ? curA : pn[0]) - curB);
-        if (n > 0) s += gup * (upB - curB);
-        if (n < NL - 1) s += gDn * (dnB - curB);
-        s -= gAmb * curB;
-        tb_cell_edges<V, NL, BND>(C, xs, nb, gi, gj + 1, gEdgeNS, gEdgeEW, curB, s);
-        if constexpr (P0) o[n * LP + 1] = (__ldg(pw + (long long)n * C.plane + 1) + s) * invC;
-        else o[n * LP + 1] = s * sc;
-      }
+      if constexpr (P0) o[n * LP] = (__ldg(pw + (long long)n * C.plane) + s) * invC;
+      else o[n * LP] = s * (invC * hf);
       gup = gDn;
-      upA = curA;
-      upB = curB;
-      curA = dnA;
-      curB = dnB;
+      up = cur;
+      cur = dn;
     }
   }
 }
