@@ -788,6 +788,18 @@ def run_ours(args):
                 line[name] = fn()
             except Exception as e:      # a failed leg is reported, the headline still prints
                 line[name] = {"error": f"{type(e).__name__}: {e}"}
+        # per-request latency of the reference on the host, from the 2-D chip
+        # leg's single-threaded reference runs (the serving mix's smallest
+        # class, 64x64): a steady request, and a 500-interval transient
+        c0, sv = line.get("chip2d", {}), line.get("serving", {})
+        cb = c0.get("cpu_baseline") if isinstance(c0, dict) else None
+        if cb and isinstance(sv, dict) and "error" not in sv:
+            sv["cpu_reference_per_request"] = {
+                "steady_64x64_s": cb["steady_s"],
+                "transient_500_intervals_64x64_s": cb["trace_s"] * 500.0 / args.chip2d_rows,
+                "cores": 1,
+                "sample": f"the 2-D chip leg's reference runs: one steady solve, {args.chip2d_rows} rows scaled to "
+                          "500; larger classes take longer in proportion to their cells"}
     print(json.dumps(line), flush=True)
     m.close()
     if pg:

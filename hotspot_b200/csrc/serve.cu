@@ -62,7 +62,7 @@
 // cell-intervals per launch of a background transient while a priority class runs
 #define CHUNK_CELL_INTERVALS (1LL << 20)
 // longest wait of a priority request for background work to reach a yield point
-#define DRAIN_MS 4.0
+#define DRAIN_MS 2.0
 #define CHUNK_MAX_INTERVALS 64
 // cell-intervals per launch of the batch engine, and its interval cap
 #define TICK_CELL_INTERVALS (1LL << 21)
