@@ -34,7 +34,10 @@ namespace hsb {
 #define MG_SWEEPS 1  // smoothing sweeps before and after each coarse-grid correction
 #endif
 #ifndef MG_INNER
-#define MG_INNER 6   // PCG iterations per FP64 refinement pass
+#define MG_INNER 6   // PCG iterations of the first FP64 refinement pass
+#endif
+#ifndef MG_INNER_NEXT
+#define MG_INNER_NEXT 3   // ... and of the later ones, which start from a small residual
 #endif
 // background solves of at least this many cells yield between PCG iterations
 #define MG_YIELD_SPLIT_CELLS (1LL << 18)
@@ -81,7 +84,7 @@ struct MgWork {
   double *red;                   // reduction scratch
   double *h_red;
   // one refinement pass (FP64 residual, inner PCG, correction) as a graph
-  cudaGraphExec_t pass_exec;
+  cudaGraphExec_t pass_exec, pass_exec_next;   // the first refinement pass; the later ones
   const double *pass_T;
   int pass_version;
   // the same pass in pieces (head + first iteration, one further iteration,
@@ -1177,6 +1180,7 @@ static void free_mg(void *p) {
     if (q) cudaFree(q);
   if (w->h_red) cudaFreeHost(w->h_red);
   if (w->pass_exec) cudaGraphExecDestroy(w->pass_exec);
+  if (w->pass_exec_next) cudaGraphExecDestroy(w->pass_exec_next);
   for (auto &e : w->piece_exec)
     if (e) cudaGraphExecDestroy(e);
   delete w;
@@ -1619,13 +1623,20 @@ int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
   // them, so that it holds the device for one iteration at most after a
   // priority request arrives; otherwise one graph per pass
   const bool pieces = m->yield_fn && m->ncell >= MG_YIELD_SPLIT_CELLS && inner > 1;
+  const int inner_next = MG_INNER_NEXT < inner ? MG_INNER_NEXT : inner;
   if (!pieces && (!w->pass_exec || w->pass_T != T || w->pass_version != m->coef_version)) {
     if ((rc = capture([&]() {
                         head();
                         for (int it = 0; it < inner; it++) iteration(it);
                         tail();
                       },
-                      &w->pass_exec, "capturing the multigrid refinement pass")))
+                      &w->pass_exec, "capturing the multigrid refinement pass")) ||
+        (rc = capture([&]() {
+                        head();
+                        for (int it = 0; it < inner_next; it++) iteration(it);
+                        tail();
+                      },
+                      &w->pass_exec_next, "capturing the later multigrid refinement passes")))
       return rc;
     w->pass_T = T;
     w->pass_version = m->coef_version;
@@ -1651,16 +1662,19 @@ int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
   double rmax = 0.0, emax = 1e300, eprev = 0.0;
   bool converged = false;
   for (refine = 0; refine < max_ref; refine++) {
+    // the first pass takes the solution from the heuristic start; the later
+    // ones correct an error the FP32 inner solve left, a few digits each
+    const int n_it = refine == 0 ? inner : inner_next;
     if (pieces) {
       HSB_CUDA(cudaGraphLaunch(w->piece_exec[0], m->stream));
-      for (int it = 1; it < inner; it++) {
+      for (int it = 1; it < n_it; it++) {
         HSB_CUDA(cudaStreamSynchronize(m->stream));
         m->yield_fn(m->yield_ctx);
         HSB_CUDA(cudaGraphLaunch(w->piece_exec[1], m->stream));
       }
       HSB_CUDA(cudaGraphLaunch(w->piece_exec[2], m->stream));
     } else {
-      HSB_CUDA(cudaGraphLaunch(w->pass_exec, m->stream));
+      HSB_CUDA(cudaGraphLaunch(refine == 0 ? w->pass_exec : w->pass_exec_next, m->stream));
     }
     HSB_CUDA(cudaStreamSynchronize(m->stream));
     {
@@ -1669,7 +1683,7 @@ int mg_steady(hsb_dev_model *m, const hsb_solver_opts *o, hsb_stats *st) {
       memcpy(&emax, &bits, sizeof(emax));
     }
     st->refinements += 1;
-    st->cycles += inner;
+    st->cycles += n_it;
     if (emax < tol) {
       converged = true;
       break;
