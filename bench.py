@@ -326,10 +326,10 @@ def leg_batched(args, flush):
     cpu_time = sum(cells[c] * chip_steps[c] / side_rate.get(sides[c], min(side_rate.values()))
                    for c in range(len(models)))
     cpu_rate = cs / cpu_time
-    # each chip's steady solve: all 512 at once through the serving loop, 16 in flight
+    # each chip's steady solve: all 512 at once through the serving loop, 32 in flight
     from hotspot_b200.serving import Request, Server
     from hotspot_b200 import _abi
-    srv = Server(workers=16)
+    srv = Server(workers=32)
     for mm in models:
         srv.add_model(mm, FORM_FAST, 1e-5)
     sreq = [Request(i, _abi.REQ_STEADY, mm.power_vector(sc.block_power[:k].mean(0)), 0.0, tag="steady")
@@ -346,7 +346,7 @@ def leg_batched(args, flush):
             "ms_per_interval": kms / K, "rk4_steps": int(chip_steps.sum()),
             "steady_solves_per_s": len(sreq) / steady_span,
             "steady_note": "every chip's steady solve (MG-PCG, FP64 refinement to 1e-5 K), all submitted at once to "
-                           "the serving loop, 16 in flight on their own streams",
+                           "the serving loop, 32 in flight on their own streams",
             "schedule": tuned, "tiles_by_grid": tiles, "setup_s": setup_s,
             "cpu_baseline": {"kind": kind, "cores": 1, "cell_steps_per_s": cpu_rate,
                              "sample": f"{len(sample)} chips stratified by side, one interval each, "
