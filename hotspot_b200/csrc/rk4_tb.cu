@@ -28,12 +28,16 @@
 // which the package recursion needs, are sum_k h^{m-k} ER[m-1-k] V^p_k with
 // ER[j][e'][e] = sum over edge e of L_cc^j L_cp u_{e'} -- a small FP64 table
 // computed once per model.  An attempt therefore takes two chip barriers:
-//   phase 1  every tile: A by temporal blocking; tiles at least dE cells from
-//            the boundary (where B = 0) finish their cells (candidate state,
-//            error); boundary tiles record the edge sums of A_0 .. A_{dE-1}
+//   phase 1  every tile: A by temporal blocking.  Cells at least dE cells
+//            from the grid's edge (where every B_m is 0) finish (candidate
+//            state, error); the others keep the A part of their increment in
+//            the candidate state and of their error sum in an FP64 buffer;
+//            boundary tiles record the edge sums of A_0 .. A_{dE-1}
 //   barrier; every CTA runs the package recursion (scalars, FP64)
-//   phase 2  tiles within dE cells of the boundary: V = A + B by temporal
-//            blocking with the now known package values, finishing their cells
+//   phase 2  B on the band of width dE along the grid's edge, in boxes
+//            (about one per CTA) whose grid-edge sides are fixed and whose
+//            other sides carry a dE + 1 halo; the band cells finish
+//            (increment += sum D_m B_m, error |E.A + E.B|)
 //   barrier; every CTA reads the error norm and takes the step decision.
 // Edge sums are reduced in a fixed order (per-tile partials), so results do
 // not depend on timing.
