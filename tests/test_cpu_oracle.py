@@ -93,3 +93,25 @@ def test_reference_steady_stops_short_of_convergence(workdir):
     T, _ = o.steady_direct(avg)
     gap = np.max(np.abs(o.grid("steady") - T))
     assert 1e-5 < gap < 1e-2
+
+
+def test_x87_rounding_spread(workdir):
+    """The oracle built with x87 80-bit intermediates runs the same algorithm
+    with other roundings: on a 1 ms interval of a 32x32 chip (rejected and
+    retried steps) it takes the same steps and moves the result by a few
+    rounding units, the floor the FP64 blocked form is held to on such
+    inputs."""
+    import contextlib
+    from oracle.restatement import x87_rounding
+    sc = W.scenario_chip2d(workdir, seed=88, grid=32, steps=2)
+    sc.dt = 1e-3
+    out = []
+    for ctx in (contextlib.nullcontext(), x87_rounding()):
+        with ctx:
+            o = OracleModel(sc)
+            t = o.vector(o.init_temp)
+            steps = o.compute_temp(o.power_vector(sc.block_power[0]), t, sc.dt)
+            out.append((steps, t.copy(), o.grid("trans")))
+    assert out[0][0] == out[1][0]
+    spread = max(np.max(np.abs(out[0][1] - out[1][1])), np.max(np.abs(out[0][2] - out[1][2])))
+    assert 0.0 < spread < 1e-6, spread
