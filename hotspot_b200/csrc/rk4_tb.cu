@@ -132,7 +132,8 @@ template <> __device__ __forceinline__ const double *tb_power_of<double>(const T
 // ---------------------------------------------------------------------------
 // one stencil pass over the region rectangle [ra, rb) x [ca, cb) of an
 // RI x RJ box whose cell (0, 0) is grid cell (gi0, gj0):
-// P0: dst = V_0 = (p + L y) / C from the state deviations in src;
+// P0: dst = V_0 = (p + L y) / C from the state deviations in src, with the
+// grid power p already in dst (staged with the state box);
 // else dst = h L src.  Package inputs from xs (BND: grid-boundary cells
 // present in the region).  The operation order per cell is rk4_krylov.cu's.
 // The rectangle's columns are dealt to the CTA's threads in row-major order
@@ -164,8 +165,6 @@ __device__ __forceinline__ void tb_pass(const TChip &C, const TSh<V> &sh, const 
     const V *p = src + r * RJ + c;
     V *o = dst + r * RJ + c;
     const bool hN = !BND || gi > 0, hS = !BND || gi < nr - 1, hW = !BND || gj > 0, hE = !BND || gj < nc - 1;
-    const V *pw = nullptr;
-    if constexpr (P0) pw = tb_power_of<V>(C) + (long long)gi * nc + gj;
     V up = 0, cur = p[0], gup = 0;
 #pragma unroll
     for (int n = 0; n < NL; n++) {
@@ -200,7 +199,7 @@ __device__ __forceinline__ void tb_pass(const TChip &C, const TSh<V> &sh, const 
           if (gj == 0) s += gEdgeEW * (xs[nb + 0] - cur);
         }
       }
-      if constexpr (P0) o[n * LP] = (__ldg(pw + (long long)n * C.plane) + s) * invC;
+      if constexpr (P0) o[n * LP] = (o[n * LP] + s) * invC;   // the grid power, staged with the state box
       else o[n * LP] = s * (invC * hf);
       gup = gDn;
       up = cur;
@@ -305,8 +304,12 @@ __device__ void tb_subtile(const TChip &C, TSh<V> &sh, V *buf0, V *buf1, const d
       const int gj = gj0 + c;
       if ((unsigned)gj >= (unsigned)nc) continue;
       const double *py = yb + (long long)gi * nc + gj;
+      const V *pw = tb_power_of<V>(C) + (long long)gi * nc + gj;
 #pragma unroll
-      for (int n = 0; n < NL; n++) buf0[n * LP + r * RJ + c] = (V)(__ldcg(py + (long long)n * C.plane) - amb);
+      for (int n = 0; n < NL; n++) {
+        buf0[n * LP + r * RJ + c] = (V)(__ldcg(py + (long long)n * C.plane) - amb);
+        buf1[n * LP + r * RJ + c] = __ldcg(pw + (long long)n * C.plane);   // pass 0 adds it in place
+      }
     }
   }
   if (tid < C.nx) sh.xs[0][tid] = (V)(sh.yp[tid] - amb);
