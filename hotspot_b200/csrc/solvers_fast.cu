@@ -480,9 +480,11 @@ __global__ void __launch_bounds__(32)
 #pragma unroll
         for (int u = 0; u < LFP; u += 4)
           *reinterpret_cast<float4 *>(lr + u) = *reinterpret_cast<const float4 *>(lf + (r * NL + n) * LFP + u);
+        // oldest values first: the value just computed (m = 1) enters last,
+        // so the recurrence waits on one multiply-add per unknown, not NL
         float a = rv[n];
 #pragma unroll
-        for (int m = 1; m <= NL; m++) a -= lr[m - 1] * (m <= n ? ycur[n - m] : yprev[NL + n - m]);
+        for (int m = NL; m >= 1; m--) a -= lr[m - 1] * (m <= n ? ycur[n - m] : yprev[NL + n - m]);
         ycur[n] = a;
         rv[n] = a;
       }
@@ -526,7 +528,7 @@ __global__ void __launch_bounds__(32)
           *reinterpret_cast<float4 *>(ur + u) = *reinterpret_cast<const float4 *>(ub + (r * NL + n) * UBP + u);
         float a = yv[n];
 #pragma unroll
-        for (int m = 1; m <= NL; m++) a -= ur[m - 1] * (n + m < NL ? xcur[n + m] : xnext[n + m - NL]);
+        for (int m = NL; m >= 1; m--) a -= ur[m - 1] * (n + m < NL ? xcur[n + m] : xnext[n + m - NL]);
         xcur[n] = a * ur[NL];
       }
 #pragma unroll
